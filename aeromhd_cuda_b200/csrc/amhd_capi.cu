@@ -1,0 +1,662 @@
+// amhd_capi.cu -- the extern "C" entry points of libaeromhd.so (include/aeromhd.h):
+// argument checks, precision dispatch, and the launch sequences of the step,
+// the device-side run loop and the ensemble.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "aeromhd.h"
+#include "amhd_launch.h"
+
+using namespace amhd;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                            \
+    do {                                                                                    \
+        cudaError_t e__ = (call);                                                           \
+        if (e__ != cudaSuccess) return fail(AMHD_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e__)); \
+    } while (0)
+
+constexpr int kNG = 2;
+constexpr int kTY = 32;
+
+int g_tile_x = 8;
+int g_ctas_per_sm = 0;
+
+inline size_t elem_size(int dtype) { return dtype == AMHD_F32 ? 4 : 8; }
+
+int check_grid(const amhd_grid *g)
+{
+    if (!g) return fail(AMHD_ERR_ARG, "grid is NULL");
+    if (g->nx < 2 || g->ny < 2) return fail(AMHD_ERR_ARG, "grid must be at least 2x2 cells (got %dx%d)", g->nx, g->ny);
+    if (g->dtype != AMHD_F32 && g->dtype != AMHD_F64) return fail(AMHD_ERR_ARG, "unknown dtype %d", g->dtype);
+    if (g->pitch < g->ny + 2 * kNG) return fail(AMHD_ERR_ARG, "pitch %d < ny+4", g->pitch);
+    if (g->var_stride < (int64_t)(g->nx + 2 * kNG) * g->pitch)
+        return fail(AMHD_ERR_ARG, "var_stride %lld < (nx+4)*pitch", (long long)g->var_stride);
+    if (!(g->dx > 0) || !(g->dy > 0)) return fail(AMHD_ERR_ARG, "dx, dy must be positive");
+    if (!(g->gamma > 1)) return fail(AMHD_ERR_ARG, "gamma must exceed 1");
+    if (g->bc_x < 0 || g->bc_x > 2 || g->bc_y < 0 || g->bc_y > 2) return fail(AMHD_ERR_ARG, "unknown boundary kind");
+    if (g->limiter != AMHD_LIMITER_VANLEER && g->limiter != AMHD_LIMITER_MINMOD)
+        return fail(AMHD_ERR_ARG, "unknown limiter %d", g->limiter);
+    return AMHD_OK;
+}
+
+void padded_dims(int nx, int ny, int *pitch, int *rows)
+{
+    *pitch = kTY * ((ny + kTY - 1) / kTY) + 2 * kNG;
+    *rows = 16 * ((nx + 15) / 16) + 2 * kNG;
+}
+
+int check_padded(const amhd_grid *g, const void *const *ptrs, int n)
+{
+    int pitch, rows;
+    padded_dims(g->nx, g->ny, &pitch, &rows);
+    const size_t es = elem_size(g->dtype);
+    if (g->pitch < pitch) return fail(AMHD_ERR_ARG, "fused step needs pitch >= %d (got %d)", pitch, g->pitch);
+    if (g->var_stride < (int64_t)rows * g->pitch)
+        return fail(AMHD_ERR_ARG, "fused step needs var_stride >= %d * pitch", rows);
+    if ((g->pitch * es) % 16 || (g->var_stride * es) % 16)
+        return fail(AMHD_ERR_ARG, "pitch and var_stride must be multiples of 16 bytes");
+    for (int k = 0; k < n; ++k) {
+        if (!ptrs[k]) return fail(AMHD_ERR_ARG, "state pointer %d is NULL", k);
+        if (reinterpret_cast<uintptr_t>(ptrs[k]) % 16) return fail(AMHD_ERR_ARG, "state pointer %d not 16-byte aligned", k);
+    }
+    return AMHD_OK;
+}
+
+Layout layout_of(const amhd_grid *g) { return Layout{g->nx + 2 * kNG, g->ny + 2 * kNG, g->pitch, g->var_stride}; }
+
+amhd_instance single_instance(const amhd_grid *g, int tile_x)
+{
+    amhd_instance in;
+    memset(&in, 0, sizeof in);
+    in.grid = *g;
+    in.offset = 0;
+    in.first_tile = 0;
+    in.tiles_x = (g->nx + tile_x - 1) / tile_x;
+    in.tiles_y = (g->ny + kTY - 1) / kTY;
+    return in;
+}
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int stage_grid(int dtype, int tile_x, int n_tiles, int ctas_per_sm)
+{
+    if (ctas_per_sm <= 0) return n_tiles;
+    int per = ctas_per_sm;
+    const int occ = dtype == AMHD_F64 ? Launch<double>::stage_ctas_per_sm(tile_x)
+                                      : Launch<float>::stage_ctas_per_sm(tile_x);
+    if (per > occ) per = occ;
+    int grid = per * device_sm_count();
+    return grid < n_tiles ? grid : n_tiles;
+}
+
+cudaError_t run_stage(int dtype, int stage, int tile_x, const StageParams &p, int grid, cudaStream_t s)
+{
+    return dtype == AMHD_F64 ? Launch<double>::stage(stage, tile_x, p, grid, s)
+                             : Launch<float>::stage(stage, tile_x, p, grid, s);
+}
+
+cudaError_t run_bc_fill(const amhd_grid *g, void *U, cudaStream_t s)
+{
+    return g->dtype == AMHD_F64 ? Launch<double>::bc_fill(*g, static_cast<double *>(U), s)
+                                : Launch<float>::bc_fill(*g, static_cast<float *>(U), s);
+}
+
+cudaError_t run_finalize(int dtype, const amhd_instance *insts, int n, const amhd_instance &one, const void *U,
+                         amhd_control *ctl, int advance, int set_only, cudaStream_t s)
+{
+    return dtype == AMHD_F64
+               ? Launch<double>::finalize(insts, n, one, static_cast<const double *>(U), ctl, advance, set_only, s)
+               : Launch<float>::finalize(insts, n, one, static_cast<const float *>(U), ctl, advance, set_only, s);
+}
+
+cudaError_t run_dt_reduce(const amhd_grid *g, const void *A, int from_prim, amhd_control *ctl, cudaStream_t s)
+{
+    const Layout l = layout_of(g);
+    return g->dtype == AMHD_F64
+               ? Launch<double>::dt_reduce(l, static_cast<const double *>(A), from_prim, g->gamma, ctl, s)
+               : Launch<float>::dt_reduce(l, static_cast<const float *>(A), from_prim, g->gamma, ctl, s);
+}
+
+// three fused stages of one step; dt/ch/decay from the host or from ctl
+int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instance *insts, const int32_t *tile_inst,
+                 int n_tiles, int tile_x, int grid, void *U, void *U1, void *U2, amhd_control *ctl, int use_ctl,
+                 double dt, double ch, double decay, int fuse_dt, cudaStream_t s)
+{
+    StageParams p;
+    memset(&p, 0, sizeof p);
+    p.inst = insts;
+    p.one = one;
+    p.tile_inst = tile_inst;
+    p.n_tiles = n_tiles;
+    p.ctl = ctl;
+    p.dt = dt;
+    p.ch = ch;
+    p.decay = decay;
+    p.use_ctl = use_ctl;
+    const int dtype = g->dtype;
+    p.uin = U;
+    p.u0 = U;
+    p.uout = U1;
+    CK(run_stage(dtype, 1, tile_x, p, grid, s));
+    p.uin = U1;
+    p.uout = U2;
+    CK(run_stage(dtype, 2, tile_x, p, grid, s));
+    p.uin = U2;
+    p.uout = U;
+    p.fuse_dt = fuse_dt;
+    CK(run_stage(dtype, 3, tile_x, p, grid, s));
+    return AMHD_OK;
+}
+
+int control_upload(amhd_control *ctl, double t, double t_end, int64_t step, int64_t max_steps, cudaStream_t s)
+{
+    amhd_control h;
+    memset(&h, 0, sizeof h);
+    h.t = t;
+    h.t_end = t_end;
+    h.step = step;
+    h.max_steps = max_steps;
+    h.active = 1;
+    h.decay = 1.0;
+    h.snap_t = __builtin_inf();
+    // pageable source: the copy is staged before the call returns
+    CK(cudaMemcpyAsync(ctl, &h, sizeof h, cudaMemcpyHostToDevice, s));
+    return AMHD_OK;
+}
+
+}  // namespace
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+const char *amhd_version(void) { return "aeromhd-b200 0.1.0 (sm_100a)"; }
+
+const char *amhd_last_error(void) { return g_err.c_str(); }
+
+int amhd_init(void)
+{
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    if (n <= 0) return fail(AMHD_ERR_CUDA, "no CUDA device");
+    CK(Launch<double>::configure());
+    CK(Launch<float>::configure());
+    return AMHD_OK;
+}
+
+size_t amhd_control_size(void) { return sizeof(amhd_control); }
+
+int amhd_padded_layout(int32_t nx, int32_t ny, int32_t dtype, int32_t *pitch, int32_t *rows)
+{
+    if (nx < 2 || ny < 2) return fail(AMHD_ERR_ARG, "grid must be at least 2x2 cells");
+    if (dtype != AMHD_F32 && dtype != AMHD_F64) return fail(AMHD_ERR_ARG, "unknown dtype %d", dtype);
+    if (!pitch || !rows) return fail(AMHD_ERR_ARG, "NULL output");
+    padded_dims(nx, ny, pitch, rows);
+    return AMHD_OK;
+}
+
+int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm)
+{
+    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16");
+    if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(AMHD_ERR_ARG, "ctas_per_sm out of range");
+    g_tile_x = tile_x;
+    g_ctas_per_sm = ctas_per_sm;
+    return AMHD_OK;
+}
+
+int amhd_stage_info(int32_t dtype, int32_t tile_x, int32_t *smem_bytes, int32_t *ctas_per_sm, int32_t *sm_count)
+{
+    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16");
+    if (dtype != AMHD_F32 && dtype != AMHD_F64) return fail(AMHD_ERR_ARG, "unknown dtype %d", dtype);
+    if (smem_bytes)
+        *smem_bytes = (int32_t)(dtype == AMHD_F64 ? Launch<double>::stage_smem(tile_x) : Launch<float>::stage_smem(tile_x));
+    if (ctas_per_sm)
+        *ctas_per_sm = dtype == AMHD_F64 ? Launch<double>::stage_ctas_per_sm(tile_x)
+                                         : Launch<float>::stage_ctas_per_sm(tile_x);
+    if (sm_count) *sm_count = device_sm_count();
+    return AMHD_OK;
+}
+
+int amhd_cons_to_prim(const amhd_grid *g, const void *U, void *W, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !W) return fail(AMHD_ERR_ARG, "NULL array");
+    const Layout l = layout_of(g);
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::cons_to_prim(l, static_cast<const double *>(U), l, static_cast<double *>(W), g->gamma, S(stream)));
+    else
+        CK(Launch<float>::cons_to_prim(l, static_cast<const float *>(U), l, static_cast<float *>(W), g->gamma, S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_prim_to_cons(const amhd_grid *g, const void *W, void *U, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !W) return fail(AMHD_ERR_ARG, "NULL array");
+    const Layout l = layout_of(g);
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::prim_to_cons(l, static_cast<const double *>(W), l, static_cast<double *>(U), g->gamma, S(stream)));
+    else
+        CK(Launch<float>::prim_to_cons(l, static_cast<const float *>(W), l, static_cast<float *>(U), g->gamma, S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_muscl(const amhd_grid *g, int32_t axis, const void *W, void *WL, void *WR, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (axis != 0 && axis != 1) return fail(AMHD_ERR_ARG, "axis must be 0 or 1");
+    if (!W || !WL || !WR) return fail(AMHD_ERR_ARG, "NULL array");
+    const Layout l = layout_of(g);
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::muscl(l, static_cast<const double *>(W), axis, g->limiter, static_cast<double *>(WL),
+                                 static_cast<double *>(WR), S(stream)));
+    else
+        CK(Launch<float>::muscl(l, static_cast<const float *>(W), axis, g->limiter, static_cast<float *>(WL),
+                                static_cast<float *>(WR), S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_hlld_flux(int32_t axis, int32_t dtype, const void *WL, const void *WR, void *F, void *smax, int64_t n_faces,
+                   double gamma, double ch, void *stream)
+{
+    if (axis != 0 && axis != 1) return fail(AMHD_ERR_ARG, "axis must be 0 or 1");
+    if (dtype != AMHD_F32 && dtype != AMHD_F64) return fail(AMHD_ERR_ARG, "unknown dtype %d", dtype);
+    if (n_faces < 0) return fail(AMHD_ERR_ARG, "n_faces < 0");
+    if (n_faces == 0) return AMHD_OK;
+    if (!WL || !WR || !F) return fail(AMHD_ERR_ARG, "NULL array");
+    if (dtype == AMHD_F64)
+        CK(Launch<double>::hlld(static_cast<const double *>(WL), static_cast<const double *>(WR), static_cast<double *>(F),
+                                static_cast<double *>(smax), n_faces, axis, gamma, ch, S(stream)));
+    else
+        CK(Launch<float>::hlld(static_cast<const float *>(WL), static_cast<const float *>(WR), static_cast<float *>(F),
+                               static_cast<float *>(smax), n_faces, axis, gamma, ch, S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_apply_bc(const amhd_grid *g, void *U, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U) return fail(AMHD_ERR_ARG, "NULL array");
+    CK(run_bc_fill(g, U, S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_enforce_scalar_bounds(const amhd_grid *g, void *U, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U) return fail(AMHD_ERR_ARG, "NULL array");
+    const Layout l = layout_of(g);
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::scalar_bounds(l, static_cast<double *>(U), S(stream)));
+    else
+        CK(Launch<float>::scalar_bounds(l, static_cast<float *>(U), S(stream)));
+    return AMHD_OK;
+}
+
+static int compute_dt_impl(const amhd_grid *g, const void *A, int from_prim, amhd_control *ctl, double *dt_host,
+                           double *ch_host, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!A || !ctl) return fail(AMHD_ERR_ARG, "NULL array or control");
+    cudaStream_t s = S(stream);
+    CK(cudaMemsetAsync(&ctl->red[0], 0, sizeof(ctl->red), s));
+    CK(run_dt_reduce(g, A, from_prim, ctl, s));
+    const amhd_instance one = single_instance(g, 8);
+    CK(run_finalize(g->dtype, nullptr, 1, one, nullptr, ctl, 0, 1, s));
+    if (dt_host || ch_host) {
+        double v[2];
+        CK(cudaMemcpyAsync(&v[0], &ctl->dt_cfl, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&v[1], &ctl->ch, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (dt_host) *dt_host = v[0];
+        if (ch_host) *ch_host = v[1];
+    }
+    return AMHD_OK;
+}
+
+int amhd_compute_dt(const amhd_grid *g, const void *W, amhd_control *ctl, double *dt_host, double *ch_host,
+                    void *stream)
+{
+    return compute_dt_impl(g, W, 1, ctl, dt_host, ch_host, stream);
+}
+
+int amhd_compute_dt_cons(const amhd_grid *g, const void *U, amhd_control *ctl, double *dt_host, double *ch_host,
+                         void *stream)
+{
+    return compute_dt_impl(g, U, 0, ctl, dt_host, ch_host, stream);
+}
+
+int amhd_boundary_energy_flux(const amhd_grid *g, const void *U, amhd_control *ctl, double *out_host, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !ctl || !out_host) return fail(AMHD_ERR_ARG, "NULL argument");
+    if (g->bc_x == AMHD_BC_PERIODIC) {
+        *out_host = 0.0;
+        return AMHD_OK;
+    }
+    cudaStream_t s = S(stream);
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::bflux(*g, static_cast<const double *>(U), &ctl->reserved[0], s));
+    else
+        CK(Launch<float>::bflux(*g, static_cast<const float *>(U), &ctl->reserved[0], s));
+    CK(cudaMemcpyAsync(out_host, &ctl->reserved[0], sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return AMHD_OK;
+}
+
+int amhd_powell_source(const amhd_grid *g, const void *W, void *Sout, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!W || !Sout) return fail(AMHD_ERR_ARG, "NULL array");
+    const Layout l = layout_of(g);
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::powell(l, static_cast<const double *>(W), static_cast<double *>(Sout), g->dx, g->dy, S(stream)));
+    else
+        CK(Launch<float>::powell(l, static_cast<const float *>(W), static_cast<float *>(Sout), g->dx, g->dy, S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_compute_rhs(const amhd_grid *g, void *U, void *R, double ch, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    const void *ptrs[2] = {U, R};
+    if (int e = check_padded(g, ptrs, 2)) return e;
+    cudaStream_t s = S(stream);
+    CK(run_bc_fill(g, U, s));
+    CK(cudaMemsetAsync(R, 0, (size_t)g->var_stride * 10 * elem_size(g->dtype), s));
+    const int tx = g_tile_x;
+    const amhd_instance one = single_instance(g, tx);
+    StageParams p;
+    memset(&p, 0, sizeof p);
+    p.uin = U;
+    p.u0 = U;
+    p.uout = R;
+    p.one = one;
+    p.n_tiles = one.tiles_x * one.tiles_y;
+    p.ch = ch;
+    CK(run_stage(g->dtype, 0, tx, p, stage_grid(g->dtype, tx, p.n_tiles, g_ctas_per_sm), s));
+    return AMHD_OK;
+}
+
+int amhd_step_ssprk3(const amhd_grid *g, void *U, void *U1, void *U2, double dt, double ch, double decay,
+                     amhd_control *ctl, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    const void *ptrs[3] = {U, U1, U2};
+    if (int e = check_padded(g, ptrs, 3)) return e;
+    cudaStream_t s = S(stream);
+    if (ctl && g->bc_x != AMHD_BC_PERIODIC) {
+        // _cumulative_boundary_energy += flux(U0) * dt (solver.py:316-317), on the device
+        if (g->dtype == AMHD_F64)
+            CK(Launch<double>::bflux_accum(*g, static_cast<const double *>(U), ctl, dt, s));
+        else
+            CK(Launch<float>::bflux_accum(*g, static_cast<const float *>(U), ctl, dt, s));
+    }
+    CK(run_bc_fill(g, U, s));  // compute_rhs(U0) fills U0's ghosts first (solver.py:276)
+    const int tx = g_tile_x;
+    const amhd_instance one = single_instance(g, tx);
+    const int n_tiles = one.tiles_x * one.tiles_y;
+    return three_stages(g, one, nullptr, nullptr, n_tiles, tx, stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm), U,
+                        U1, U2, ctl, 0, dt, ch, ch > 0 ? decay : 1.0, 0, s);
+}
+
+int amhd_rk_stage(const amhd_grid *g, int32_t stage, const void *Uin, const void *U0, void *Uout, double dt,
+                  double ch, double decay, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (stage < 1 || stage > 3) return fail(AMHD_ERR_ARG, "stage must be 1, 2 or 3");
+    const void *ptrs[3] = {Uin, U0, Uout};
+    if (int e = check_padded(g, ptrs, 3)) return e;
+    const int tx = g_tile_x;
+    const amhd_instance one = single_instance(g, tx);
+    StageParams p;
+    memset(&p, 0, sizeof p);
+    p.uin = Uin;
+    p.u0 = U0;
+    p.uout = Uout;
+    p.one = one;
+    p.n_tiles = one.tiles_x * one.tiles_y;
+    p.dt = dt;
+    p.ch = ch;
+    p.decay = ch > 0 ? decay : 1.0;
+    CK(run_stage(g->dtype, stage, tx, p, stage_grid(g->dtype, tx, p.n_tiles, g_ctas_per_sm), S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_control_init(const amhd_grid *g, const void *U, amhd_control *ctl, double t, double t_end, int64_t step,
+                      int64_t max_steps, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !ctl) return fail(AMHD_ERR_ARG, "NULL argument");
+    cudaStream_t s = S(stream);
+    if (int e = control_upload(ctl, t, t_end, step, max_steps, s)) return e;
+    // dt from the state as the caller left it, ghosts included (solver.py:476-477)
+    CK(run_dt_reduce(g, U, 0, ctl, s));
+    const amhd_instance one = single_instance(g, 8);
+    CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, 0, 0, s));
+    CK(run_bc_fill(g, const_cast<void *>(U), s));
+    return AMHD_OK;
+}
+
+int amhd_control_resume(amhd_control *ctl, int32_t n, double snap_t, void *stream)
+{
+    if (!ctl || n <= 0) return fail(AMHD_ERR_ARG, "bad control arguments");
+    CK(launch_control_resume(ctl, n, snap_t, S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    const void *ptrs[3] = {U, U1, U2};
+    if (int e = check_padded(g, ptrs, 3)) return e;
+    if (!ctl) return fail(AMHD_ERR_ARG, "NULL control");
+    if (n_steps < 0) return fail(AMHD_ERR_ARG, "n_steps < 0");
+    cudaStream_t s = S(stream);
+    const int tx = g_tile_x;
+    const amhd_instance one = single_instance(g, tx);
+    const int n_tiles = one.tiles_x * one.tiles_y;
+    const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
+    for (int k = 0; k < n_steps; ++k) {
+        if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, grid, U, U1, U2, ctl, 1, 0, 0, 1, 1, s))
+            return e;
+        CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, 1, 0, s));
+    }
+    return AMHD_OK;
+}
+
+int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps,
+                         double *ms_out, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    const void *ptrs[3] = {U, U1, U2};
+    if (int e = check_padded(g, ptrs, 3)) return e;
+    if (!ctl || !ms_out) return fail(AMHD_ERR_ARG, "NULL argument");
+    if (n_steps <= 0) return fail(AMHD_ERR_ARG, "n_steps must be positive");
+    cudaStream_t s = S(stream);
+    const int tx = g_tile_x;
+    const amhd_instance one = single_instance(g, tx);
+    const int n_tiles = one.tiles_x * one.tiles_y;
+    const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
+    std::vector<cudaEvent_t> ev(4 * (size_t)n_steps + 1);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    int rc = AMHD_OK;
+    StageParams p;
+    memset(&p, 0, sizeof p);
+    p.one = one;
+    p.n_tiles = n_tiles;
+    p.ctl = ctl;
+    p.use_ctl = 1;
+    cudaError_t ce = cudaEventRecord(ev[0], s);
+    for (int k = 0; k < n_steps && ce == cudaSuccess; ++k) {
+        for (int st = 1; st <= 3 && ce == cudaSuccess; ++st) {
+            p.uin = st == 1 ? U : (st == 2 ? U1 : U2);
+            p.u0 = U;
+            p.uout = st == 1 ? U1 : (st == 2 ? U2 : U);
+            p.fuse_dt = st == 3;
+            ce = run_stage(g->dtype, st, tx, p, grid, s);
+            if (ce == cudaSuccess) ce = cudaEventRecord(ev[4 * k + st], s);
+        }
+        if (ce == cudaSuccess) ce = run_finalize(g->dtype, nullptr, 1, one, U, ctl, 1, 0, s);
+        if (ce == cudaSuccess) ce = cudaEventRecord(ev[4 * k + 4], s);
+    }
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(ev.back());
+    if (ce != cudaSuccess) {
+        rc = fail(AMHD_ERR_CUDA, "amhd_advance_profile: %s", cudaGetErrorString(ce));
+    } else {
+        for (int q = 0; q < 5; ++q) ms_out[q] = 0.0;
+        for (int k = 0; k < n_steps; ++k)
+            for (int q = 0; q < 4; ++q) {
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, ev[4 * k + q], ev[4 * k + q + 1]);
+                ms_out[q] += ms;
+            }
+        float tot = 0.f;
+        cudaEventElapsedTime(&tot, ev[0], ev.back());
+        ms_out[4] = tot;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, void *dev_U2, amhd_control *ctl,
+                   double t, double t_end, double *out_host, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    const void *ptrs[3] = {dev_U, dev_U1, dev_U2};
+    if (int e = check_padded(g, ptrs, 3)) return e;
+    if (!U_host || !ctl) return fail(AMHD_ERR_ARG, "NULL argument");
+    cudaStream_t s = S(stream);
+    const size_t es = elem_size(g->dtype);
+    const int nxt = g->nx + 2 * kNG, nyt = g->ny + 2 * kNG;
+    char *h = static_cast<char *>(U_host);
+    char *d = static_cast<char *>(dev_U);
+    for (int v = 0; v < 10; ++v)
+        CK(cudaMemcpy2DAsync(d + (size_t)v * g->var_stride * es, (size_t)g->pitch * es, h + (size_t)v * nxt * nyt * es,
+                             (size_t)nyt * es, (size_t)nyt * es, nxt, cudaMemcpyHostToDevice, s));
+    // dt of this step from the uploaded state, ghosts as given (solver.py:476-479)
+    if (int e = control_upload(ctl, t, t_end, 0, 1, s)) return e;
+    CK(run_dt_reduce(g, dev_U, 0, ctl, s));
+    const int tx = g_tile_x;
+    const amhd_instance one = single_instance(g, tx);
+    CK(run_finalize(g->dtype, nullptr, 1, one, dev_U, ctl, 0, 0, s));
+    CK(run_bc_fill(g, dev_U, s));
+    const int n_tiles = one.tiles_x * one.tiles_y;
+    if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm),
+                             dev_U, dev_U1, dev_U2, ctl, 1, 0, 0, 1, 0, s))
+        return e;
+    CK(run_finalize(g->dtype, nullptr, 1, one, dev_U, ctl, 1, 0, s));
+    for (int v = 0; v < 10; ++v)
+        CK(cudaMemcpy2DAsync(h + (size_t)v * nxt * nyt * es, (size_t)nyt * es, d + (size_t)v * g->var_stride * es,
+                             (size_t)g->pitch * es, (size_t)nyt * es, nxt, cudaMemcpyDeviceToHost, s));
+    amhd_control r;
+    CK(cudaMemcpyAsync(&r, ctl, sizeof r, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (out_host) {
+        out_host[0] = r.t;
+        out_host[1] = r.last_dt;
+        out_host[2] = r.ch;
+        out_host[3] = r.e_bnd;
+    }
+    if (r.flags & AMHD_FLAG_NONFINITE) return fail(AMHD_ERR_NONFINITE, "non-finite value in the new state");
+    return AMHD_OK;
+}
+
+int amhd_diagnostics(const amhd_grid *g, const void *U, double x0, double *out_dev, double *rows_dev, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !out_dev || !rows_dev) return fail(AMHD_ERR_ARG, "NULL argument");
+    cudaStream_t s = S(stream);
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::diag_rows(*g, static_cast<const double *>(U), rows_dev, s));
+    else
+        CK(Launch<float>::diag_rows(*g, static_cast<const float *>(U), rows_dev, s));
+    CK(launch_diag_finish(*g, x0, rows_dev, out_dev, s));
+    return AMHD_OK;
+}
+
+int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst_dev, int32_t n_inst, int32_t dtype,
+                       void *U, amhd_control *ctl_dev, double t_end, int64_t max_steps, void *stream)
+{
+    if (!inst_host || !inst_dev || !U || !ctl_dev || n_inst <= 0) return fail(AMHD_ERR_ARG, "bad ensemble arguments");
+    cudaStream_t s = S(stream);
+    const size_t es = elem_size(dtype);
+    std::vector<amhd_control> h(n_inst);
+    memset(h.data(), 0, sizeof(amhd_control) * n_inst);
+    for (int k = 0; k < n_inst; ++k) {
+        h[k].t_end = t_end;
+        h[k].max_steps = max_steps;
+        h[k].active = 1;
+        h[k].decay = 1.0;
+        h[k].snap_t = __builtin_inf();
+    }
+    CK(cudaMemcpyAsync(ctl_dev, h.data(), sizeof(amhd_control) * n_inst, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));  // h goes out of scope
+    for (int k = 0; k < n_inst; ++k) {
+        const amhd_grid *g = &inst_host[k].grid;
+        if (int e = check_grid(g)) return fail(e, "instance %d: %s", k, g_err.c_str());
+        if (g->dtype != dtype) return fail(AMHD_ERR_ARG, "instance %d has a different dtype", k);
+        void *Uk = static_cast<char *>(U) + (size_t)inst_host[k].offset * es;
+        CK(run_dt_reduce(g, Uk, 0, ctl_dev + k, s));
+    }
+    amhd_instance dummy;
+    memset(&dummy, 0, sizeof dummy);
+    CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 0, 0, s));
+    for (int k = 0; k < n_inst; ++k) {
+        void *Uk = static_cast<char *>(U) + (size_t)inst_host[k].offset * es;
+        CK(run_bc_fill(&inst_host[k].grid, Uk, s));
+    }
+    return AMHD_OK;
+}
+
+int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev, int32_t n_tiles,
+                          int32_t dtype, int32_t tile_x, void *U, void *U1, void *U2, amhd_control *ctl_dev,
+                          int32_t n_steps, int32_t ctas, void *stream)
+{
+    if (!inst_dev || !tile_inst_dev || !U || !U1 || !U2 || !ctl_dev || n_inst <= 0 || n_tiles <= 0)
+        return fail(AMHD_ERR_ARG, "bad ensemble arguments");
+    if (dtype != AMHD_F32 && dtype != AMHD_F64) return fail(AMHD_ERR_ARG, "unknown dtype %d", dtype);
+    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16");
+    cudaStream_t s = S(stream);
+    int grid = ctas;
+    if (grid <= 0) {
+        const int occ = dtype == AMHD_F64 ? Launch<double>::stage_ctas_per_sm(tile_x)
+                                          : Launch<float>::stage_ctas_per_sm(tile_x);
+        grid = occ * device_sm_count();
+    }
+    if (grid > n_tiles) grid = n_tiles;
+    amhd_grid gdt;
+    memset(&gdt, 0, sizeof gdt);
+    gdt.dtype = dtype;
+    amhd_instance dummy;
+    memset(&dummy, 0, sizeof dummy);
+    for (int k = 0; k < n_steps; ++k) {
+        if (int e = three_stages(&gdt, dummy, inst_dev, tile_inst_dev, n_tiles, tile_x, grid, U, U1, U2, ctl_dev, 1, 0,
+                                 0, 1, 1, s))
+            return e;
+        CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 1, 0, s));
+    }
+    return AMHD_OK;
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

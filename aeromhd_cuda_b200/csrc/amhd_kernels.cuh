@@ -1,0 +1,712 @@
+// amhd_kernels.cuh -- CUDA kernels of the MHD hot path, templated on the real
+// type.  Included by amhd_f64.cu (Real = double, -fmad=false) and amhd_f32.cu
+// (Real = float).  Host-side launchers are declared in amhd_launch.h.
+//
+// The fused RK stage (rk_stage_kernel) does, per 8..16 x 32 tile of interior
+// cells: stage the tile plus its 2-cell halo of the stage's input state into
+// shared memory as primitives (float64 pressure recovery), MUSCL + HLLD on
+// every x and y face of the tile (interface states and fluxes never leave
+// shared memory / registers), flux divergence + Powell source, the SSP-RK3
+// combination with the step's base state, the passive-scalar clamp, psi
+// damping (last stage), the boundary conditions (boundary cells push their
+// values into the ghost cells that copy them), and on the last stage the CFL
+// reduction of the new state for the next dt.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "aeromhd.h"
+#include "amhd_launch.h"
+#include "amhd_physics.cuh"
+
+namespace amhd {
+
+constexpr int TY = 32;           // tile width along y (the contiguous axis): one warp
+constexpr int HW = TY + 2 * NG;  // halo width along y
+
+template <typename R>
+struct Vec;
+template <>
+struct Vec<float> {
+    using T = float4;
+    static constexpr int N = 4;
+};
+template <>
+struct Vec<double> {
+    using T = double2;
+    static constexpr int N = 2;
+};
+
+template <typename R, int TX>
+struct TileSmem {
+    R w[NV][TX + 2 * NG][HW];      // primitives of the tile + halo
+    R fx[NV][TX + 1][TY];          // x-face fluxes (face a: between tile rows a-1 and a)
+    R fy[NV][TX][TY + 1];          // y-face fluxes
+    unsigned long long red[4][32]; // per-warp dt partials
+    int nonfinite;
+};
+
+__device__ __forceinline__ const amhd_instance &inst_of(const StageParams &p, int tile, int &inst_idx)
+{
+    if (p.inst != nullptr) {
+        inst_idx = p.tile_inst[tile];
+        return p.inst[inst_idx];
+    }
+    inst_idx = 0;
+    return p.one;
+}
+
+// ---------------------------------------------------------------------------
+// fused RK stage; STAGE 1..3 (solver.py:319-329), STAGE 0 = compute_rhs (R out)
+// ---------------------------------------------------------------------------
+template <typename R, int TX, int STAGE>
+__device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, TX> &sm, int tile)
+{
+    constexpr int NT = TX * TY;  // threads per block: one per tile cell
+    constexpr int VN = Vec<R>::N;
+    constexpr int HROWS = TX + 2 * NG;
+    using VT = typename Vec<R>::T;
+
+    int ii;
+    const amhd_instance &in = inst_of(p, tile, ii);
+    const amhd_grid g = in.grid;
+    amhd_control *ctl = p.ctl ? p.ctl + ii : nullptr;
+
+    double dt = p.dt, ch = p.ch, decay = p.decay;
+    if (p.use_ctl) {
+        if (!ctl->active) return;
+        dt = ctl->dt;
+        ch = ctl->ch;
+        decay = ctl->decay;
+    }
+    const int local = tile - in.first_tile;
+    const int ty = local % in.tiles_y, tx = local / in.tiles_y;
+    const int i0 = NG + tx * TX, j0 = NG + ty * TY;  // first interior cell of the tile
+    const int64_t vs = g.var_stride;
+    const int pitch = g.pitch;
+    const R *uin = reinterpret_cast<const R *>(p.uin) + in.offset;
+    const R *u0 = reinterpret_cast<const R *>(p.u0) + in.offset;
+    R *uout = reinterpret_cast<R *>(p.uout) + in.offset;
+    const int t = threadIdx.x;
+
+    // ---- phase A: tile + halo -> primitives in shared memory --------------
+    // the padded layout keeps every halo row/column of every tile in bounds
+    constexpr int QPR = HW / VN;  // vectors per halo row
+    for (int q = t; q < HROWS * QPR; q += NT) {
+        const int r = q / QPR, c = (q % QPR) * VN;
+        const int64_t gi = (int64_t)(i0 - NG + r) * pitch + (j0 - NG + c);
+        R u[VN][NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            VT x = __ldg(reinterpret_cast<const VT *>(uin + v * vs + gi));
+            const R *xs = reinterpret_cast<const R *>(&x);
+#pragma unroll
+            for (int k = 0; k < VN; ++k) u[k][v] = xs[k];
+        }
+#pragma unroll
+        for (int k = 0; k < VN; ++k) {
+            R w[NV];
+            cons_to_prim_cell(u[k], g.gamma, w);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sm.w[v][r][c + k] = w[v];
+        }
+    }
+    __syncthreads();
+
+    // ---- phase B: MUSCL + HLLD on all faces of the tile -------------------
+    const R gam = R(g.gamma), chr = R(ch);
+    const int lim = g.limiter;
+    constexpr int NFX = (TX + 1) * TY;
+    constexpr int NFY = TX * (TY + 1);
+    for (int f = t; f < NFX + NFY; f += NT) {
+        R wl[NV], wr[NV], fl[NV];
+        if (f < NFX) {
+            const int a = f / TY, c = f % TY + NG;  // face between halo rows a+1, a+2
+#pragma unroll
+            for (int v = 0; v < NV; ++v)
+                muscl_pair(sm.w[v][a][c], sm.w[v][a + 1][c], sm.w[v][a + 2][c], sm.w[v][a + 3][c], lim, wl[v],
+                           wr[v]);
+        } else {
+            const int h = f - NFX;
+            const int a = h / (TY + 1) + NG, k = h % (TY + 1);  // face between halo cols k+1, k+2
+#pragma unroll
+            for (int v = 0; v < NV; ++v)
+                muscl_pair(sm.w[v][a][k], sm.w[v][a][k + 1], sm.w[v][a][k + 2], sm.w[v][a][k + 3], lim, wl[v],
+                           wr[v]);
+        }
+        wl[RHO] = np_max(wl[RHO], R(FLOOR_RHO));
+        wr[RHO] = np_max(wr[RHO], R(FLOOR_RHO));
+        wl[IPR] = np_max(wl[IPR], R(FLOOR_PR));
+        wr[IPR] = np_max(wr[IPR], R(FLOOR_PR));
+        if (f < NFX) {
+            hlld_flux(wl, wr, gam, chr, fl);
+            const int a = f / TY, c = f % TY;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sm.fx[v][a][c] = fl[v];
+        } else {
+            rot_xy(wl);
+            rot_xy(wr);
+            hlld_flux(wl, wr, gam, chr, fl);
+            rot_xy(fl);
+            const int h = f - NFX;
+            const int a = h / (TY + 1), k = h % (TY + 1);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) sm.fy[v][a][k] = fl[v];
+        }
+    }
+    __syncthreads();
+
+    // ---- phase C: divergence, Powell, RK combine, clamp, BC push ----------
+    const int a = t / TY, c = t % TY;  // tile cell
+    const int i = i0 + a, j = j0 + c;   // storage index
+    const bool valid = (i < NG + g.nx) && (j < NG + g.ny);
+    unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
+    bool bad = false;
+    if (valid) {
+        const int64_t gi = (int64_t)i * pitch + j;
+        R rhs[NV];
+        const R dx = R(g.dx), dy = R(g.dy);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            R r0 = R(0);
+            r0 -= (sm.fx[v][a + 1][c] - sm.fx[v][a][c]) / dx;
+            r0 -= (sm.fy[v][a][c + 1] - sm.fy[v][a][c]) / dy;
+            rhs[v] = r0;
+        }
+        if (g.powell) {
+            // _compute_powell_source, solver.py:242-266 (centred face-average divB)
+            const int hr = a + NG, hc = c + NG;
+            R bxc = sm.w[BX][hr][hc], byc = sm.w[BY][hr][hc];
+            R divb = (R(0.5) * (bxc + sm.w[BX][hr + 1][hc]) - R(0.5) * (sm.w[BX][hr - 1][hc] + bxc)) / dx +
+                     (R(0.5) * (byc + sm.w[BY][hr][hc + 1]) - R(0.5) * (sm.w[BY][hr][hc - 1] + byc)) / dy;
+            R vx = sm.w[IVX][hr][hc], vy = sm.w[IVY][hr][hc], vz = sm.w[IVZ][hr][hc];
+            R bzc = sm.w[BZ][hr][hc];
+            R vb = vx * bxc + vy * byc + vz * bzc;
+            rhs[MX] += -divb * bxc;
+            rhs[MY] += -divb * byc;
+            rhs[MZ] += -divb * bzc;
+            rhs[BX] += -divb * vx;
+            rhs[BY] += -divb * vy;
+            rhs[BZ] += -divb * vz;
+            rhs[EN] += -divb * vb;
+            rhs[RHO] += R(0);  // the reference adds a zero source to these slots too
+            rhs[PSI] += R(0);
+            rhs[RHOC] += R(0);
+        }
+        R out[NV];
+        if (STAGE == 0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) out[v] = rhs[v];
+        } else {
+            const R dtr = R(dt);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                R b0 = u0[v * vs + gi];
+                if (STAGE == 1) {
+                    out[v] = b0 + dtr * rhs[v];
+                } else {
+                    R us = uin[v * vs + gi];
+                    if (STAGE == 2)
+                        out[v] = R(0.75) * b0 + R(0.25) * (us + dtr * rhs[v]);
+                    else
+                        out[v] = R(1.0 / 3.0) * b0 + R(2.0 / 3.0) * (us + dtr * rhs[v]);
+                }
+            }
+            // enforce_scalar_bounds, solver.py:199-204
+            R rho = np_max(out[RHO], R(FLOOR_RHO));
+            R cc = np_min(np_max(out[RHOC] / rho, R(0)), R(1));
+            out[RHOC] = rho * cc;
+            if (STAGE == 3) {
+                if (ch > 0.0) out[PSI] *= R(decay);  // solver.py:331-333
+                if (p.fuse_dt) {
+                    double qd[4];
+                    cfl_quantities(out, g.gamma, qd);
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) q[k] = ord_bits(qd[k]);
+                }
+#pragma unroll
+                for (int v = 0; v < NV; ++v) bad |= !isfinite((double)out[v]);
+            }
+        }
+        // write the cell and every ghost that copies it (apply_bc, solver.py:158-197)
+        int gx[4], gy[4];
+        const int nxg = (STAGE == 0) ? 0 : ghost_targets(i, g.nx, g.bc_x, gx);
+        const int nyg = (STAGE == 0) ? 0 : ghost_targets(j, g.ny, g.bc_y, gy);
+        const bool zero_psi_x = g.bc_x != AMHD_BC_PERIODIC;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            uout[v * vs + gi] = out[v];
+            for (int m = 0; m < nyg; ++m) uout[v * vs + (int64_t)i * pitch + gy[m]] = out[v];
+            const R ox = (v == PSI && zero_psi_x) ? R(0) : out[v];
+            for (int n = 0; n < nxg; ++n) {
+                uout[v * vs + (int64_t)gx[n] * pitch + j] = ox;
+                for (int m = 0; m < nyg; ++m) uout[v * vs + (int64_t)gx[n] * pitch + gy[m]] = ox;
+            }
+        }
+    }
+    if (STAGE == 3) {
+        // block reduction of the CFL maxima and of the non-finite flag
+        const int lane = t & 31, warp = t >> 5;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            for (int o = 16; o > 0; o >>= 1) q[k] = umax64(q[k], __shfl_xor_sync(0xffffffffu, q[k], o));
+        const unsigned any_bad = __any_sync(0xffffffffu, bad);
+        if (t == 0) sm.nonfinite = 0;
+        __syncthreads();
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) sm.red[k][warp] = q[k];
+            if (any_bad) sm.nonfinite = 1;
+        }
+        __syncthreads();
+        if (t == 0 && ctl != nullptr) {
+            if (p.fuse_dt) {
+                for (int k = 0; k < 4; ++k) {
+                    unsigned long long m = 0ull;
+                    for (int w = 0; w < NT / 32; ++w) m = umax64(m, sm.red[k][w]);
+                    atomicMax(reinterpret_cast<unsigned long long *>(&ctl->red[k]), m);
+                }
+            }
+            if (sm.nonfinite) atomicOr(&ctl->flags, AMHD_FLAG_NONFINITE);
+        }
+    }
+}
+
+template <typename R, int TX, int STAGE>
+__global__ void __launch_bounds__(TX * TY) rk_stage_kernel(const StageParams p)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TileSmem<R, TX> &sm = *reinterpret_cast<TileSmem<R, TX> *>(smem_raw);
+    for (int tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x) {
+        rk_stage_tile<R, TX, STAGE>(p, sm, tile);
+        __syncthreads();  // shared memory is reused by the next tile
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ghost fill by pull (apply_bc, solver.py:158-197): every ghost takes its
+// interior source, so one pass in any order reproduces the reference.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void bc_fill_kernel(const amhd_grid g, R *U)
+{
+    const int nxt = g.nx + 2 * NG, nyt = g.ny + 2 * NG;
+    const int64_t n_rows = 4LL * nyt;  // x-ghost rows, full length
+    const int64_t n_total = n_rows + 4LL * g.nx;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n_total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        int i, j;
+        if (k < n_rows) {
+            const int r = (int)(k / nyt);
+            i = r < NG ? r : nxt - 2 * NG + r;
+            j = (int)(k % nyt);
+        } else {
+            const int64_t h = k - n_rows;
+            i = NG + (int)(h / 4);
+            const int c = (int)(h % 4);
+            j = c < NG ? c : nyt - 2 * NG + c;
+        }
+        const int si = ghost_source(i, g.nx, g.bc_x), sj = ghost_source(j, g.ny, g.bc_y);
+        const bool xg = (i < NG) || (i >= NG + g.nx);
+        for (int v = 0; v < NV; ++v) {
+            R val = U[v * g.var_stride + (int64_t)si * g.pitch + sj];
+            if (v == PSI && xg && g.bc_x != AMHD_BC_PERIODIC) val = R(0);
+            U[v * g.var_stride + (int64_t)i * g.pitch + j] = val;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// elementwise kernels over all cells (ghosts included)
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void cons_to_prim_kernel(const Layout li, const R *U, const Layout lo, R *W, double gamma)
+{
+    const int64_t n = (int64_t)li.nxt * li.nyt;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k / li.nyt), j = (int)(k % li.nyt);
+        R u[NV], w[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) u[v] = U[v * li.var_stride + (int64_t)i * li.pitch + j];
+        cons_to_prim_cell(u, gamma, w);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) W[v * lo.var_stride + (int64_t)i * lo.pitch + j] = w[v];
+    }
+}
+
+// prim_to_cons, physics.py:304-320 (double arithmetic for both precisions)
+template <typename R>
+__global__ void prim_to_cons_kernel(const Layout li, const R *W, const Layout lo, R *U, double gamma)
+{
+    const int64_t n = (int64_t)li.nxt * li.nyt;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k / li.nyt), j = (int)(k % li.nyt);
+        double w[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) w[v] = (double)W[v * li.var_stride + (int64_t)i * li.pitch + j];
+        double rho = np_max(w[0], FLOOR_RHO);
+        double u[NV];
+        u[RHO] = rho;
+        u[MX] = rho * w[1];
+        u[MY] = rho * w[2];
+        u[MZ] = rho * w[3];
+        u[BX] = w[4];
+        u[BY] = w[5];
+        u[BZ] = w[6];
+        u[PSI] = w[8];
+        u[RHOC] = rho * w[9];
+        double ke = 0.5 * rho * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+        double me = 0.5 * (w[4] * w[4] + w[5] * w[5] + w[6] * w[6]);
+        u[EN] = w[7] / (gamma - 1.0) + ke + me;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) U[v * lo.var_stride + (int64_t)i * lo.pitch + j] = (R)u[v];
+    }
+}
+
+// enforce_scalar_bounds, solver.py:199-204
+template <typename R>
+__global__ void scalar_bounds_kernel(const Layout l, R *U)
+{
+    const int64_t n = (int64_t)l.nxt * l.nyt;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = (k / l.nyt) * l.pitch + (k % l.nyt);
+        R rho = np_max(U[RHO * l.var_stride + c], R(FLOOR_RHO));
+        R cc = np_min(np_max(U[RHOC * l.var_stride + c] / rho, R(0)), R(1));
+        U[RHOC * l.var_stride + c] = rho * cc;
+    }
+}
+
+// muscl_x / muscl_y, physics.py:323-350 -> contiguous [10][nf]
+template <typename R>
+__global__ void muscl_kernel(const Layout l, const R *W, int axis, int limiter, R *WL, R *WR)
+{
+    const int nfx = axis == 0 ? l.nxt - 3 : l.nxt, nfy = axis == 0 ? l.nyt : l.nyt - 3;
+    const int64_t nf = (int64_t)nfx * nfy;
+    const int64_t step = axis == 0 ? l.pitch : 1;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nf; k += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k / nfy), j = (int)(k % nfy);
+        const int64_t c0 = (int64_t)i * l.pitch + j;
+        R wl[NV], wr[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const R *pv = W + v * l.var_stride + c0;
+            muscl_pair(pv[0], pv[step], pv[2 * step], pv[3 * step], limiter, wl[v], wr[v]);
+        }
+        wl[RHO] = np_max(wl[RHO], R(FLOOR_RHO));
+        wr[RHO] = np_max(wr[RHO], R(FLOOR_RHO));
+        wl[IPR] = np_max(wl[IPR], R(FLOOR_PR));
+        wr[IPR] = np_max(wr[IPR], R(FLOOR_PR));
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            WL[v * nf + k] = wl[v];
+            WR[v * nf + k] = wr[v];
+        }
+    }
+}
+
+// hlld_flux_x / hlld_flux_y, physics.py:353-379
+template <typename R>
+__global__ void hlld_kernel(const R *WL, const R *WR, R *F, R *smax, int64_t n, int axis, R gamma, R ch)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        R wl[NV], wr[NV], f[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            wl[v] = WL[v * n + k];
+            wr[v] = WR[v * n + k];
+        }
+        if (axis == 1) {
+            rot_xy(wl);
+            rot_xy(wr);
+        }
+        R s = hlld_flux(wl, wr, gamma, ch, f);
+        if (axis == 1) rot_xy(f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) F[v * n + k] = f[v];
+        if (smax) smax[k] = s;
+    }
+}
+
+// _compute_powell_source, solver.py:242-266 from primitive W
+template <typename R>
+__global__ void powell_kernel(const Layout l, const R *W, R *S, R dx, R dy)
+{
+    const int64_t n = (int64_t)l.nxt * l.nyt;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k / l.nyt), j = (int)(k % l.nyt);
+        const int64_t c = (int64_t)i * l.pitch + j;
+        R s[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) s[v] = R(0);
+        if (i >= 1 && i < l.nxt - 1 && j >= 1 && j < l.nyt - 1) {
+            const R *bx = W + BX * l.var_stride, *by = W + BY * l.var_stride;
+            R divb = (R(0.5) * (bx[c] + bx[c + l.pitch]) - R(0.5) * (bx[c - l.pitch] + bx[c])) / dx +
+                     (R(0.5) * (by[c] + by[c + 1]) - R(0.5) * (by[c - 1] + by[c])) / dy;
+            R vx = W[IVX * l.var_stride + c], vy = W[IVY * l.var_stride + c], vz = W[IVZ * l.var_stride + c];
+            R b0 = bx[c], b1 = by[c], b2 = W[BZ * l.var_stride + c];
+            R vb = vx * b0 + vy * b1 + vz * b2;
+            s[MX] = -divb * b0;
+            s[MY] = -divb * b1;
+            s[MZ] = -divb * b2;
+            s[BX] = -divb * vx;
+            s[BY] = -divb * vy;
+            s[BZ] = -divb * vz;
+            s[EN] = -divb * vb;
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) S[v * l.var_stride + c] = s[v];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CFL reduction over all cells (compute_dt, solver.py:206-223) into ctl->red.
+// from_prim: W (primitive) instead of U (conserved).
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void dt_reduce_kernel(const Layout l, const R *A, int from_prim, double gamma, amhd_control *ctl)
+{
+    const int64_t n = (int64_t)l.nxt * l.nyt;
+    unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = (k / l.nyt) * l.pitch + (k % l.nyt);
+        double qd[4];
+        if (from_prim) {
+            double w[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) w[v] = (double)A[v * l.var_stride + c];
+            cfl_quantities_prim(w, gamma, qd);
+        } else {
+            R u[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u[v] = A[v * l.var_stride + c];
+            cfl_quantities(u, gamma, qd);
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) q[m] = umax64(q[m], ord_bits(qd[m]));
+    }
+    __shared__ unsigned long long red[4][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int m = 0; m < 4; ++m)
+        for (int o = 16; o > 0; o >>= 1) q[m] = umax64(q[m], __shfl_xor_sync(0xffffffffu, q[m], o));
+    if (lane == 0)
+        for (int m = 0; m < 4; ++m) red[m][warp] = q[m];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int m = 0; m < 4; ++m) {
+            unsigned long long v = 0ull;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = umax64(v, red[m][w]);
+            atomicMax(reinterpret_cast<unsigned long long *>(&ctl->red[m]), v);
+        }
+    }
+}
+
+// _compute_boundary_energy_flux, solver.py:225-240: one block sums both columns
+template <typename R>
+__device__ double boundary_flux_block(const amhd_grid &g, const R *U)
+{
+    __shared__ double part[2][32];
+    const int nyt = g.ny + 2 * NG;
+    const int cols[2] = {NG, g.nx + NG - 1};
+    double acc[2] = {0.0, 0.0};
+    for (int s = 0; s < 2; ++s)
+        for (int j = NG + threadIdx.x; j < nyt - NG; j += blockDim.x) {
+            const int64_t c = (int64_t)cols[s] * g.pitch + j;
+            double u[NV], w[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u[v] = (double)U[v * g.var_stride + c];
+            cons_to_prim_cell(u, g.gamma, w);
+            double b2 = w[4] * w[4] + w[5] * w[5] + w[6] * w[6];
+            double pt = w[7] + 0.5 * b2;
+            double vb = w[1] * w[4] + w[2] * w[5] + w[3] * w[6];
+            acc[s] += ((u[EN] + pt) * w[1] - w[4] * vb) * g.dy;
+        }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int s = 0; s < 2; ++s) {
+        double a = acc[s];
+        for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) part[s][warp] = a;
+    }
+    __syncthreads();
+    double r = 0.0;
+    if (threadIdx.x == 0) {
+        double t0 = 0.0, t1 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            t0 += part[0][w];
+            t1 += part[1][w];
+        }
+        r = t0 - t1;
+    }
+    __syncthreads();
+    return r;  // valid in thread 0
+}
+
+template <typename R>
+__global__ void bflux_kernel(const amhd_grid g, const R *U, double *out)
+{
+    double r = boundary_flux_block(g, U);
+    if (threadIdx.x == 0) *out = r;
+}
+
+template <typename R>
+__global__ void bflux_accum_kernel(const amhd_grid g, const R *U, amhd_control *ctl, double dt)
+{
+    double r = boundary_flux_block(g, U);
+    if (threadIdx.x == 0) ctl->e_bnd += r * dt;
+}
+
+// ---------------------------------------------------------------------------
+// finalize: dt, ch and loop control from the reduced maxima.
+//   advance = 0: before the first step (run(), solver.py:476-479)
+//   advance = 1: after a step: t += dt, step += 1, then the next dt
+//   set_only = 1: compute_dt API -- only dt_cfl / ch (no loop state touched)
+// One block per instance (blockIdx.x), U / grid from the instance table.
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void finalize_kernel(const amhd_instance *insts, const amhd_instance one, const R *Ubase,
+                                amhd_control *ctls, int advance, int set_only)
+{
+    const amhd_instance &in = insts ? insts[blockIdx.x] : one;
+    const amhd_grid &g = in.grid;
+    amhd_control *ctl = ctls + blockIdx.x;
+    const R *U = Ubase ? Ubase + in.offset : nullptr;
+    __shared__ int go;
+    __shared__ double dt_next;
+    if (threadIdx.x == 0) {
+        go = 0;
+        if (set_only || ctl->active || !advance) {
+            if (advance && !set_only) {
+                ctl->t += ctl->dt;  // solver.py:481-482
+                ctl->last_dt = ctl->dt;
+                ctl->step += 1;
+            }
+            const bool loop_on = set_only || (ctl->t < ctl->t_end && ctl->step < ctl->max_steps);
+            if (loop_on) {
+                // compute_dt, solver.py:213-223 (max cf = sqrt of max cf^2; max(cf, ch) == ch)
+                double cf_max = sqrt(__longlong_as_double((long long)ctl->red[0]));
+                double vabs = __longlong_as_double((long long)ctl->red[1]);
+                double s = cf_max + vabs;
+                double ch = (1.0 > s ? 1.0 : s) * 1.5;
+                double sx = (__longlong_as_double((long long)ctl->red[2]) + ch) / g.dx;
+                double sy = (__longlong_as_double((long long)ctl->red[3]) + ch) / g.dy;
+                double smx = (sx != sx || sx >= sy) ? sx : sy;
+                double dtc = (smx < 1e-14) ? g.cfl * (g.dx < g.dy ? g.dx : g.dy) : g.cfl / smx;
+                ctl->ch = ch;
+                ctl->dt_cfl = dtc;
+                if (!set_only) {
+                    double rem = ctl->t_end - ctl->t;
+                    double dt = (rem < dtc) ? rem : dtc;  // solver.py:478
+                    ctl->dt = dt;
+                    if (dt <= 1e-16) {
+                        ctl->active = 0;
+                        ctl->flags |= AMHD_FLAG_DT_TINY;
+                    } else {
+                        ctl->active = 1;
+                        // snapshot due after this step (solver.py:487-490): pause, the host resumes
+                        if (advance && fabs(ctl->t - ctl->snap_t) < 1.5 * ctl->last_dt) {
+                            ctl->active = 0;
+                            ctl->flags |= AMHD_FLAG_PAUSED;
+                        }
+                        double m = g.dx < g.dy ? g.dx : g.dy;
+                        ctl->decay = ch > 0 ? exp(-g.glm_alpha * ch * dt / m) : 1.0;
+                        go = (g.bc_x != AMHD_BC_PERIODIC) && (U != nullptr);
+                        dt_next = dt;
+                    }
+                }
+            } else {
+                ctl->active = 0;
+            }
+            for (int k = 0; k < 4; ++k) ctl->red[k] = 0ull;
+        }
+    }
+    __syncthreads();
+    if (go) {
+        double bf = boundary_flux_block(g, U);  // solver.py:316-317
+        if (threadIdx.x == 0) ctl->e_bnd += bf * dt_next;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// diagnostics (solver.py:335-444, conserved-quantity part) in float64
+//   row pass: per interior x-row i, sum_j clip(C), sum_j rho, sum_j E,
+//   sum_j rho w^2 and row maxima of |divB| and stagnation pressure; sum divB^2
+// ---------------------------------------------------------------------------
+template <typename R>
+__global__ void diag_rows_kernel(const amhd_grid g, const R *U, double *rows)
+{
+    // one block per interior row
+    const int r = blockIdx.x;
+    const int i = NG + r;
+    double s_c = 0, s_rho = 0, s_e = 0, s_div2 = 0, s_ens = 0, m_div = 0, m_stag = 0;
+    const int nx = g.nx, ny = g.ny;
+    for (int jj = threadIdx.x; jj < ny; jj += blockDim.x) {
+        const int j = NG + jj;
+        auto load = [&](int ii, int jx, double w[NV]) {
+            double u[NV];
+            const int64_t c = (int64_t)ii * g.pitch + jx;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u[v] = (double)U[v * g.var_stride + c];
+            cons_to_prim_cell(u, g.gamma, w);
+        };
+        double w[NV];
+        load(i, j, w);
+        double cc = fmin(fmax(w[9], 0.0), 1.0);
+        s_c += cc;
+        s_rho += (double)U[RHO * g.var_stride + (int64_t)i * g.pitch + j];
+        s_e += (double)U[EN * g.var_stride + (int64_t)i * g.pitch + j];
+        double v2 = w[1] * w[1] + w[2] * w[2];
+        double b2 = w[4] * w[4] + w[5] * w[5] + w[6] * w[6];
+        m_stag = fmax(m_stag, w[7] + 0.5 * w[0] * v2 + 0.5 * b2);
+        // divB on the interior minus its outer ring (solver.py:419-426)
+        if (r >= 1 && r < nx - 1 && jj >= 1 && jj < ny - 1) {
+            double wxp[NV], wxm[NV], wyp[NV], wym[NV];
+            load(i + 1, j, wxp);
+            load(i - 1, j, wxm);
+            load(i, j + 1, wyp);
+            load(i, j - 1, wym);
+            double d = (0.5 * (w[4] + wxp[4]) - 0.5 * (wxm[4] + w[4])) / g.dx +
+                       (0.5 * (w[5] + wyp[5]) - 0.5 * (wym[5] + w[5])) / g.dy;
+            s_div2 += d * d;
+            m_div = fmax(m_div, fabs(d));
+        }
+        // vorticity with numpy.gradient's one-sided ends on the interior (solver.py:399-402)
+        {
+            double vyp, vym, hx, vxp, vxm, hy;
+            double t[NV];
+            if (r == 0) { load(i + 1, j, t); vyp = t[2]; vym = w[2]; hx = g.dx; }
+            else if (r == nx - 1) { load(i - 1, j, t); vyp = w[2]; vym = t[2]; hx = g.dx; }
+            else { load(i + 1, j, t); vyp = t[2]; load(i - 1, j, t); vym = t[2]; hx = 2 * g.dx; }
+            if (jj == 0) { load(i, j + 1, t); vxp = t[1]; vxm = w[1]; hy = g.dy; }
+            else if (jj == ny - 1) { load(i, j - 1, t); vxp = w[1]; vxm = t[1]; hy = g.dy; }
+            else { load(i, j + 1, t); vxp = t[1]; load(i, j - 1, t); vxm = t[1]; hy = 2 * g.dy; }
+            double om = (vyp - vym) / hx - (vxp - vxm) / hy;
+            s_ens += w[0] * om * om;
+        }
+    }
+    __shared__ double red[7][32];
+    double vals[7] = {s_c, s_rho, s_e, s_div2, s_ens, m_div, m_stag};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = 0; k < 7; ++k) {
+        double a = vals[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            double b = __shfl_xor_sync(0xffffffffu, a, o);
+            a = k < 5 ? a + b : fmax(a, b);
+        }
+        if (lane == 0) red[k][warp] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double out[7];
+        for (int k = 0; k < 7; ++k) {
+            double a = red[k][0];
+            for (int w2 = 1; w2 < (int)(blockDim.x >> 5); ++w2) a = k < 5 ? a + red[k][w2] : fmax(a, red[k][w2]);
+            out[k] = a;
+        }
+        for (int k = 0; k < 7; ++k) rows[(int64_t)k * nx + r] = out[k];
+    }
+}
+
+// finish: trapezoid mixing width and global sums, single block
+__global__ void diag_finish_kernel(const amhd_grid g, double x0, const double *rows, double *out);
+
+}  // namespace amhd

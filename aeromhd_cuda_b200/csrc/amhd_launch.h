@@ -1,0 +1,60 @@
+// amhd_launch.h -- host-side launch interface between the C ABI (amhd_capi.cu)
+// and the per-precision kernel translation units (amhd_f64.cu, amhd_f32.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "aeromhd.h"
+
+namespace amhd {
+
+// arguments of one fused RK stage launch over a list of (instance, tile)
+struct StageParams {
+    const void *uin;               // stage input state (stencil source)
+    const void *u0;                // step base state U0
+    void *uout;                    // stage output (may alias u0 on stage 3)
+    const amhd_instance *inst;     // device instance table, or nullptr: use `one`
+    amhd_instance one;             // the single instance when inst == nullptr
+    const int32_t *tile_inst;      // device: instance of each tile (with inst)
+    int32_t n_tiles;
+    amhd_control *ctl;             // per-instance controls (device) or nullptr
+    double dt, ch, decay;          // host scalars when !use_ctl
+    int32_t use_ctl;               // take dt / ch / decay / active from ctl
+    int32_t fuse_dt;               // stage 3: accumulate the CFL reduction
+};
+
+struct Layout {
+    int32_t nxt, nyt, pitch;
+    int64_t var_stride;
+};
+
+template <typename R>
+struct Launch {
+    static cudaError_t stage(int stage, int tile_x, const StageParams &p, int grid, cudaStream_t s);
+    static size_t stage_smem(int tile_x);
+    static cudaError_t configure();
+    static int stage_ctas_per_sm(int tile_x);
+    static cudaError_t bc_fill(const amhd_grid &g, R *U, cudaStream_t s);
+    static cudaError_t cons_to_prim(const Layout &li, const R *U, const Layout &lo, R *W, double gamma,
+                                    cudaStream_t s);
+    static cudaError_t prim_to_cons(const Layout &li, const R *W, const Layout &lo, R *U, double gamma,
+                                    cudaStream_t s);
+    static cudaError_t scalar_bounds(const Layout &l, R *U, cudaStream_t s);
+    static cudaError_t muscl(const Layout &l, const R *W, int axis, int limiter, R *WL, R *WR, cudaStream_t s);
+    static cudaError_t hlld(const R *WL, const R *WR, R *F, R *smax, int64_t n, int axis, double gamma, double ch,
+                            cudaStream_t s);
+    static cudaError_t powell(const Layout &l, const R *W, R *S, double dx, double dy, cudaStream_t s);
+    static cudaError_t dt_reduce(const Layout &l, const R *A, int from_prim, double gamma, amhd_control *ctl,
+                                 cudaStream_t s);
+    static cudaError_t finalize(const amhd_instance *insts, int n_inst, const amhd_instance &one, const R *U,
+                                amhd_control *ctl, int advance, int set_only, cudaStream_t s);
+    static cudaError_t diag_rows(const amhd_grid &g, const R *U, double *rows, cudaStream_t s);
+    static cudaError_t bflux(const amhd_grid &g, const R *U, double *out, cudaStream_t s);
+    static cudaError_t bflux_accum(const amhd_grid &g, const R *U, amhd_control *ctl, double dt, cudaStream_t s);
+};
+
+cudaError_t launch_control_resume(amhd_control *ctl, int n, double snap_t, cudaStream_t s);
+cudaError_t launch_diag_finish(const amhd_grid &g, double x0, const double *rows, double *out, cudaStream_t s);
+int device_sm_count();
+
+}  // namespace amhd

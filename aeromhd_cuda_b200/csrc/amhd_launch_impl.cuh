@@ -1,0 +1,212 @@
+// amhd_launch_impl.cuh -- definitions of Launch<R>; included once per
+// precision translation unit, which then instantiates Launch<R>.
+#pragma once
+#include "amhd_kernels.cuh"
+
+namespace amhd {
+
+static inline int elem_blocks(int64_t n, int threads = 256)
+{
+    int64_t b = (n + threads - 1) / threads;
+    const int64_t cap = 148LL * 16;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+template <typename R>
+size_t Launch<R>::stage_smem(int tile_x)
+{
+    switch (tile_x) {
+    case 4: return sizeof(TileSmem<R, 4>);
+    case 8: return sizeof(TileSmem<R, 8>);
+    case 16: return sizeof(TileSmem<R, 16>);
+    default: return 0;
+    }
+}
+
+// shared-memory opt-in of one stage instantiation, set once per process
+template <typename R, int TX, int ST>
+struct StageConfigured {
+    static bool done;
+};
+template <typename R, int TX, int ST>
+bool StageConfigured<R, TX, ST>::done = false;
+
+template <typename R, int TX, int ST>
+static cudaError_t configure_t()
+{
+    if (StageConfigured<R, TX, ST>::done) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(rk_stage_kernel<R, TX, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(TileSmem<R, TX>));
+    if (e == cudaSuccess) StageConfigured<R, TX, ST>::done = true;
+    return e;
+}
+
+template <typename R, int TX, int ST>
+static cudaError_t launch_stage_t(const StageParams &p, int grid, cudaStream_t s)
+{
+    cudaError_t e = configure_t<R, TX, ST>();
+    if (e != cudaSuccess) return e;
+    rk_stage_kernel<R, TX, ST><<<grid, TX * TY, sizeof(TileSmem<R, TX>), s>>>(p);
+    return cudaGetLastError();
+}
+
+template <typename R, int TX>
+static cudaError_t configure_tx()
+{
+    cudaError_t e;
+    if ((e = configure_t<R, TX, 0>()) != cudaSuccess) return e;
+    if ((e = configure_t<R, TX, 1>()) != cudaSuccess) return e;
+    if ((e = configure_t<R, TX, 2>()) != cudaSuccess) return e;
+    return configure_t<R, TX, 3>();
+}
+
+template <typename R>
+cudaError_t Launch<R>::configure()
+{
+    cudaError_t e;
+    if ((e = configure_tx<R, 4>()) != cudaSuccess) return e;
+    if ((e = configure_tx<R, 8>()) != cudaSuccess) return e;
+    return configure_tx<R, 16>();
+}
+
+template <typename R, int TX>
+static cudaError_t launch_stage_tx(int stage, const StageParams &p, int grid, cudaStream_t s)
+{
+    switch (stage) {
+    case 0: return launch_stage_t<R, TX, 0>(p, grid, s);
+    case 1: return launch_stage_t<R, TX, 1>(p, grid, s);
+    case 2: return launch_stage_t<R, TX, 2>(p, grid, s);
+    case 3: return launch_stage_t<R, TX, 3>(p, grid, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename R>
+cudaError_t Launch<R>::stage(int stage, int tile_x, const StageParams &p, int grid, cudaStream_t s)
+{
+    if (grid <= 0) grid = p.n_tiles;
+    if (p.n_tiles <= 0) return cudaSuccess;
+    switch (tile_x) {
+    case 4: return launch_stage_tx<R, 4>(stage, p, grid, s);
+    case 8: return launch_stage_tx<R, 8>(stage, p, grid, s);
+    case 16: return launch_stage_tx<R, 16>(stage, p, grid, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <typename R, int TX>
+static int ctas_per_sm_t()
+{
+    int n = 0;
+    const size_t smem = sizeof(TileSmem<R, TX>);
+    configure_t<R, TX, 3>();
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, rk_stage_kernel<R, TX, 3>, TX * TY, smem) != cudaSuccess)
+        return 1;
+    return n > 0 ? n : 1;
+}
+
+template <typename R>
+int Launch<R>::stage_ctas_per_sm(int tile_x)
+{
+    switch (tile_x) {
+    case 4: return ctas_per_sm_t<R, 4>();
+    case 8: return ctas_per_sm_t<R, 8>();
+    case 16: return ctas_per_sm_t<R, 16>();
+    default: return 1;
+    }
+}
+
+template <typename R>
+cudaError_t Launch<R>::bc_fill(const amhd_grid &g, R *U, cudaStream_t s)
+{
+    const int64_t n = 4LL * (g.ny + 2 * NG) + 4LL * g.nx;
+    bc_fill_kernel<R><<<elem_blocks(n), 256, 0, s>>>(g, U);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::cons_to_prim(const Layout &li, const R *U, const Layout &lo, R *W, double gamma,
+                                    cudaStream_t s)
+{
+    cons_to_prim_kernel<R><<<elem_blocks((int64_t)li.nxt * li.nyt), 256, 0, s>>>(li, U, lo, W, gamma);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::prim_to_cons(const Layout &li, const R *W, const Layout &lo, R *U, double gamma,
+                                    cudaStream_t s)
+{
+    prim_to_cons_kernel<R><<<elem_blocks((int64_t)li.nxt * li.nyt), 256, 0, s>>>(li, W, lo, U, gamma);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::scalar_bounds(const Layout &l, R *U, cudaStream_t s)
+{
+    scalar_bounds_kernel<R><<<elem_blocks((int64_t)l.nxt * l.nyt), 256, 0, s>>>(l, U);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::muscl(const Layout &l, const R *W, int axis, int limiter, R *WL, R *WR, cudaStream_t s)
+{
+    const int64_t nf = axis == 0 ? (int64_t)(l.nxt - 3) * l.nyt : (int64_t)l.nxt * (l.nyt - 3);
+    muscl_kernel<R><<<elem_blocks(nf), 256, 0, s>>>(l, W, axis, limiter, WL, WR);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::hlld(const R *WL, const R *WR, R *F, R *smax, int64_t n, int axis, double gamma, double ch,
+                            cudaStream_t s)
+{
+    hlld_kernel<R><<<elem_blocks(n), 256, 0, s>>>(WL, WR, F, smax, n, axis, R(gamma), R(ch));
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::powell(const Layout &l, const R *W, R *S, double dx, double dy, cudaStream_t s)
+{
+    powell_kernel<R><<<elem_blocks((int64_t)l.nxt * l.nyt), 256, 0, s>>>(l, W, S, R(dx), R(dy));
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::dt_reduce(const Layout &l, const R *A, int from_prim, double gamma, amhd_control *ctl,
+                                 cudaStream_t s)
+{
+    dt_reduce_kernel<R><<<elem_blocks((int64_t)l.nxt * l.nyt), 256, 0, s>>>(l, A, from_prim, gamma, ctl);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::finalize(const amhd_instance *insts, int n_inst, const amhd_instance &one, const R *U,
+                                amhd_control *ctl, int advance, int set_only, cudaStream_t s)
+{
+    finalize_kernel<R><<<n_inst, 256, 0, s>>>(insts, one, U, ctl, advance, set_only);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::diag_rows(const amhd_grid &g, const R *U, double *rows, cudaStream_t s)
+{
+    diag_rows_kernel<R><<<g.nx, 256, 0, s>>>(g, U, rows);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::bflux(const amhd_grid &g, const R *U, double *out, cudaStream_t s)
+{
+    bflux_kernel<R><<<1, 256, 0, s>>>(g, U, out);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t Launch<R>::bflux_accum(const amhd_grid &g, const R *U, amhd_control *ctl, double dt, cudaStream_t s)
+{
+    bflux_accum_kernel<R><<<1, 256, 0, s>>>(g, U, ctl, dt);
+    return cudaGetLastError();
+}
+
+}  // namespace amhd

@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Zone-updates/s of the SSP-RK3 MHD step (MUSCL + HLLD x/y + GLM/Powell + CFL dt) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp32|fp64] [--n 2048]
+
+Workload: the Orszag-Tang vortex on an n x n periodic grid (default 2048^2,
+the largest single-GPU configuration of the Orszag-Tang / convergence
+benchmark), synthetic analytic initial data.  A step is one full SSP-RK3
+step of the device-resident run loop: three fused stage launches (the last
+one also reducing the CFL condition of the new state) and one finalize
+launch that sets t, dt and the GLM speed for the next step.  The three
+state buffers (3 x 168 MB in fp32) exceed the 126 MB L2, so every step
+streams from HBM.
+
+N > 1 (torchrun, one process per GPU): every rank advances its own replica
+(weak scaling; the solver has no data-path collective), times are the max
+over ranks, value = zone-updates of all ranks / that time.
+
+``--impl reference`` times the reference scheme on the host cores (the
+float64 CPU restatement under oracle/, all OpenMP threads) on the same
+workload and prints the same JSON line with "impl": "reference".
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "zone-updates/s on 1 B200 (FP32 vs FP64; learned vs plain) at fixed L1 error"
+UNIT = "zone-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args(argv)
+
+
+def ot_config(n, precision):
+    from aeromhd_cuda_b200.config import Config
+    return Config(nx=n, ny=n, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, t_end=1e30, max_steps=1 << 60, cfl=0.4,
+                  gamma=5.0 / 3.0, powell_source=False, bc_x_type="periodic", bc_y_type="periodic",
+                  precision=precision)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic():
+    """dram bytes per stage-kernel step from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "rk_stage_kernel_traffic.txt")
+    try:
+        vals = {}
+        for line in open(path):
+            if ":" in line and not line.startswith("#"):
+                k, v = line.split(":", 1)
+                vals[k.strip()] = v.strip()
+        return vals
+    except OSError:
+        return {}
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """NVML clock / throttle-reason sampling during the timed region (read only)."""
+
+    def __init__(self, device_index: int, period_s: float = 0.2):
+        self.samples = []
+        self.period = period_s
+        self._stop = threading.Event()
+        self._th = None
+        self.ok = False
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+            self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid.encode() if isinstance(uuid, str) else uuid)
+            self.nv = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception as e:  # NVML missing: report no clocks rather than guess
+            self.err = repr(e)
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                util = nv.nvmlDeviceGetUtilizationRates(self.h).gpu
+                self.samples.append((mhz, reasons, util))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self._th = threading.Thread(target=self._run, daemon=True)
+            self._th.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._th:
+            self._th.join(timeout=2)
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": getattr(self, "max_mhz", None), "reasons": [],
+                    "note": getattr(self, "err", "no samples")}
+        nv = self.nv
+        names = {
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "hw_power_brake_slowdown": getattr(nv, "nvmlClocksEventReasonHwPowerBrakeSlowdown", 0x80),
+        }
+        loaded = [s for s in self.samples if s[2] >= 50] or self.samples
+        seen = set()
+        for _, r, _ in loaded:
+            for k, bit in names.items():
+                if r & bit:
+                    seen.add(k)
+        return {"sm_mhz": statistics.median(s[0] for s in loaded), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(seen), "samples": len(loaded)}
+
+
+# ------------------------------------------------------------ distributed
+def dist_setup(gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_oracle_rate(n, target_s=10.0, max_steps=None):
+    """Zone-updates/s of the float64 CPU restatement (all OpenMP threads) on OT n x n."""
+    import numpy as np
+    from oracle import oracle as O
+    from aeromhd_cuda_b200.config import Config
+    cfg = Config(nx=n, ny=n, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, t_end=1e30, max_steps=1 << 60, cfl=0.4,
+                 gamma=5.0 / 3.0, powell_source=False, bc_x_type="periodic", bc_y_type="periodic")
+    s = O.OracleSolver(cfg)
+    x, y = s.x[:, None], s.y[None, :]
+    g = cfg.gamma
+    W = np.zeros((10, s.nx_tot, s.ny_tot))
+    W[0] = g * g
+    W[1] = -np.sin(2 * np.pi * y)
+    W[2] = np.sin(2 * np.pi * x)
+    W[4] = -np.sin(2 * np.pi * y)
+    W[5] = np.sin(4 * np.pi * x)
+    W[7] = g
+    W[9] = (x < 0.5) + 0 * y
+    s.U = O.prim_to_cons(W, g)
+    t0 = time.perf_counter()
+    s.advance_native(max_steps=1)
+    one = time.perf_counter() - t0
+    steps = max(1, int(target_s / max(one, 1e-6)))
+    if max_steps:
+        steps = min(steps, max_steps)
+    t0 = time.perf_counter()
+    k = s.advance_native(max_steps=s.step + steps)
+    el = time.perf_counter() - t0
+    return n * n * k / el, k, el, O.max_threads()
+
+
+# ------------------------------------------------------------------- ours
+def run_ours(a, world, rank, local):
+    import numpy as np
+    import torch
+    from aeromhd_cuda_b200 import _lib, _tensors, initial_conditions as ic
+    from aeromhd_cuda_b200.solver import MHDSolver
+
+    n = a.n
+    cfg = ot_config(n, a.precision)
+    s = MHDSolver(cfg)
+    s.set_primitive(ic.orszag_tang(s))
+    es = 4 if a.precision == "fp32" else 8
+    cells = n * n
+    g = s._grid()
+    stream = _tensors.stream_ptr()
+    s._loop_init(cfg.t_end, cfg.max_steps)
+
+    ms = (ctypes.c_double * 5)()
+
+    def advance_profiled(k):
+        _lib.call("amhd_advance_profile", g, _tensors.ptr(s._U), _tensors.ptr(s._U1), _tensors.ptr(s._U2),
+                  _tensors.ptr(s._ctl), int(k), ms, stream)
+        return [ms[i] for i in range(5)]
+
+    if a.warmup > 0:
+        advance_profiled(a.warmup)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        prof = advance_profiled(a.steps)
+        torch.cuda.synchronize()
+    barrier(world)
+    total_ms = max_over_ranks(prof[4], world)
+    c = _tensors.read_controls(s._ctl)[0]
+    if c.flags & _lib.AMHD_FLAG_NONFINITE:
+        raise SystemExit("non-finite state during the benchmark")
+    value = world * cells * a.steps / (total_ms / 1e3)
+
+    # roofline of the fused stage kernel: 80 state values per zone-update per step
+    hbm, hbm_kind = peaks()
+    stage_ms = prof[0] + prof[1] + prof[2]
+    alg_bytes_step = 80 * es * cells
+    achieved = alg_bytes_step * a.steps / (stage_ms / 1e3) / 1e9
+    tr = profile_traffic()
+    traffic = None
+    if tr.get("precision") == a.precision and tr.get("n"):
+        try:
+            traffic = float(tr["dram_bytes_per_step"]) * (cells / float(tr["n"]) ** 2)
+        except (KeyError, ValueError):
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": hbm_kind,
+                "kernel": "rk_stage_kernel (3 launches/step)",
+                "algorithmic_bytes_per_step": alg_bytes_step,
+                "ms_per_step": {"stage1": prof[0] / a.steps, "stage2": prof[1] / a.steps,
+                                "stage3_fused_dt": prof[2] / a.steps, "finalize": prof[3] / a.steps}}
+
+    # ---- end to end: host state in pinned memory, one C-ABI call per step
+    e2e = None
+    if a.e2e_steps > 0:
+        host = torch.empty((10, n + 4, n + 4), dtype=s.dtype).pin_memory()
+        host.copy_(s.U.cpu())
+        out = (ctypes.c_double * 4)()
+        t_now = float(c.t)
+
+        def e2e_step(t):
+            _lib.call("amhd_step_host", g, host.data_ptr(), _tensors.ptr(s._U), _tensors.ptr(s._U1),
+                      _tensors.ptr(s._U2), _tensors.ptr(s._ctl), t, cfg.t_end, out, stream)
+            return out[0]
+
+        for _ in range(2):
+            t_now = e2e_step(t_now)
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(a.e2e_steps):
+            t_now = e2e_step(t_now)
+        ev1.record()
+        torch.cuda.synchronize()
+        e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+        state_bytes = 10 * (n + 4) * (n + 4) * es
+        ctl_bytes = ctypes.sizeof(_lib.Control)
+        e2e = {"value": world * cells * a.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": state_bytes + ctl_bytes, "d2h_bytes_per_step": state_bytes + ctl_bytes,
+               "ms_per_step": e2e_ms / a.e2e_steps,
+               "path": "amhd_step_host: pinned host state -> device, one run-loop step, -> host"}
+
+    # ---- float64 side by side (shorter run)
+    fp64 = None
+    if a.precision == "fp32" and not a.no_fp64:
+        s64 = MHDSolver(ot_config(n, "fp64"))
+        s64.set_primitive(ic.orszag_tang(s64))
+        s64._loop_init(1e30, 1 << 60)
+        g64 = s64._grid()
+        k64 = max(3, a.steps // 2)
+        _lib.call("amhd_advance_profile", g64, _tensors.ptr(s64._U), _tensors.ptr(s64._U1), _tensors.ptr(s64._U2),
+                  _tensors.ptr(s64._ctl), 2, ms, stream)
+        _lib.call("amhd_advance_profile", g64, _tensors.ptr(s64._U), _tensors.ptr(s64._U1), _tensors.ptr(s64._U2),
+                  _tensors.ptr(s64._ctl), k64, ms, stream)
+        t64 = max_over_ranks(ms[4], world)
+        fp64 = {"value": world * cells * k64 / (t64 / 1e3), "steps": k64,
+                "stage_hbm_frac": round(80 * 8 * cells * k64 / ((ms[0] + ms[1] + ms[2]) / 1e3) / 1e9 / hbm, 4)}
+        del s64
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        rate, k, el, cores = cpu_oracle_rate(512, target_s=10.0)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"float64 CPU restatement (oracle/), Orszag-Tang 512x512, {k} steps in {el:.1f} s"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": total_ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if a.precision == "fp32" else "f64", "data": "synthetic (analytic Orszag-Tang initial data)",
+        "config": {"workload": f"orszag_tang_{n}x{n}_{a.precision}", "nx": n, "ny": n, "precision": a.precision,
+                   "pressure_recovery": "f64", "dt_reduction": "f64",
+                   "l2": "inputs larger than L2 (3 state buffers of %.0f MB)" % (10 * (n + 4) * (n + 4) * es / 1e6),
+                   "parallelism": f"replicas x{world}", "tile": "8x32, one CTA per tile"},
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * a.steps,
+        "clocks": clk.summary(), "fp64": fp64,
+    }
+    return line
+
+
+def run_reference(a, world, rank):
+    """The reference scheme on host cores (float64 oracle port), same workload and metric."""
+    if rank != 0:
+        return None
+    n_full = a.n
+    # bounded sample: the largest of n, n/2, n/4 ... whose W+K steps fit in ~150 s
+    rate512, _, _, cores = cpu_oracle_rate(512, target_s=2.0, max_steps=3)
+    n = n_full
+    while n > 256 and (a.warmup + a.steps) * n * n / rate512 > 150.0:
+        n //= 2
+    rate, k, el, cores = cpu_oracle_rate(n, target_s=1e9, max_steps=a.warmup + a.steps)
+    sample = (f"float64 CPU restatement (oracle/), Orszag-Tang {n}x{n}" + ("" if n == n_full else
+              f" (bounded sample of the {n_full}x{n_full} workload)") + f", {k} steps in {el:.1f} s")
+    return {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": el / max(k, 1) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Orszag-Tang initial data)",
+        "config": {"workload": f"orszag_tang_{n_full}x{n_full}_{a.precision}", "nx": n_full, "ny": n_full,
+                   "precision": "fp64 (the reference computes in float64)"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main(argv=None):
+    a = parse_args(argv)
+    if a.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        line = run_reference(a, world, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+    world, rank, local = dist_setup(a.gpus)
+    try:
+        line = run_ours(a, world, rank, local)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

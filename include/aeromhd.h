@@ -1,0 +1,245 @@
+/*
+ * aeromhd.h -- C ABI of libaeromhd.so, the B200 (sm_100a) implementation of
+ * the AeroMHD-CUDA solver hot path: one SSP-RK3 step of 2-D ideal MHD
+ * (van Leer / minmod MUSCL, HLLD fluxes in x and y, GLM + Powell source,
+ * CFL dt), plus the batched-ensemble driver.
+ *
+ * Conventions
+ *   - Every entry point returns int: AMHD_OK (0) or a negative AMHD_ERR_*;
+ *     amhd_last_error() gives a message for the calling thread.
+ *   - All array pointers are DEVICE pointers owned by the caller unless the
+ *     name says _host.  The library never allocates device memory on a step.
+ *   - `stream` is a cudaStream_t passed as void*; calls are asynchronous on
+ *     it, except those that return host scalars (they synchronise it).
+ *   - A state array holds 10 planes (conserved slots rho, mx, my, mz, Bx, By,
+ *     Bz, E, psi, rho*C; reference config.py:13-16).  Element (v, i, j) with
+ *     i the x index and j the y index, ghosts included (i in [0, nx+4),
+ *     j in [0, ny+4)), lives at  base[v*var_stride + i*pitch + j].
+ *     The reference's contiguous U[10, nx+4, ny+4] (solver.py:83) is the case
+ *     pitch = ny+4, var_stride = (nx+4)*(ny+4).
+ *   - dtype AMHD_F64: double everywhere; AMHD_F32: float state and fluxes,
+ *     double pressure recovery, dt reduction and diagnostics.
+ *
+ * Each declaration cites the reference routine it replaces (file:line of the
+ * reference project).
+ */
+#ifndef AEROMHD_H
+#define AEROMHD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMHD_OK 0
+#define AMHD_ERR_ARG (-1)
+#define AMHD_ERR_CUDA (-2)
+#define AMHD_ERR_NONFINITE (-3)
+#define AMHD_ERR_TIMEOUT (-4)
+#define AMHD_ERR_UNSUPPORTED (-5)
+
+#define AMHD_F64 0
+#define AMHD_F32 1
+
+#define AMHD_BC_PERIODIC 0
+#define AMHD_BC_EXTRAPOLATION 1
+#define AMHD_BC_CHARACTERISTIC 2
+
+#define AMHD_LIMITER_VANLEER 0
+#define AMHD_LIMITER_MINMOD 1
+
+/* flags set in amhd_control.flags by the kernels */
+#define AMHD_FLAG_NONFINITE 1   /* a non-finite value was written by a step */
+#define AMHD_FLAG_DT_TINY 2     /* dt <= 1e-16 stopped the loop (solver.py:479) */
+#define AMHD_FLAG_PAUSED 4      /* loop paused at a snapshot time (amhd_control.snap_t) */
+
+/* Grid and physics parameters of one instance (reference Config,
+ * config.py:47-89, flattened; dx, dy precomputed as config.py:78-84 does). */
+typedef struct amhd_grid {
+    int32_t nx, ny;          /* interior cells                                  */
+    int32_t pitch;           /* elements between x-rows, >= ny + 4              */
+    int32_t dtype;           /* AMHD_F64 or AMHD_F32                            */
+    int64_t var_stride;      /* elements between planes, >= (nx + 4) * pitch    */
+    double dx, dy;
+    double gamma, cfl, glm_alpha;
+    int32_t bc_x, bc_y;      /* AMHD_BC_*; y knows periodic / extrapolation     */
+    int32_t powell;          /* 1: add the Powell source (solver.py:304-306)    */
+    int32_t limiter;         /* AMHD_LIMITER_*                                  */
+} amhd_grid;
+
+/* Per-instance time-stepping state kept in DEVICE memory, so that a loop of
+ * steps (and a CUDA graph of it) needs no host round trip.  Fields mirror the
+ * reference solver's attributes: t, dt, step (solver.py:84-86),
+ * cfg.glm_ch (solver.py:215), _glm_ch_frozen (:87),
+ * _cumulative_boundary_energy (:103).  Allocate sizeof(amhd_control) bytes of
+ * device memory per instance and initialise it with amhd_control_init. */
+typedef struct amhd_control {
+    double t;            /* simulation time                                    */
+    double t_end;        /* loop stops at t >= t_end                           */
+    double dt;           /* dt of the next step = min(dt_cfl, t_end - t)       */
+    double dt_cfl;       /* last CFL dt (solver.py:206-223)                    */
+    double ch;           /* cfg.glm_ch set by the last dt computation          */
+    double decay;        /* psi damping factor of the next step (:331-333)    */
+    double e_bnd;        /* cumulative boundary energy flux x dt (:316-317)   */
+    double last_dt;      /* dt of the last step taken                          */
+    int64_t step;        /* steps taken                                        */
+    int64_t max_steps;   /* loop stops at step >= max_steps                    */
+    int32_t active;      /* 1 while the loop should continue                   */
+    int32_t flags;       /* AMHD_FLAG_*                                        */
+    uint64_t red[4];     /* dt reduction accumulators (bit patterns of         */
+                         /* non-negative doubles): max cf^2, max(|vx|+|vy|),   */
+                         /* max |vx|, max |vy|                                 */
+    uint32_t tiles_done; /* completion counter of the fused dt reduction       */
+    uint32_t pad_;
+    double snap_t;       /* pause the loop after the step that brings t within */
+                         /* 1.5 dt of snap_t (run(), solver.py:487-490);       */
+                         /* +inf or NaN: never                                 */
+    double reserved[3];
+} amhd_control;
+
+/* ---- library ---------------------------------------------------------- */
+const char *amhd_version(void);
+const char *amhd_last_error(void);
+/* Configure every kernel of the library on the current device (shared
+ * memory limits); idempotent.  Call once before capturing a CUDA graph. */
+int amhd_init(void);
+/* element counts of the padded layout the fused step kernels require:
+ * pitch and rows per plane (multiples the kernels' tiles need). */
+int amhd_padded_layout(int32_t nx, int32_t ny, int32_t dtype, int32_t *pitch, int32_t *rows);
+size_t amhd_control_size(void);
+/* Tiling of the fused stage kernel for single-grid calls: tile_x (x rows per
+ * 32-column tile: 4, 8 or 16) and ctas_per_sm (0: one CTA per tile,
+ * otherwise a persistent grid of ctas_per_sm x SM-count CTAs).  Process-wide;
+ * chosen by the autotuner.  No counterpart in the reference. */
+int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm);
+/* shared memory per CTA and resident CTAs per SM of the stage kernel */
+int amhd_stage_info(int32_t dtype, int32_t tile_x, int32_t *smem_bytes, int32_t *ctas_per_sm, int32_t *sm_count);
+
+/* ---- physics.py ------------------------------------------------------- */
+/* cons_to_prim, physics.py:284-301 (all cells, ghosts included) */
+int amhd_cons_to_prim(const amhd_grid *g, const void *U, void *W, void *stream);
+/* prim_to_cons, physics.py:304-320 */
+int amhd_prim_to_cons(const amhd_grid *g, const void *W, void *U, void *stream);
+/* muscl_x / muscl_y, physics.py:323-350.  axis 0: WL, WR are contiguous
+ * [10][nx+1][ny+4]; axis 1: [10][nx+4][ny+1]. */
+int amhd_muscl(const amhd_grid *g, int32_t axis, const void *W, void *WL, void *WR, void *stream);
+/* hlld_flux_x / hlld_flux_y, physics.py:353-379 (kernel physics.py:43-276).
+ * axis 0: x faces; axis 1: y faces (components rotated as physics.py:376-379).
+ * WL, WR, F: contiguous [10][n_faces]; smax: [n_faces] per-face signal speed
+ * (may be NULL). */
+int amhd_hlld_flux(int32_t axis, int32_t dtype, const void *WL, const void *WR, void *F, void *smax, int64_t n_faces,
+                   double gamma, double ch, void *stream);
+
+/* ---- solver.py: MHDSolver -------------------------------------------- */
+/* apply_bc, solver.py:158-197 (in place) */
+int amhd_apply_bc(const amhd_grid *g, void *U, void *stream);
+/* enforce_scalar_bounds, solver.py:199-204 (in place, all cells) */
+int amhd_enforce_scalar_bounds(const amhd_grid *g, void *U, void *stream);
+/* compute_dt, solver.py:206-223, from primitive W (all cells, ghosts
+ * included).  Writes dt_cfl and ch (the new cfg.glm_ch) into *ctl and leaves
+ * the loop fields alone.  If dt_host / ch_host are not NULL the call
+ * synchronises and stores them. */
+int amhd_compute_dt(const amhd_grid *g, const void *W, amhd_control *ctl, double *dt_host, double *ch_host,
+                    void *stream);
+/* the same from conserved U (cons_to_prim fused in) */
+int amhd_compute_dt_cons(const amhd_grid *g, const void *U, amhd_control *ctl, double *dt_host, double *ch_host,
+                         void *stream);
+/* _compute_boundary_energy_flux, solver.py:225-240 (0 for periodic x).
+ * ctl is used as device scratch (its reserved[0] receives the flux, nothing
+ * else changes); synchronises. */
+int amhd_boundary_energy_flux(const amhd_grid *g, const void *U, amhd_control *ctl, double *out_host, void *stream);
+/* _compute_powell_source, solver.py:242-266: S from primitive W (same layout
+ * as W); zero on the outermost ring, as the reference. */
+int amhd_powell_source(const amhd_grid *g, const void *W, void *S, void *stream);
+/* compute_rhs, solver.py:268-308: fills U's ghosts in place, then R (same
+ * layout as U; zero outside the interior). */
+int amhd_compute_rhs(const amhd_grid *g, void *U, void *R, double ch, void *stream);
+/* step_ssprk3, solver.py:310-333, with the step's dt, frozen ch and psi
+ * damping factor given by the host.  U is advanced in place; U1, U2 are
+ * scratch states of the same layout.  Needs the padded layout
+ * (amhd_padded_layout).  If ctl is not NULL: ctl->e_bnd accumulates the
+ * boundary energy flux x dt (solver.py:316-317) and ctl->flags records a
+ * non-finite result. */
+int amhd_step_ssprk3(const amhd_grid *g, void *U, void *U1, void *U2, double dt, double ch, double decay,
+                     amhd_control *ctl, void *stream);
+/* one RK stage (1, 2 or 3) of step_ssprk3 (solver.py:319-329) on states that
+ * already hold their ghost cells: stage 1: Uout = U0 + dt L(U0); stage 2:
+ * Uout = 3/4 U0 + 1/4 (Uin + dt L(Uin)); stage 3: 1/3 U0 + 2/3 (Uin + dt
+ * L(Uin)), psi damped; each followed by the scalar clamp and the boundary
+ * conditions.  Padded layout. */
+int amhd_rk_stage(const amhd_grid *g, int32_t stage, const void *Uin, const void *U0, void *Uout, double dt,
+                  double ch, double decay, void *stream);
+/* Initialise *ctl (device) for a run from state U: t, t_end, step,
+ * max_steps; computes dt/ch from U exactly as run() does before its first
+ * step (solver.py:476-479).  Asynchronous. */
+int amhd_control_init(const amhd_grid *g, const void *U, amhd_control *ctl, double t, double t_end, int64_t step,
+                      int64_t max_steps, void *stream);
+/* Set the snapshot time at which the device loop pauses next (snap_t, +inf
+ * for none) for n controls, and resume those paused at the previous one.
+ * Asynchronous; no counterpart in the reference (its loop is on the host). */
+int amhd_control_resume(amhd_control *ctl, int32_t n, double snap_t, void *stream);
+/* The run loop (solver.py:475-482 / main.py:66-73) for n_steps iterations on
+ * the device: each iteration is one SSP-RK3 step with dt, ch and the psi
+ * damping taken from *ctl, the CFL reduction of the new state fused into the
+ * last stage, then t += dt, step += 1, boundary-energy bookkeeping and the
+ * next dt.  Iterations after the stop condition (t >= t_end, step >=
+ * max_steps, dt <= 1e-16) do nothing.  No host synchronisation; capturable
+ * in a CUDA graph. */
+int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps,
+                 void *stream);
+/* amhd_advance with a CUDA event recorded after every launch: ms_out[0..3]
+ * receive the summed device time of the stage-1, stage-2, stage-3 and
+ * finalize launches, ms_out[4] the whole interval.  Synchronises.  For
+ * profiling; no counterpart in the reference. */
+int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps,
+                         double *ms_out, void *stream);
+/* One iteration of the run loop (solver.py:476-482) on a HOST state: copies
+ * U_host (pinned or pageable, contiguous [10][nx+4][ny+4] of the grid's
+ * dtype) to the device, computes dt from it (CFL, capped at t_end - t),
+ * advances one SSP-RK3 step, and copies the new state back into U_host.
+ * out_host (may be NULL) receives {t + dt, dt, glm_ch, boundary energy
+ * flux x dt}.  dev_U/dev_U1/dev_U2 and ctl are caller device buffers (padded
+ * layout).  Returns AMHD_ERR_NONFINITE if the new state holds a NaN/Inf.
+ * Synchronises. */
+int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, void *dev_U2, amhd_control *ctl,
+                   double t, double t_end, double *out_host, void *stream);
+/* compute_diagnostics, solver.py:335-444 (the conserved-quantity part):
+ * out_dev receives (float64) [0] mass = sum(rho) dx dy, [1] energy = sum(E)
+ * dx dy (solver.py:430), [2] max|divB|, [3] sqrt(mean divB^2) (:419-428),
+ * [4] integral mixing width (:353-356), [5] peak stagnation pressure (:415-417),
+ * [6] global enstrophy mean(rho w^2) (:399-402).
+ * rows_dev: scratch of 4*nx doubles.  Asynchronous. */
+int amhd_diagnostics(const amhd_grid *g, const void *U, double x0, double *out_dev, double *rows_dev, void *stream);
+
+/* ---- batched ensemble -------------------------------------------------- */
+/* One entry per instance of the packed ensemble; offsets are element offsets
+ * of each instance's state in the three packed state buffers. */
+typedef struct amhd_instance {
+    amhd_grid grid;
+    int64_t offset;          /* element offset of plane 0, row 0, col 0          */
+    int32_t first_tile;      /* index of the instance's first tile in the list   */
+    int32_t tiles_x, tiles_y;/* tiles of this instance (tile_x rows x 32 cols)   */
+    int32_t pad_;
+} amhd_instance;
+
+/* Advance every active instance of a packed ensemble by n_steps run-loop
+ * steps: one persistent launch per RK stage over the (instance, tile) work
+ * list, per-instance dt/ch/t in ctl[n_inst].  U, U1, U2 are the packed
+ * buffers; inst and ctl are device arrays; tile_inst is the device work list
+ * (instance index of each tile); ctas is the persistent grid size (0: one
+ * per SM times occupancy).  Capturable in a CUDA graph. */
+int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev,
+                          int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U, void *U1, void *U2,
+                          amhd_control *ctl_dev, int32_t n_steps, int32_t ctas, void *stream);
+/* amhd_control_init for every instance of the ensemble (inst_host: a host
+ * copy of the instance table).  Asynchronous. */
+int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst_dev, int32_t n_inst,
+                       int32_t dtype, void *U, amhd_control *ctl_dev, double t_end, int64_t max_steps,
+                       void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AEROMHD_H */

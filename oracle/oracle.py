@@ -20,6 +20,7 @@ Arrays are numpy float64 ``[10, nx_tot, ny_tot]`` exactly as in the reference.
 from __future__ import annotations
 
 import ctypes
+import hashlib
 import os
 import subprocess
 
@@ -44,12 +45,22 @@ _I = ctypes.c_int
 _P = ctypes.c_void_p
 
 
+def _src_hash() -> str:
+    with open(SRC, "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()
+
+
 def build(force: bool = False) -> str:
-    """Compile liboracle.so with gcc (OpenMP, no FMA contraction)."""
-    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < os.path.getmtime(SRC):
+    """Compile liboracle.so with gcc (OpenMP, no FMA contraction); skipped when the
+    source hash recorded beside the library matches."""
+    stamp = LIB_PATH + ".srchash"
+    current = os.path.exists(LIB_PATH) and os.path.exists(stamp) and open(stamp).read().strip() == _src_hash()
+    if force or not current:
         cmd = ["gcc", "-O2", "-std=c11", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-fPIC",
                "-shared", "-o", LIB_PATH, SRC, "-lm"]
         subprocess.check_call(cmd)
+        with open(stamp, "w") as f:
+            f.write(_src_hash())
     return LIB_PATH
 
 

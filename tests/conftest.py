@@ -26,3 +26,18 @@ def oracle():
     O.build()
     O.lib()
     return O
+
+
+def pytest_collection_modifyitems(config, items):
+    """GPU tests need a CUDA device; on a machine without one they are skipped."""
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:  # pragma: no cover
+        has_gpu = False
+    if has_gpu:
+        return
+    skip = pytest.mark.skip(reason="no CUDA device")
+    for item in items:
+        if "gpu" in item.keywords:
+            item.add_marker(skip)

@@ -113,6 +113,8 @@ def _fake_cupy() -> types.ModuleType:
 def _fake_matplotlib():
     class _Anything:
         def __getattr__(self, name):
+            if name.startswith("__"):
+                raise AttributeError(name)
             return _Anything()
 
         def __call__(self, *a, **k):
@@ -125,7 +127,12 @@ def _fake_matplotlib():
     mpl.use = lambda *a, **k: None
     mpl.rcParams = {}
     plt = types.ModuleType("matplotlib.pyplot")
-    plt.__getattr__ = lambda name: _Anything()
+    def _plt_attr(name):
+        if name.startswith("__"):
+            raise AttributeError(name)
+        return _Anything()
+
+    plt.__getattr__ = _plt_attr
     lines = types.ModuleType("matplotlib.lines")
     lines.Line2D = _Anything
     mpl.pyplot = plt

@@ -1,0 +1,335 @@
+"""CUDA path (through the C ABI) against the reference's own outputs and the
+CPU oracle.  float64 mode: bit-exact (np.array_equal) wherever the oracle is;
+the device-resident loop computes the psi damping factor with the device's
+exp(), which may differ from numpy's by an ulp: there the bar is 1e-12
+relative.  float32 mode: relative L1 <= 1e-5 per conserved variable against
+the float64 oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+STEP_CASES = [(bx, by, B) for bx in ("periodic", "extrapolation", "characteristic")
+              for by in ("periodic", "outflow") for B in (0.0, 0.5)]
+
+
+@pytest.fixture(scope="module")
+def amhd():
+    from aeromhd_cuda_b200 import build
+    build.build()
+    import aeromhd_cuda_b200.physics as physics
+    import aeromhd_cuda_b200.solver as solver
+    from aeromhd_cuda_b200 import _lib, config
+    _lib.call("amhd_set_tiling", 8, 0)
+    return type("M", (), dict(physics=physics, solver=solver, lib=_lib, config=config))
+
+
+def C(**kw):
+    from aeromhd_cuda_b200.config import Config
+    return Config(**kw)
+
+
+def np_(t):
+    return t.detach().cpu().numpy()
+
+
+def rel_l1(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.sum(np.abs(a - b)) / max(np.sum(np.abs(b)), 1e-300))
+
+
+# ------------------------------------------------------------- physics.py
+def test_hlld_faces_bit_exact(amhd):
+    g = golden("hlld_faces.npz")
+    for k, ch in enumerate(g["chs"]):
+        F, smax = amhd.physics.hlld_flux_x(g["WL"], g["WR"], g["gamma"], ch, return_smax_array=True)
+        assert np.array_equal(np_(F), g[f"Fx_{k}"])
+        assert np.array_equal(np_(smax), g[f"smaxx_{k}"])
+        F, smax = amhd.physics.hlld_flux_y(g["WL"], g["WR"], g["gamma"], ch, return_smax_array=True)
+        assert np.array_equal(np_(F), g[f"Fy_{k}"])
+        assert np.array_equal(np_(smax), g[f"smaxy_{k}"])
+        F, mx = amhd.physics.hlld_flux_x(g["WL"], g["WR"], g["gamma"], ch)
+        assert mx == float(np.max(g[f"smaxx_{k}"]))
+
+
+def test_hlld_faces_fp32_close(amhd):
+    g = golden("hlld_faces.npz")
+    ok = np.ones(g["WL"].shape[1], bool)
+    ok[:24] = False  # the degenerate floor faces are ill-conditioned in float32 by construction
+    for k, ch in enumerate(g["chs"]):
+        F, _ = amhd.physics.hlld_flux_x(torch.tensor(g["WL"], dtype=torch.float32),
+                                        torch.tensor(g["WR"], dtype=torch.float32), g["gamma"], ch)
+        ref = g[f"Fx_{k}"][:, ok]
+        got = np_(F).astype(np.float64)[:, ok]
+        scale = np.maximum(np.abs(ref).max(axis=1, keepdims=True), 1e-30)
+        assert np.median(np.abs(got - ref) / scale) < 1e-6
+
+
+def test_conversions_and_muscl_bit_exact(amhd):
+    g = golden("conversions.npz")
+    P = amhd.physics
+    W = P.cons_to_prim(g["U"], g["gamma"])
+    assert np.array_equal(np_(W), g["W"])
+    assert np.array_equal(np_(P.prim_to_cons(g["W"], g["gamma"])), g["U2"])
+    WL, WR = P.muscl_x(g["W"])
+    assert np.array_equal(np_(WL), g["WLx"]) and np.array_equal(np_(WR), g["WRx"])
+    WL, WR = P.muscl_y(g["W"])
+    assert np.array_equal(np_(WL), g["WLy"]) and np.array_equal(np_(WR), g["WRy"])
+
+
+# ------------------------------------------------------------- solver.py
+def step_cfg(bcx, bcy, By, **kw):
+    return C(nx=10, ny=8, x_min=0.0, x_max=1.0, y_min=0.0, y_max=0.8, cfl=0.3, gamma=5.0 / 3.0, B_transverse=By,
+             powell_source=True, bc_x_type=bcx, bc_y_type=bcy, glm_alpha=1.5, **kw)
+
+
+@pytest.mark.parametrize("tile_x", [8, 4, 16])
+@pytest.mark.parametrize("k", range(len(STEP_CASES)))
+def test_three_steps_bit_exact(amhd, k, tile_x):
+    g = golden("steps.npz")
+    amhd.lib.call("amhd_set_tiling", tile_x, 0)
+    try:
+        cfg = step_cfg(*STEP_CASES[k])
+        s = amhd.solver.MHDSolver(cfg)
+        s.U = g[f"U0_{k}"]
+        for n in range(3):
+            W = amhd.physics.cons_to_prim(s.U, cfg.gamma)
+            s.dt = s.compute_dt(W)
+            assert s.dt == g[f"dt_{k}"][n]
+            assert cfg.glm_ch == g[f"ch_{k}"][n]
+            s.step_ssprk3()
+        assert np.array_equal(np_(s.U), g[f"U3_{k}"])
+        np.testing.assert_allclose(s._cumulative_boundary_energy, g[f"ebnd_{k}"], rtol=1e-12, atol=1e-15)
+    finally:
+        amhd.lib.call("amhd_set_tiling", 8, 0)
+
+
+def test_single_routines_bit_exact(amhd):
+    g = golden("steps.npz")
+    cfg = step_cfg("periodic", "outflow", 0.5)
+    cfg.glm_ch = 2.0
+    s = amhd.solver.MHDSolver(cfg)
+    s._glm_ch_frozen = 2.0
+    U = torch.tensor(g["rhs_U"], device="cuda")
+    R = s.compute_rhs(U)
+    assert np.array_equal(np_(U), g["rhs_Ubc"])
+    assert np.array_equal(np_(R), g["rhs_R"])
+    W = amhd.physics.cons_to_prim(U, cfg.gamma)
+    assert np.array_equal(np_(s._compute_powell_source(U, W)), g["rhs_S"])
+    Ub = torch.tensor(g["bounds_in"], device="cuda")
+    assert np.array_equal(np_(s.enforce_scalar_bounds(Ub)), g["bounds_out"])
+    U2 = torch.tensor(g["rhs_U"], device="cuda")
+    assert np.array_equal(np_(s.apply_bc(U2)), g["rhs_Ubc"])
+
+
+def brio_wu_cfg(nx, **kw):
+    return C(nx=nx, ny=4, x_min=0.0, x_max=1.0, y_min=0.0, y_max=0.05, t_end=0.1, cfl=0.30, gamma=2.0, mach=1.0,
+             B_transverse=0.0, interface_x=0.5, perturbation_amp=0.0, density_ratio=1.0, powell_source=False,
+             use_char_bc=False, bc_x_type="extrapolation", bc_y_type="periodic", **kw)
+
+
+def host_loop(amhd, s, t_end, max_steps):
+    """main.py:66-73 through the drop-in API."""
+    cfg = s.cfg
+    while s.t < t_end and s.step < max_steps:
+        W = amhd.physics.cons_to_prim(s.U, cfg.gamma)
+        s.dt = min(s.compute_dt(W), t_end - s.t)
+        if s.dt <= 1e-16:
+            break
+        s.step_ssprk3()
+        s.t += s.dt
+        s.step += 1
+
+
+def test_brio_wu_drop_in_loop_bit_exact(amhd):
+    g = golden("brio_wu.npz")
+    s = amhd.solver.MHDSolver(brio_wu_cfg(800))
+    s.U = np.repeat(g["U0_800"][:, :, None], s.ny_tot, axis=2)
+    host_loop(amhd, s, 0.1, 200000)
+    assert s.step == int(g["steps_800"]) and s.t == float(g["t_800"])
+    assert np.array_equal(np_(s.U[:, :, 2]), g["row_800"])
+
+
+def test_brio_wu_device_loop_and_reference_checks(amhd):
+    g = golden("brio_wu.npz")
+    s = amhd.solver.MHDSolver(brio_wu_cfg(800))
+    s.U = np.repeat(g["U0_800"][:, :, None], s.ny_tot, axis=2)
+    s.advance()
+    assert s.step == int(g["steps_800"]) and s.t == float(g["t_800"])
+    assert rel_l1(np_(s.U[:, 2:-2, 2]), g["row_800"][:, 2:-2]) < 1e-12
+    W = np_(amhd.physics.cons_to_prim(s.U, 2.0))
+    rho, By, vx = W[0, 2:-2, 2], W[5, 2:-2, 2], W[1, 2:-2, 2]
+    assert 0.1 < rho.min() < 0.18 and 0.9 < rho.max() < 1.05           # main.py:88-89, :93
+    assert len(np.unique(np.round(rho, 2))) > 10                       # :90-91
+    assert np.any(By[:-1] * By[1:] < 0) and vx.max() - vx.min() > 0.5  # :92, :94-95
+
+
+def test_alfven_convergence_device_loop(amhd):
+    g = golden("alfven.npz")
+    errs = []
+    for k, nx in enumerate(g["resolutions"]):
+        nx = int(nx)
+        cfg = C(nx=nx, ny=4, x_min=0.0, x_max=1.0, y_min=0.0, y_max=0.05, t_end=float(g["period"]), cfl=0.25,
+                gamma=5.0 / 3.0, B_transverse=0.0, powell_source=False, use_char_bc=False, bc_x_type="periodic",
+                bc_y_type="periodic")
+        s = amhd.solver.MHDSolver(cfg)
+        s.U = np.repeat(g[f"U0_{nx}"][:, :, None], s.ny_tot, axis=2)
+        W0 = np_(amhd.physics.cons_to_prim(s.U, cfg.gamma))
+        s.advance(max_steps=100000)
+        assert s.step == int(g["steps"][k])
+        assert rel_l1(np_(s.U[:, :, 2]), g[f"row_{nx}"]) < 1e-12
+        W = np_(amhd.physics.cons_to_prim(s.U, cfg.gamma))
+        errs.append(float(np.mean(np.abs(W[5, 2:-2, 2] - W0[5, 2:-2, 2]))))
+    np.testing.assert_allclose(errs, g["L1"], rtol=1e-6)
+    res = g["resolutions"]
+    orders = [np.log(errs[i - 1] / errs[i]) / np.log(res[i] / res[i - 1]) for i in range(1, len(errs))]
+    assert np.mean(orders) >= 1.9
+
+
+def test_contact_bit_exact(amhd):
+    g = golden("contact.npz")
+    cfg = C(nx=400, ny=4, x_min=0.0, x_max=1.0, y_min=0.0, y_max=0.01, t_end=0.2, cfl=0.30, gamma=5.0 / 3.0,
+            B_transverse=0.0, powell_source=False, use_char_bc=False, bc_x_type="extrapolation", bc_y_type="periodic")
+    s = amhd.solver.MHDSolver(cfg)
+    s.U = np.repeat(g["U0"][:, :, None], s.ny_tot, axis=2)
+    host_loop(amhd, s, 0.2, 200000)
+    assert s.step == int(g["steps"])
+    assert np.array_equal(np_(s.U[:, :, 2]), g["row"])
+
+
+def rmi_cfg(**kw):
+    return C(nx=48, ny=24, t_end=0.25, cfl=0.30, mach=10.0, B_transverse=0.5, powell_source=True, use_char_bc=True,
+             bc_x_type="characteristic", bc_y_type="periodic", **kw)
+
+
+def test_rmi_steps_and_diagnostics(amhd):
+    g = golden("rmi.npz")
+    s = amhd.solver.MHDSolver(rmi_cfg())
+    s.U = g["U_init"]
+    host_loop(amhd, s, 0.25, int(g["steps"]))
+    assert s.t == float(g["t"]) and s.cfg.glm_ch == float(g["ch"])
+    assert np.array_equal(np_(s.U), g["U_final"])
+    np.testing.assert_allclose(s._cumulative_boundary_energy, g["ebnd"], rtol=1e-11)
+    s.compute_diagnostics()
+    for name in ("mixing_width_integral", "mixing_width_thresh", "mixedness", "enstrophy", "enstrophy_local",
+                 "perturbation_amp", "stag_pressure", "divB_max", "divB_L2", "energy_total",
+                 "boundary_flux_cumulative"):
+        np.testing.assert_allclose(getattr(s, f"diag_{name}")[-1], g[f"diag_{name}"], rtol=1e-10, atol=1e-13,
+                                   err_msg=name)
+    np.testing.assert_allclose(s.diag_mode_amps[-1], g["diag_mode_amps"], rtol=1e-8, atol=1e-12)
+
+
+def test_rmi_initialize_matches_reference(amhd):
+    g = golden("rmi.npz")
+    s = amhd.solver.MHDSolver(rmi_cfg())
+    s.initialize()
+    assert s._rh_results["rho2"] == float(g["rh_rho2"]) and s._rh_results["p2"] == float(g["rh_p2"])
+    # sin / tanh of the device library vs numpy: ulp-level
+    assert rel_l1(np_(s.U), g["U_init"]) < 1e-14
+
+
+def test_orszag_tang_bit_exact(amhd):
+    g = golden("orszag_tang.npz")
+    cfg = C(nx=32, ny=32, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, t_end=0.5, cfl=0.4, gamma=5.0 / 3.0,
+            powell_source=False, bc_x_type="periodic", bc_y_type="periodic")
+    s = amhd.solver.MHDSolver(cfg)
+    s.U = g["U0"]
+    host_loop(amhd, s, 0.5, int(g["steps"]))
+    assert s.t == float(g["t"])
+    assert np.array_equal(np_(s.U), g["U_final"])
+
+
+# ------------------------------------------------------- device loop
+def ot_cfg(n, **kw):
+    return C(nx=n, ny=n, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, t_end=0.5, cfl=0.4, gamma=5.0 / 3.0,
+             powell_source=False, bc_x_type="periodic", bc_y_type="periodic", **kw)
+
+
+def test_device_loop_matches_host_loop(amhd):
+    from aeromhd_cuda_b200 import initial_conditions as ic
+    a = amhd.solver.MHDSolver(ot_cfg(64))
+    b = amhd.solver.MHDSolver(ot_cfg(64))
+    a.set_primitive(ic.orszag_tang(a))
+    b.U = a.U.clone()
+    host_loop(amhd, a, 0.5, 40)
+    b.advance(max_steps=40, chunk=16)
+    assert a.step == b.step == 40
+    assert abs(a.t - b.t) <= 1e-15
+    assert rel_l1(np_(b.U), np_(a.U)) < 1e-12
+
+
+def test_graph_replay_equals_eager(amhd):
+    from aeromhd_cuda_b200 import initial_conditions as ic
+    a = amhd.solver.MHDSolver(ot_cfg(96, precision="fp32"))
+    b = amhd.solver.MHDSolver(ot_cfg(96, precision="fp32"))
+    a.set_primitive(ic.orszag_tang(a))
+    b.U = a.U.clone()
+    a.advance(max_steps=50, chunk=16, graph=True)
+    b.advance(max_steps=50, chunk=16, graph=False)
+    assert a.step == b.step == 50 and a.t == b.t
+    assert torch.equal(a.U, b.U)
+
+
+def test_fp32_vs_fp64_oracle(amhd):
+    """float32 state with float64 pressure recovery vs the float64 CPU oracle."""
+    from oracle import oracle as O
+    from aeromhd_cuda_b200 import initial_conditions as ic
+    n, steps = 128, 60
+    s = amhd.solver.MHDSolver(ot_cfg(n, precision="fp32"))
+    s.set_primitive(ic.orszag_tang(s))
+    o = O.OracleSolver(ot_cfg(n))
+    s64 = amhd.solver.MHDSolver(ot_cfg(n))
+    s64.set_primitive(ic.orszag_tang(s64))
+    o.U = np_(s64.U).copy()
+    o.advance(max_steps=steps)
+    s.advance(max_steps=steps)
+    assert s.step == o.step == steps
+    U32, U64 = np_(s.U)[:, 2:-2, 2:-2], o.U[:, 2:-2, 2:-2]
+    errs = {v: rel_l1(U32[v], U64[v]) for v in (0, 1, 2, 4, 5, 7)}
+    print("fp32 vs fp64 oracle rel L1:", errs)
+    assert max(errs.values()) < 1e-5, errs
+
+
+def test_step_host_entry_point_matches_device_loop(amhd):
+    from aeromhd_cuda_b200 import _tensors, initial_conditions as ic
+    s = amhd.solver.MHDSolver(ot_cfg(64))
+    s.set_primitive(ic.orszag_tang(s))
+    host = np.ascontiguousarray(np_(s.U))
+    ref = amhd.solver.MHDSolver(ot_cfg(64))
+    ref.U = s.U.clone()
+    ref.advance(max_steps=1)
+    out = (ctypes.c_double * 4)()
+    amhd.lib.call("amhd_step_host", s._grid(), host.ctypes.data, _tensors.ptr(s._U), _tensors.ptr(s._U1),
+                  _tensors.ptr(s._U2), _tensors.ptr(s._ctl), 0.0, 0.5, out, _tensors.stream_ptr())
+    assert out[0] == ref.t and out[1] == ref.dt
+    assert rel_l1(host[:, 2:-2, 2:-2], np_(ref.U)[:, 2:-2, 2:-2]) < 1e-13
+
+
+def test_nonfinite_state_is_reported_not_trapped(amhd):
+    """A NaN planted on the host is reported through the control flags; the context stays usable."""
+    from aeromhd_cuda_b200 import initial_conditions as ic
+    s = amhd.solver.MHDSolver(ot_cfg(32))
+    s.set_primitive(ic.orszag_tang(s))
+    U = s.U.clone()
+    U[7, 10, 10] = float("nan")
+    s.U = U
+    with pytest.raises(FloatingPointError):
+        s.advance(max_steps=5, chunk=5)
+    s2 = amhd.solver.MHDSolver(ot_cfg(32))
+    s2.set_primitive(ic.orszag_tang(s2))
+    s2.advance(max_steps=3)
+    assert s2.step == 3 and np.isfinite(np_(s2.U)).all()
+
+
+def test_device_argument_errors(amhd):
+    from aeromhd_cuda_b200 import _tensors
+    s = amhd.solver.MHDSolver(ot_cfg(32))
+    bad = torch.zeros(10 * 40 * 40 + 1, dtype=torch.float64, device="cuda")[1:]
+    with pytest.raises(amhd.lib.AmhdError):
+        amhd.lib.call("amhd_step_ssprk3", s._grid(), bad.data_ptr(), _tensors.ptr(s._U1), _tensors.ptr(s._U2), 0.1,
+                      1.0, 1.0, None, _tensors.stream_ptr())
