@@ -140,13 +140,14 @@ cudaError_t run_dt_reduce(const amhd_grid *g, const void *A, int from_prim, amhd
 // three fused stages of one step; dt/ch/decay from the host or from ctl
 int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instance *insts, const int32_t *tile_inst,
                  int n_tiles, int tile_x, int grid, void *U, void *U1, void *U2, amhd_control *ctl, int use_ctl,
-                 double dt, double ch, double decay, int fuse_dt, cudaStream_t s)
+                 double dt, double ch, double decay, int fuse_dt, cudaStream_t s, const int32_t *tile_order = nullptr)
 {
     StageParams p;
     memset(&p, 0, sizeof p);
     p.inst = insts;
     p.one = one;
     p.tile_inst = tile_inst;
+    p.tile_order = tile_order;
     p.n_tiles = n_tiles;
     p.ctl = ctl;
     p.dt = dt;
@@ -628,9 +629,9 @@ int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst
     return AMHD_OK;
 }
 
-int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev, int32_t n_tiles,
-                          int32_t dtype, int32_t tile_x, void *U, void *U1, void *U2, amhd_control *ctl_dev,
-                          int32_t n_steps, int32_t ctas, void *stream)
+int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev,
+                          const int32_t *tile_order_dev, int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U,
+                          void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas, void *stream)
 {
     if (!inst_dev || !tile_inst_dev || !U || !U1 || !U2 || !ctl_dev || n_inst <= 0 || n_tiles <= 0)
         return fail(AMHD_ERR_ARG, "bad ensemble arguments");
@@ -651,7 +652,7 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
     memset(&dummy, 0, sizeof dummy);
     for (int k = 0; k < n_steps; ++k) {
         if (int e = three_stages(&gdt, dummy, inst_dev, tile_inst_dev, n_tiles, tile_x, grid, U, U1, U2, ctl_dev, 1, 0,
-                                 0, 1, 1, s))
+                                 0, 1, 1, s, tile_order_dev))
             return e;
         CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 1, 0, s));
     }

@@ -17,7 +17,10 @@
 
 #include "aeromhd.h"
 #include "amhd_launch.h"
+#include "amhd_fast.cuh"
 #include "amhd_physics.cuh"
+
+#include <type_traits>
 
 namespace amhd {
 
@@ -37,9 +40,16 @@ struct Vec<double> {
     static constexpr int N = 2;
 };
 
+template <typename R>
+constexpr bool kFast = std::is_same<R, float>::value;  // float32: slope pre-pass + fast HLLD
+
 template <typename R, int TX>
 struct TileSmem {
     R w[NV][TX + 2 * NG][HW];      // primitives of the tile + halo
+    // limited slopes (float32 path only): x-slopes of halo rows 1..TX+2 over the
+    // tile's columns, y-slopes of the tile's rows over halo columns 1..TY+2
+    R sx[kFast<R> ? NV : 1][kFast<R> ? TX + 2 : 1][TY];
+    R sy[kFast<R> ? NV : 1][kFast<R> ? TX : 1][TY + 2];
     R fx[NV][TX + 1][TY];          // x-face fluxes (face a: between tile rows a-1 and a)
     R fy[NV][TX][TY + 1];          // y-face fluxes
     unsigned long long red[4][32]; // per-warp dt partials
@@ -106,52 +116,93 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
 #pragma unroll
         for (int k = 0; k < VN; ++k) {
             R w[NV];
-            cons_to_prim_cell(u[k], g.gamma, w);
+            if constexpr (kFast<R>)
+                fast::cons_to_prim(u[k], g.gamma, w);
+            else
+                cons_to_prim_cell(u[k], g.gamma, w);
 #pragma unroll
             for (int v = 0; v < NV; ++v) sm.w[v][r][c + k] = w[v];
         }
     }
     __syncthreads();
 
+    if constexpr (kFast<R>) {
+        // ---- phase A2 (float32): limited slopes, once per cell and direction
+        constexpr int NSX = (TX + 2) * TY, NSY = TX * (TY + 2);
+        for (int q = t; q < NSX + NSY; q += NT) {
+            if (q < NSX) {
+                const int r = q / TY + 1, c = q % TY + NG;
+#pragma unroll
+                for (int v = 0; v < NV; ++v)
+                    sm.sx[v][r - 1][c - NG] = fast::slope(sm.w[v][r - 1][c], sm.w[v][r][c], sm.w[v][r + 1][c],
+                                                          g.limiter);
+            } else {
+                const int h = q - NSX;
+                const int r = h / (TY + 2) + NG, k = h % (TY + 2) + 1;
+#pragma unroll
+                for (int v = 0; v < NV; ++v)
+                    sm.sy[v][r - NG][k - 1] = fast::slope(sm.w[v][r][k - 1], sm.w[v][r][k], sm.w[v][r][k + 1],
+                                                          g.limiter);
+            }
+        }
+        __syncthreads();
+    }
+
     // ---- phase B: MUSCL + HLLD on all faces of the tile -------------------
     const R gam = R(g.gamma), chr = R(ch);
     const int lim = g.limiter;
     constexpr int NFX = (TX + 1) * TY;
     constexpr int NFY = TX * (TY + 1);
+    // one HLLD call site for x and y faces (y faces in the rotated slot order
+    // rho, vy, vx, vz, By, Bx, Bz, p, psi, C of physics.py:376-379)
+    constexpr int rot[NV] = {0, 2, 1, 3, 5, 4, 6, 7, 8, 9};
+    const float igm1 = 1.0f / float(g.gamma - 1.0), half_ich = ch > 0.0 ? float(0.5 / ch) : 0.f;
     for (int f = t; f < NFX + NFY; f += NT) {
         R wl[NV], wr[NV], fl[NV];
-        if (f < NFX) {
-            const int a = f / TY, c = f % TY + NG;  // face between halo rows a+1, a+2
+        const bool xf = f < NFX;
+        const int h = xf ? f : f - NFX;
+        const int a = xf ? h / TY : h / (TY + 1);
+        const int c = xf ? h % TY : h % (TY + 1);
+        if constexpr (kFast<R>) {
+            if (xf) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v)
-                muscl_pair(sm.w[v][a][c], sm.w[v][a + 1][c], sm.w[v][a + 2][c], sm.w[v][a + 3][c], lim, wl[v],
-                           wr[v]);
+                for (int v = 0; v < NV; ++v) {
+                    wl[v] = sm.w[v][a + 1][c + NG] + 0.5f * sm.sx[v][a][c];
+                    wr[v] = sm.w[v][a + 2][c + NG] - 0.5f * sm.sx[v][a + 1][c];
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    wl[v] = sm.w[rot[v]][a + NG][c + 1] + 0.5f * sm.sy[rot[v]][a][c];
+                    wr[v] = sm.w[rot[v]][a + NG][c + 2] - 0.5f * sm.sy[rot[v]][a][c + 1];
+                }
+            }
+            fast::hlld(wl, wr, gam, igm1, chr, half_ich, fl);
         } else {
-            const int h = f - NFX;
-            const int a = h / (TY + 1) + NG, k = h % (TY + 1);  // face between halo cols k+1, k+2
+            if (xf) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v)
-                muscl_pair(sm.w[v][a][k], sm.w[v][a][k + 1], sm.w[v][a][k + 2], sm.w[v][a][k + 3], lim, wl[v],
-                           wr[v]);
-        }
-        wl[RHO] = np_max(wl[RHO], R(FLOOR_RHO));
-        wr[RHO] = np_max(wr[RHO], R(FLOOR_RHO));
-        wl[IPR] = np_max(wl[IPR], R(FLOOR_PR));
-        wr[IPR] = np_max(wr[IPR], R(FLOOR_PR));
-        if (f < NFX) {
+                for (int v = 0; v < NV; ++v)
+                    muscl_pair(sm.w[v][a][c + NG], sm.w[v][a + 1][c + NG], sm.w[v][a + 2][c + NG],
+                               sm.w[v][a + 3][c + NG], lim, wl[v], wr[v]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v)
+                    muscl_pair(sm.w[rot[v]][a + NG][c], sm.w[rot[v]][a + NG][c + 1], sm.w[rot[v]][a + NG][c + 2],
+                               sm.w[rot[v]][a + NG][c + 3], lim, wl[v], wr[v]);
+            }
+            // floors of physics.py:331-334 (slot 7 is p in both orders)
+            wl[RHO] = np_max(wl[RHO], R(FLOOR_RHO));
+            wr[RHO] = np_max(wr[RHO], R(FLOOR_RHO));
+            wl[IPR] = np_max(wl[IPR], R(FLOOR_PR));
+            wr[IPR] = np_max(wr[IPR], R(FLOOR_PR));
             hlld_flux(wl, wr, gam, chr, fl);
-            const int a = f / TY, c = f % TY;
+        }
+        if (xf) {
 #pragma unroll
             for (int v = 0; v < NV; ++v) sm.fx[v][a][c] = fl[v];
         } else {
-            rot_xy(wl);
-            rot_xy(wr);
-            hlld_flux(wl, wr, gam, chr, fl);
-            rot_xy(fl);
-            const int h = f - NFX;
-            const int a = h / (TY + 1), k = h % (TY + 1);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) sm.fy[v][a][k] = fl[v];
+            for (int v = 0; v < NV; ++v) sm.fy[rot[v]][a][c] = fl[v];
         }
     }
     __syncthreads();
@@ -166,12 +217,19 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
         const int64_t gi = (int64_t)i * pitch + j;
         R rhs[NV];
         const R dx = R(g.dx), dy = R(g.dy);
+        if constexpr (kFast<R>) {
+            const float idx = float(1.0 / g.dx), idy = float(1.0 / g.dy);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            R r0 = R(0);
-            r0 -= (sm.fx[v][a + 1][c] - sm.fx[v][a][c]) / dx;
-            r0 -= (sm.fy[v][a][c + 1] - sm.fy[v][a][c]) / dy;
-            rhs[v] = r0;
+            for (int v = 0; v < NV; ++v)
+                rhs[v] = -(sm.fx[v][a + 1][c] - sm.fx[v][a][c]) * idx - (sm.fy[v][a][c + 1] - sm.fy[v][a][c]) * idy;
+        } else {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                R r0 = R(0);
+                r0 -= (sm.fx[v][a + 1][c] - sm.fx[v][a][c]) / dx;
+                r0 -= (sm.fy[v][a][c + 1] - sm.fy[v][a][c]) / dy;
+                rhs[v] = r0;
+            }
         }
         if (g.powell) {
             // _compute_powell_source, solver.py:242-266 (centred face-average divB)
@@ -220,7 +278,10 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
                 if (ch > 0.0) out[PSI] *= R(decay);  // solver.py:331-333
                 if (p.fuse_dt) {
                     double qd[4];
-                    cfl_quantities(out, g.gamma, qd);
+                    if constexpr (kFast<R>)
+                        fast::cfl_quantities(out, g.gamma, qd);
+                    else
+                        cfl_quantities(out, g.gamma, qd);
 #pragma unroll
                     for (int k = 0; k < 4; ++k) q[k] = ord_bits(qd[k]);
                 }
@@ -272,12 +333,17 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
     }
 }
 
+// resident CTAs per SM the register budget is shaped for (float32 path)
+template <typename R, int TX>
+constexpr int kMinBlocks = kFast<R> ? (TX == 4 ? 6 : (TX == 8 ? 3 : 1)) : 1;
+
 template <typename R, int TX, int STAGE>
-__global__ void __launch_bounds__(TX * TY) rk_stage_kernel(const StageParams p)
+__global__ void __launch_bounds__(TX * TY, (kMinBlocks<R, TX>)) rk_stage_kernel(const StageParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     TileSmem<R, TX> &sm = *reinterpret_cast<TileSmem<R, TX> *>(smem_raw);
-    for (int tile = blockIdx.x; tile < p.n_tiles; tile += gridDim.x) {
+    for (int pos = blockIdx.x; pos < p.n_tiles; pos += gridDim.x) {
+        const int tile = p.tile_order ? p.tile_order[pos] : pos;
         rk_stage_tile<R, TX, STAGE>(p, sm, tile);
         __syncthreads();  // shared memory is reused by the next tile
     }

@@ -16,6 +16,7 @@ struct StageParams {
     const amhd_instance *inst;     // device instance table, or nullptr: use `one`
     amhd_instance one;             // the single instance when inst == nullptr
     const int32_t *tile_inst;      // device: instance of each tile (with inst)
+    const int32_t *tile_order;     // device: tile taken at each work position, or nullptr
     int32_t n_tiles;
     amhd_control *ctl;             // per-instance controls (device) or nullptr
     double dt, ch, decay;          // host scalars when !use_ctl

@@ -1,0 +1,254 @@
+"""Batched ensemble of independent shock-accelerated-interface runs on one GPU.
+
+Every instance keeps its own grid size, physics parameters and time step; all
+of them advance together, one persistent launch per SSP-RK3 stage over a work
+list of (instance, tile) pairs, plus one launch that finishes every
+instance's CFL reduction and clock.  A run of steps is captured once as a
+CUDA graph and replayed.  Instances that reach their end time stop (their
+tiles return at once) while the others continue.
+
+Layout: the three ensemble states are single device buffers; instance k
+occupies ``10 * rows_k * pitch_k`` elements at ``offset_k`` in each (its own
+padded layout, 16-byte aligned), described by an ``amhd_instance`` table in
+device memory.
+
+No counterpart in the reference, which runs one grid per ``MHDSolver``;
+instance i of an ensemble produces exactly the state the single-grid solver
+produces for it (the same kernels over the same tiles).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import replace
+from typing import List, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib, initial_conditions
+from ._tensors import NG, control_tensor, read_controls, stream_ptr, torch_dtype
+from .config import Config, bc_x_code, bc_y_code
+from .physics import prim_to_cons
+
+
+def draw_configs(n: int = 256, seed: int = 0, t_end: float = 3.0, precision: str = "fp32",
+                 ny_choices: Sequence[int] = (32, 64, 128, 256), noise_amp: float = 1e-3) -> List[Config]:
+    """Seeded parameter draws of the uneven shock-interface ensemble:
+    Ny in ny_choices, Nx = 4 Ny on [0,4]x[0,1]; Mach ~ U[2,5]; density ratio ~
+    U[1.5,5]; mode k in 1..8, amplitude ~ U[0.01,0.08]; B = (B0 + B1 sin(2 pi m y), 0, 0)
+    with B0, B1 ~ U[0,0.3], m in 1..6."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        ny = int(rng.choice(ny_choices))
+        out.append(Config(
+            nx=4 * ny, ny=ny, x_min=0.0, x_max=4.0, y_min=0.0, y_max=1.0, t_end=t_end, cfl=0.4, gamma=5.0 / 3.0,
+            mach=float(rng.uniform(2.0, 5.0)), density_ratio=float(rng.uniform(1.5, 5.0)),
+            perturbation_mode=int(rng.integers(1, 9)), perturbation_amp=float(rng.uniform(0.01, 0.08)),
+            bx0=float(rng.uniform(0.0, 0.3)), b1=float(rng.uniform(0.0, 0.3)), b_mode=int(rng.integers(1, 7)),
+            ic="shock_interface", interface_x=1.0, shock_x=0.5, perturbation_shape="cos", interface_cells=2.0,
+            noise_amp=noise_amp, seed=seed * 100003 + k, powell_mode="on", bc_x_type="extrapolation",
+            bc_y_type="periodic", precision=precision))
+    return out
+
+
+def pack_layout(configs: Sequence[Config], dtype_code: int):
+    """Element offset, pitch and rows of every instance in the packed buffers,
+    each start 16-byte aligned; returns (layouts, total elements)."""
+    es = 4 if dtype_code == _lib.AMHD_F32 else 8
+    align = 16 // es
+    layouts, off = [], 0
+    for c in configs:
+        pitch, rows = _lib.padded_layout(c.nx, c.ny, dtype_code)
+        layouts.append((off, pitch, rows))
+        off += 10 * rows * pitch
+        off = (off + align - 1) // align * align
+    return layouts, off
+
+
+def tile_counts(configs: Sequence[Config], tile_x: int) -> np.ndarray:
+    return np.array([((c.nx + tile_x - 1) // tile_x) * ((c.ny + 31) // 32) for c in configs], dtype=np.int64)
+
+
+def work_list(counts: Sequence[int], order: str = "instance"):
+    """(tile_order, tile_inst, first_tile) of a packed ensemble.
+
+    Tiles are numbered instance by instance (instance k owns ids first_tile[k] ..
+    first_tile[k] + counts[k] - 1, taken in that order); tile_inst maps an id to
+    its instance; tile_order is the id taken at each work position:
+      instance       instance by instance (neighbouring tiles share halo lines in L2)
+      largest_first  the instances with most tiles first
+      interleave     round robin over instances
+    """
+    counts = np.asarray(counts, dtype=np.int64)
+    first = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int64)
+    n_tiles = int(counts.sum())
+    tile_inst = np.repeat(np.arange(len(counts), dtype=np.int32), counts)
+    if order == "instance":
+        seq = [np.arange(first[k], first[k] + counts[k]) for k in range(len(counts))]
+        tile_order = np.concatenate(seq) if seq else np.zeros(0, np.int64)
+    elif order == "largest_first":
+        ks = np.argsort(-counts, kind="stable")
+        tile_order = np.concatenate([np.arange(first[k], first[k] + counts[k]) for k in ks])
+    elif order == "interleave":
+        m = int(counts.max())
+        grid = np.full((m, len(counts)), -1, dtype=np.int64)
+        for k in range(len(counts)):
+            grid[: counts[k], k] = np.arange(first[k], first[k] + counts[k])
+        flat = grid.reshape(-1)
+        tile_order = flat[flat >= 0]
+    else:
+        raise ValueError(f"unknown order {order!r}")
+    assert len(tile_order) == n_tiles
+    return tile_order.astype(np.int32), tile_inst, first.astype(np.int32)
+
+
+def shard(configs: Sequence[Config], world: int, rank: int) -> List[int]:
+    """Instances of this rank: longest-processing-time greedy over cell counts,
+    so that every GPU gets about the same number of zone updates per step."""
+    cells = np.array([c.nx * c.ny for c in configs])
+    load = np.zeros(world)
+    owner = np.empty(len(configs), dtype=np.int64)
+    for k in np.argsort(-cells, kind="stable"):
+        r = int(np.argmin(load))
+        owner[k] = r
+        load[r] += cells[k]
+    return [k for k in range(len(configs)) if owner[k] == rank]
+
+
+class _GridView:
+    """The coordinate attributes initial_conditions needs, for one instance."""
+
+    def __init__(self, cfg: Config, device):
+        self.cfg = cfg
+        self.nx_tot, self.ny_tot = cfg.nx + 2 * NG, cfg.ny + 2 * NG
+        self.device = device
+        self.x = torch.as_tensor(cfg.x_min + (np.arange(self.nx_tot) - NG + 0.5) * cfg.dx, device=device)
+        self.y = torch.as_tensor(cfg.y_min + (np.arange(self.ny_tot) - NG + 0.5) * cfg.dy, device=device)
+        self.X, self.Y = torch.meshgrid(self.x, self.y, indexing="ij")
+
+
+class Ensemble:
+    def __init__(self, configs: Sequence[Config], tile_x: int = 8, order: str = "instance", ctas: int = 0,
+                 device=None):
+        if not configs:
+            raise ValueError("empty ensemble")
+        precs = {c.precision for c in configs}
+        if len(precs) != 1:
+            raise ValueError("all instances must share one precision")
+        for c in configs:
+            c.validate()
+        _lib.call("amhd_init")
+        self.configs = [replace(c) for c in configs]
+        self.precision = precs.pop()
+        self.dtype = torch_dtype(self.precision)
+        self.code = _lib.AMHD_F64 if self.dtype == torch.float64 else _lib.AMHD_F32
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.n = len(self.configs)
+        self.tile_x = int(tile_x)
+        self.ctas = int(ctas)
+        self.layouts, off = pack_layout(self.configs, self.code)
+        self.total = off
+        self.U = torch.zeros(off, dtype=self.dtype, device=self.device)
+        self.U1 = torch.zeros_like(self.U)
+        self.U2 = torch.zeros_like(self.U)
+        self.ctl = control_tensor(self.n, self.device)
+        self._graphs = {}
+        self.set_schedule(tile_x, order, ctas)
+
+    # -------------------------------------------------------- schedule
+    def set_schedule(self, tile_x: int, order: str = "instance", ctas: int = 0):
+        """Tile shape, work-list order and persistent grid size (chosen by autotune).
+        ctas: 0 = resident CTAs per SM x SM count; -1 = one CTA per tile."""
+        if tile_x not in (4, 8, 16):
+            raise ValueError("tile_x must be 4, 8 or 16")
+        self.tile_x, self.order, self.ctas = int(tile_x), order, int(ctas)
+        counts = tile_counts(self.configs, tile_x)
+        tile_order, tile_inst, first = work_list(counts, order)
+        table = (_lib.Instance * self.n)()
+        for k, (c, (off, pitch, rows)) in enumerate(zip(self.configs, self.layouts)):
+            inst = table[k]
+            inst.grid = self._grid(k)
+            inst.offset = off
+            inst.tiles_x = (c.nx + tile_x - 1) // tile_x
+            inst.tiles_y = (c.ny + 31) // 32
+            inst.first_tile = int(first[k])
+        self.n_tiles = int(counts.sum())
+        self._table = table
+        raw = np.frombuffer(bytes(table), dtype=np.uint8).copy()
+        self.inst_dev = torch.from_numpy(raw).to(self.device)
+        self.tile_inst = torch.from_numpy(tile_inst).to(self.device)
+        self.tile_order = torch.from_numpy(tile_order).to(self.device)
+        self._graphs = {}
+
+    def _grid(self, k: int) -> _lib.Grid:
+        c = self.configs[k]
+        off, pitch, rows = self.layouts[k]
+        g = _lib.Grid()
+        g.nx, g.ny, g.pitch, g.dtype = c.nx, c.ny, pitch, self.code
+        g.var_stride = rows * pitch
+        g.dx, g.dy, g.gamma, g.cfl, g.glm_alpha = c.dx, c.dy, c.gamma, c.cfl, c.glm_alpha
+        g.bc_x, g.bc_y = bc_x_code(c), bc_y_code(c)
+        g.powell = int(c.powell_enabled())
+        g.limiter = _lib.LIMITER_CODES[c.limiter]
+        return g
+
+    # ----------------------------------------------------------- state
+    def state(self, k: int, buf: torch.Tensor | None = None) -> torch.Tensor:
+        """[10, nx+4, ny+4] view of instance k's state."""
+        c = self.configs[k]
+        off, pitch, rows = self.layouts[k]
+        b = self.U if buf is None else buf
+        return b[off: off + 10 * rows * pitch].view(10, rows, pitch)[:, : c.nx + 2 * NG, : c.ny + 2 * NG]
+
+    def cells(self) -> np.ndarray:
+        return np.array([c.nx * c.ny for c in self.configs], dtype=np.int64)
+
+    def initialize(self):
+        """Each instance's configured initial condition (shock_interface or rmi)."""
+        for k, c in enumerate(self.configs):
+            gv = _GridView(c, self.device)
+            W = initial_conditions.shock_interface(gv)[0] if c.ic == "shock_interface" else \
+                initial_conditions.rmi(gv)[0]
+            self.state(k).copy_(prim_to_cons(W, c.gamma).to(self.dtype))
+        self._graphs = {}
+
+    def start(self, t_end: float | None = None, max_steps: int = 1 << 62):
+        """dt / GLM speed of every instance from its current state (run-loop head)."""
+        t_end = float(self.configs[0].t_end if t_end is None else t_end)
+        _lib.call("amhd_ensemble_init", ctypes.byref(self._table), self.inst_dev.data_ptr(), self.n, self.code,
+                  self.U.data_ptr(), self.ctl.data_ptr(), t_end, int(max_steps), stream_ptr())
+
+    def _advance_eager(self, n: int):
+        _lib.call("amhd_ensemble_advance", self.inst_dev.data_ptr(), self.n, self.tile_inst.data_ptr(),
+                  self.tile_order.data_ptr(), self.n_tiles, self.code, self.tile_x, self.U.data_ptr(),
+                  self.U1.data_ptr(), self.U2.data_ptr(), self.ctl.data_ptr(), int(n),
+                  self.n_tiles if self.ctas < 0 else self.ctas, stream_ptr())
+
+    def advance(self, n: int, graph: bool = True):
+        """n run-loop steps of every active instance (one graph replay)."""
+        if not graph:
+            self._advance_eager(n)
+            return
+        g = self._graphs.get(n)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._advance_eager(n)
+            self._graphs[n] = g
+        g.replay()
+
+    def controls(self):
+        return read_controls(self.ctl)
+
+    def run(self, chunk: int = 50, max_chunks: int = 1 << 30):
+        """Advance until every instance reached its end time; returns steps per instance."""
+        for _ in range(max_chunks):
+            self.advance(chunk)
+            c = self.controls()
+            if any(x.flags & _lib.AMHD_FLAG_NONFINITE for x in c):
+                bad = [k for k, x in enumerate(c) if x.flags & _lib.AMHD_FLAG_NONFINITE]
+                raise FloatingPointError(f"non-finite state in instances {bad[:8]}")
+            if not any(x.active for x in c):
+                break
+        return np.array([x.step for x in self.controls()])

@@ -36,6 +36,13 @@ def _zeros(solver):
     return torch.zeros((10, solver.nx_tot, solver.ny_tot), dtype=torch.float64, device=solver.device)
 
 
+def _sel(mask, a, b):
+    """torch.where in float64 (python-float operands would otherwise give float32)."""
+    def f64(v):
+        return v if isinstance(v, torch.Tensor) else torch.tensor(float(v), dtype=torch.float64, device=mask.device)
+    return torch.where(mask, f64(a), f64(b)).to(torch.float64)
+
+
 def _xy(solver):
     X = solver.X.to(torch.float64)
     Y = solver.Y.to(torch.float64)
@@ -61,11 +68,11 @@ def rmi(solver):
     W = _zeros(solver)
     post = X < x_shock
     rho_pre = rho1 * (1 - phi) + rho_h * phi
-    W[iRHO] = torch.where(post, rho2, rho_pre)
-    W[iVX] = torch.where(post, vx2, 0.0)
-    W[iBY] = torch.where(post, by2, by_pre)
-    W[iPR] = torch.where(post, p2, p1)
-    W[iCLR] = torch.where(post, 0.0, phi)
+    W[iRHO] = _sel(post, rho2, rho_pre)
+    W[iVX] = _sel(post, vx2, 0.0)
+    W[iBY] = _sel(post, by2, by_pre)
+    W[iPR] = _sel(post, p2, p1)
+    W[iCLR] = _sel(post, 0.0, phi)
     return W, rh
 
 
@@ -93,11 +100,11 @@ def shock_interface(solver):
         rho_pre = rho_pre * (1.0 + cfg.noise_amp * xi)
     post = X < x_shock
     W = _zeros(solver)
-    W[iRHO] = torch.where(post, rho2, rho_pre)
-    W[iVX] = torch.where(post, vx2, 0.0)
-    W[iPR] = torch.where(post, p2, p1)
+    W[iRHO] = _sel(post, rho2, rho_pre)
+    W[iVX] = _sel(post, vx2, 0.0)
+    W[iPR] = _sel(post, p2, p1)
     W[iBX] = cfg.bx0 + cfg.b1 * torch.sin(2 * np.pi * cfg.b_mode * yy / ly)
-    W[iCLR] = torch.where(post, 0.0, phi)
+    W[iCLR] = _sel(post, 0.0, phi)
     return W, rh
 
 
@@ -152,11 +159,11 @@ def brio_wu(solver):
     """main.py:51-59"""
     left = (solver.x < 0.5)[:, None].expand(solver.nx_tot, solver.ny_tot)
     W = _zeros(solver)
-    W[iRHO] = torch.where(left, 1.0, 0.125)
-    W[iPR] = torch.where(left, 1.0, 0.1)
+    W[iRHO] = _sel(left, 1.0, 0.125)
+    W[iPR] = _sel(left, 1.0, 0.1)
     W[iBX] = 0.75
-    W[iBY] = torch.where(left, 1.0, -1.0)
-    W[iCLR] = torch.where(left, 1.0, 0.0)
+    W[iBY] = _sel(left, 1.0, -1.0)
+    W[iCLR] = _sel(left, 1.0, 0.0)
     return W
 
 
@@ -177,9 +184,9 @@ def contact(solver):
     """main.py:231-237"""
     left = (solver.x < 0.5)[:, None].expand(solver.nx_tot, solver.ny_tot)
     W = _zeros(solver)
-    W[iRHO] = torch.where(left, 1.0, 3.0)
+    W[iRHO] = _sel(left, 1.0, 3.0)
     W[iPR] = 1.0
     W[iVX] = 1.0
     W[iBX] = 0.5
-    W[iCLR] = torch.where(left, 0.0, 1.0)
+    W[iCLR] = _sel(left, 0.0, 1.0)
     return W

@@ -227,12 +227,16 @@ typedef struct amhd_instance {
 /* Advance every active instance of a packed ensemble by n_steps run-loop
  * steps: one persistent launch per RK stage over the (instance, tile) work
  * list, per-instance dt/ch/t in ctl[n_inst].  U, U1, U2 are the packed
- * buffers; inst and ctl are device arrays; tile_inst is the device work list
- * (instance index of each tile); ctas is the persistent grid size (0: one
- * per SM times occupancy).  Capturable in a CUDA graph. */
+ * buffers; inst and ctl are device arrays.  Tiles are numbered per instance
+ * from inst[k].first_tile (tile_x rows x 32 columns, y fastest);
+ * tile_inst[tile] is the instance of each tile; tile_order (may be NULL for
+ * the identity) is the order in which the persistent CTAs take them
+ * (CTA b takes positions b, b + ctas, ...).  ctas is the persistent grid size
+ * (0: resident CTAs per SM x SM count).  Capturable in a CUDA graph.
+ * No counterpart in the reference (one grid per solver there). */
 int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev,
-                          int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U, void *U1, void *U2,
-                          amhd_control *ctl_dev, int32_t n_steps, int32_t ctas, void *stream);
+                          const int32_t *tile_order_dev, int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U,
+                          void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas, void *stream);
 /* amhd_control_init for every instance of the ensemble (inst_host: a host
  * copy of the instance table).  Asynchronous. */
 int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst_dev, int32_t n_inst,

@@ -1,0 +1,75 @@
+"""Batched ensemble on the GPU: instance i of a packed ensemble advances
+exactly (bitwise) as the same grid run alone, for every tile shape and work
+order; instances stop at their own end time; the autotuner runs."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def small_configs(precision, n=6, seed=11):
+    from aeromhd_cuda_b200.ensemble import draw_configs
+    return draw_configs(n, seed=seed, t_end=3.0, precision=precision, ny_choices=(32, 64))
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_instances_equal_single_grid_runs(precision):
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200.ensemble import Ensemble
+    from aeromhd_cuda_b200.solver import MHDSolver
+    cfgs = small_configs(precision)
+    ens = Ensemble(cfgs, tile_x=8)
+    ens.initialize()
+    ens.start(max_steps=12)
+    ens.advance(12)
+    ctl = ens.controls()
+    _lib.call("amhd_set_tiling", 8, 0)
+    for k, c in enumerate(cfgs):
+        s = MHDSolver(c)
+        s.initialize()
+        s.advance(max_steps=12, chunk=12)
+        assert s.step == ctl[k].step == 12
+        assert s.t == ctl[k].t
+        assert torch.equal(s.U, ens.state(k)), k
+
+
+def test_schedules_give_identical_results():
+    from aeromhd_cuda_b200.ensemble import Ensemble
+    cfgs = small_configs("fp32", n=5, seed=12)
+    ref = None
+    for tx, order, ctas in [(8, "instance", -1), (4, "interleave", 0), (16, "largest_first", 0),
+                            (8, "interleave", 200)]:
+        ens = Ensemble(cfgs, tile_x=tx, order=order, ctas=ctas)
+        ens.initialize()
+        ens.start(max_steps=6)
+        ens.advance(6)
+        if ref is None:
+            ref = ens.U.clone()
+        else:
+            assert torch.equal(ens.U, ref), (tx, order, ctas)
+
+
+def test_instances_stop_at_their_end_time():
+    from aeromhd_cuda_b200.ensemble import Ensemble
+    cfgs = small_configs("fp32", n=4, seed=13)
+    ens = Ensemble(cfgs)
+    ens.initialize()
+    ens.start(t_end=0.01)
+    steps = ens.run(chunk=8)
+    ctl = ens.controls()
+    assert all(abs(c.t - 0.01) < 1e-12 and not c.active for c in ctl)
+    assert len(set(steps.tolist())) > 1            # different grids, different dt
+
+
+def test_autotuner_picks_a_candidate_and_restores_state():
+    from aeromhd_cuda_b200.autotune import Cache, candidates, tune_ensemble
+    from aeromhd_cuda_b200.ensemble import Ensemble
+    cfgs = small_configs("fp32", n=4, seed=14)
+    ens = Ensemble(cfgs)
+    ens.initialize()
+    ens.start(max_steps=100)
+    before = ens.U.clone()
+    best, timings = tune_ensemble(ens, steps=2, cands=candidates(True, "fp32")[:6], cache=Cache())
+    assert best in timings and all(t > 0 for t in timings.values())
+    assert torch.equal(ens.U, before)
