@@ -40,6 +40,7 @@ constexpr int kTY = 32;
 
 int g_tile_x = 8;
 int g_ctas_per_sm = 0;
+int g_use_tma = 1;
 
 inline size_t elem_size(int dtype) { return dtype == AMHD_F32 ? 4 : 8; }
 
@@ -109,6 +110,14 @@ int stage_grid(int dtype, int tile_x, int n_tiles, int ctas_per_sm)
     return grid < n_tiles ? grid : n_tiles;
 }
 
+// stage input: pointer, and its tensor map when TMA staging is on
+void set_input(StageParams &p, const void *uin, const amhd_grid *g, int tile_x)
+{
+    p.uin = uin;
+    p.use_tma = 0;
+    if (g_use_tma && encode_state_map(&p.tmap, uin, g->dtype, g->pitch, g->var_stride, tile_x) == 0) p.use_tma = 1;
+}
+
 cudaError_t run_stage(int dtype, int stage, int tile_x, const StageParams &p, int grid, cudaStream_t s)
 {
     return dtype == AMHD_F64 ? Launch<double>::stage(stage, tile_x, p, grid, s)
@@ -140,7 +149,8 @@ cudaError_t run_dt_reduce(const amhd_grid *g, const void *A, int from_prim, amhd
 // three fused stages of one step; dt/ch/decay from the host or from ctl
 int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instance *insts, const int32_t *tile_inst,
                  int n_tiles, int tile_x, int grid, void *U, void *U1, void *U2, amhd_control *ctl, int use_ctl,
-                 double dt, double ch, double decay, int fuse_dt, cudaStream_t s, const int32_t *tile_order = nullptr)
+                 double dt, double ch, double decay, int fuse_dt, cudaStream_t s, const int32_t *tile_order = nullptr,
+                 const CUtensorMap *tmaps = nullptr)
 {
     StageParams p;
     memset(&p, 0, sizeof p);
@@ -155,17 +165,22 @@ int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instan
     p.decay = decay;
     p.use_ctl = use_ctl;
     const int dtype = g->dtype;
-    p.uin = U;
-    p.u0 = U;
-    p.uout = U1;
-    CK(run_stage(dtype, 1, tile_x, p, grid, s));
-    p.uin = U1;
-    p.uout = U2;
-    CK(run_stage(dtype, 2, tile_x, p, grid, s));
-    p.uin = U2;
-    p.uout = U;
-    p.fuse_dt = fuse_dt;
-    CK(run_stage(dtype, 3, tile_x, p, grid, s));
+    void *in[3] = {U, U1, U2};
+    void *out[3] = {U1, U2, U};
+    for (int st = 1; st <= 3; ++st) {
+        if (insts) {  // ensemble: per-instance maps in device memory
+            p.uin = in[st - 1];
+            p.use_tma = tmaps != nullptr;
+            p.tmaps = tmaps;
+            p.in_buf = st - 1;
+        } else {
+            set_input(p, in[st - 1], g, tile_x);
+        }
+        p.u0 = U;
+        p.uout = out[st - 1];
+        p.fuse_dt = st == 3 ? fuse_dt : 0;
+        CK(run_stage(dtype, st, tile_x, p, grid, s));
+    }
     return AMHD_OK;
 }
 
@@ -185,7 +200,43 @@ int control_upload(amhd_control *ctl, double t, double t_end, int64_t step, int6
     return AMHD_OK;
 }
 
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(ptr);
+    }
+    return fn;
+}
+
 }  // namespace
+
+namespace amhd {
+int encode_state_map(CUtensorMap *map, const void *base, int dtype, int pitch, int64_t var_stride, int tile_x)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || !base) return -1;
+    const size_t es = elem_size(dtype);
+    const cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)(var_stride / pitch), 10};
+    const cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)var_stride * es};
+    const cuuint32_t box[3] = {(cuuint32_t)(kTY + 2 * kNG), (cuuint32_t)(tile_x + 2 * kNG), 10};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    CUresult r = fn(map, dtype == AMHD_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                    const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : -1;
+}
+}  // namespace amhd
 
 #pragma GCC visibility push(default)
 extern "C" {
@@ -221,6 +272,34 @@ int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm)
     if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(AMHD_ERR_ARG, "ctas_per_sm out of range");
     g_tile_x = tile_x;
     g_ctas_per_sm = ctas_per_sm;
+    return AMHD_OK;
+}
+
+int amhd_set_tma(int32_t on)
+{
+    g_use_tma = on ? 1 : 0;
+    return AMHD_OK;
+}
+
+int amhd_ensemble_tensormaps(const amhd_instance *inst_host, int32_t n_inst, int32_t dtype, int32_t tile_x,
+                             const void *U, const void *U1, const void *U2, void *maps_host)
+{
+    if (!inst_host || n_inst <= 0 || !U || !U1 || !U2 || !maps_host) return fail(AMHD_ERR_ARG, "bad arguments");
+    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16");
+    const size_t es = elem_size(dtype);
+    CUtensorMap *maps = static_cast<CUtensorMap *>(maps_host);
+    const void *bufs[3] = {U, U1, U2};
+    for (int k = 0; k < n_inst; ++k) {
+        const amhd_grid *g = &inst_host[k].grid;
+        if (int e = check_grid(g)) return fail(e, "instance %d: %s", k, g_err.c_str());
+        for (int b = 0; b < 3; ++b) {
+            const char *base = static_cast<const char *>(bufs[b]) + (size_t)inst_host[k].offset * es;
+            if (reinterpret_cast<uintptr_t>(base) % 16)
+                return fail(AMHD_ERR_ARG, "instance %d state not 16-byte aligned", k);
+            if (encode_state_map(&maps[3 * k + b], base, dtype, g->pitch, g->var_stride, tile_x) != 0)
+                return fail(AMHD_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled failed for instance %d", k);
+        }
+    }
     return AMHD_OK;
 }
 
@@ -388,7 +467,7 @@ int amhd_compute_rhs(const amhd_grid *g, void *U, void *R, double ch, void *stre
     const amhd_instance one = single_instance(g, tx);
     StageParams p;
     memset(&p, 0, sizeof p);
-    p.uin = U;
+    set_input(p, U, g, tx);
     p.u0 = U;
     p.uout = R;
     p.one = one;
@@ -431,7 +510,7 @@ int amhd_rk_stage(const amhd_grid *g, int32_t stage, const void *Uin, const void
     const amhd_instance one = single_instance(g, tx);
     StageParams p;
     memset(&p, 0, sizeof p);
-    p.uin = Uin;
+    set_input(p, Uin, g, tx);
     p.u0 = U0;
     p.uout = Uout;
     p.one = one;
@@ -510,7 +589,7 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
     cudaError_t ce = cudaEventRecord(ev[0], s);
     for (int k = 0; k < n_steps && ce == cudaSuccess; ++k) {
         for (int st = 1; st <= 3 && ce == cudaSuccess; ++st) {
-            p.uin = st == 1 ? U : (st == 2 ? U1 : U2);
+            set_input(p, st == 1 ? U : (st == 2 ? U1 : U2), g, tx);
             p.u0 = U;
             p.uout = st == 1 ? U1 : (st == 2 ? U2 : U);
             p.fuse_dt = st == 3;
@@ -631,7 +710,8 @@ int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst
 
 int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev,
                           const int32_t *tile_order_dev, int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U,
-                          void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas, void *stream)
+                          void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas,
+                          const void *tmaps_dev, void *stream)
 {
     if (!inst_dev || !tile_inst_dev || !U || !U1 || !U2 || !ctl_dev || n_inst <= 0 || n_tiles <= 0)
         return fail(AMHD_ERR_ARG, "bad ensemble arguments");
@@ -652,7 +732,7 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
     memset(&dummy, 0, sizeof dummy);
     for (int k = 0; k < n_steps; ++k) {
         if (int e = three_stages(&gdt, dummy, inst_dev, tile_inst_dev, n_tiles, tile_x, grid, U, U1, U2, ctl_dev, 1, 0,
-                                 0, 1, 1, s, tile_order_dev))
+                                 0, 1, 1, s, tile_order_dev, static_cast<const CUtensorMap *>(tmaps_dev)))
             return e;
         CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 1, 0, s));
     }

@@ -19,6 +19,7 @@
 #include "amhd_launch.h"
 #include "amhd_fast.cuh"
 #include "amhd_physics.cuh"
+#include "amhd_tma.cuh"
 
 #include <type_traits>
 
@@ -45,7 +46,7 @@ constexpr bool kFast = std::is_same<R, float>::value;  // float32: slope pre-pas
 
 template <typename R, int TX>
 struct TileSmem {
-    R w[NV][TX + 2 * NG][HW];      // primitives of the tile + halo
+    alignas(128) R w[NV][TX + 2 * NG][HW];  // tile + halo: TMA lands conserved, converted in place
     // limited slopes (float32 path only): x-slopes of halo rows 1..TX+2 over the
     // tile's columns, y-slopes of the tile's rows over halo columns 1..TY+2
     R sx[kFast<R> ? NV : 1][kFast<R> ? TX + 2 : 1][TY];
@@ -53,7 +54,9 @@ struct TileSmem {
     R fx[NV][TX + 1][TY];          // x-face fluxes (face a: between tile rows a-1 and a)
     R fy[NV][TX][TY + 1];          // y-face fluxes
     unsigned long long red[4][32]; // per-warp dt partials
+    uint64_t mbar;                 // TMA completion barrier
     int nonfinite;
+    int tma_ok;
 };
 
 __device__ __forceinline__ const amhd_instance &inst_of(const StageParams &p, int tile, int &inst_idx)
@@ -69,8 +72,9 @@ __device__ __forceinline__ const amhd_instance &inst_of(const StageParams &p, in
 // ---------------------------------------------------------------------------
 // fused RK stage; STAGE 1..3 (solver.py:319-329), STAGE 0 = compute_rhs (R out)
 // ---------------------------------------------------------------------------
+// returns false when the CTA must stop (a TMA transfer did not complete)
 template <typename R, int TX, int STAGE>
-__device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, TX> &sm, int tile)
+__device__ __forceinline__ bool rk_stage_tile(const StageParams &p, TileSmem<R, TX> &sm, int tile, uint32_t &phase)
 {
     constexpr int NT = TX * TY;  // threads per block: one per tile cell
     constexpr int VN = Vec<R>::N;
@@ -84,7 +88,7 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
 
     double dt = p.dt, ch = p.ch, decay = p.decay;
     if (p.use_ctl) {
-        if (!ctl->active) return;
+        if (!ctl->active) return true;
         dt = ctl->dt;
         ch = ctl->ch;
         decay = ctl->decay;
@@ -102,17 +106,46 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
     // ---- phase A: tile + halo -> primitives in shared memory --------------
     // the padded layout keeps every halo row/column of every tile in bounds
     constexpr int QPR = HW / VN;  // vectors per halo row
+    if (p.use_tma) {
+        if (t == 0) {
+            const CUtensorMap *map = p.inst ? &p.tmaps[3 * ii + p.in_buf] : &p.tmap;
+            tma::fence_proxy_async();
+            tma::arrive_expect_tx(&sm.mbar, (uint32_t)sizeof(sm.w));
+            tma::load_3d(&sm.w[0][0][0], map, j0 - NG, i0 - NG, 0, &sm.mbar);
+            sm.tma_ok = tma::wait(&sm.mbar, phase);
+        }
+        phase ^= 1u;
+        __syncthreads();
+        if (!sm.tma_ok) {
+            if (t == 0) {
+                if (ctl != nullptr) atomicOr(&ctl->flags, AMHD_FLAG_TIMEOUT);
+                tma::wait(&sm.mbar, phase ^ 1u);  // give the copy in flight a second bounded chance to land
+            }
+            return false;
+        }
+    }
     for (int q = t; q < HROWS * QPR; q += NT) {
         const int r = q / QPR, c = (q % QPR) * VN;
-        const int64_t gi = (int64_t)(i0 - NG + r) * pitch + (j0 - NG + c);
         R u[VN][NV];
+        if (p.use_tma) {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            VT x = __ldg(reinterpret_cast<const VT *>(uin + v * vs + gi));
-            const R *xs = reinterpret_cast<const R *>(&x);
+            for (int v = 0; v < NV; ++v) {
+                VT x = *reinterpret_cast<const VT *>(&sm.w[v][r][c]);
+                const R *xs = reinterpret_cast<const R *>(&x);
 #pragma unroll
-            for (int k = 0; k < VN; ++k) u[k][v] = xs[k];
+                for (int k = 0; k < VN; ++k) u[k][v] = xs[k];
+            }
+        } else {
+            const int64_t gi = (int64_t)(i0 - NG + r) * pitch + (j0 - NG + c);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                VT x = __ldg(reinterpret_cast<const VT *>(uin + v * vs + gi));
+                const R *xs = reinterpret_cast<const R *>(&x);
+#pragma unroll
+                for (int k = 0; k < VN; ++k) u[k][v] = xs[k];
+            }
         }
+        R wq[NV][VN];
 #pragma unroll
         for (int k = 0; k < VN; ++k) {
             R w[NV];
@@ -121,24 +154,38 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
             else
                 cons_to_prim_cell(u[k], g.gamma, w);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) sm.w[v][r][c + k] = w[v];
+            for (int v = 0; v < NV; ++v) wq[v][k] = w[v];
         }
+        // one 16-byte shared store per plane (rows are 16-byte aligned: HW * sizeof(R) % 16 == 0)
+#pragma unroll
+        for (int v = 0; v < NV; ++v) *reinterpret_cast<VT *>(&sm.w[v][r][c]) = *reinterpret_cast<const VT *>(wq[v]);
     }
     __syncthreads();
 
     if constexpr (kFast<R>) {
-        // ---- phase A2 (float32): limited slopes, once per cell and direction
-        constexpr int NSX = (TX + 2) * TY, NSY = TX * (TY + 2);
-        for (int q = t; q < NSX + NSY; q += NT) {
-            if (q < NSX) {
-                const int r = q / TY + 1, c = q % TY + NG;
+        // ---- phase A2 (float32): limited slopes, once per cell and direction.
+        // Work in 32-lane tasks that each stay on one shared-memory row:
+        // TX+2 rows of x-slopes, TX rows of y-slopes (columns 1..32), and one
+        // task for the last two y-slope columns of every row.
+        constexpr int NTASK = (TX + 2) + TX + 1;
+        const int lane = t & 31;
+        for (int task = t >> 5; task < NTASK; task += NT / 32) {
+            if (task < TX + 2) {
+                const int r = task + 1, c = lane + NG;
 #pragma unroll
                 for (int v = 0; v < NV; ++v)
-                    sm.sx[v][r - 1][c - NG] = fast::slope(sm.w[v][r - 1][c], sm.w[v][r][c], sm.w[v][r + 1][c],
-                                                          g.limiter);
+                    sm.sx[v][r - 1][lane] = fast::slope(sm.w[v][r - 1][c], sm.w[v][r][c], sm.w[v][r + 1][c],
+                                                        g.limiter);
             } else {
-                const int h = q - NSX;
-                const int r = h / (TY + 2) + NG, k = h % (TY + 2) + 1;
+                int r, k;
+                if (task < 2 * TX + 2) {
+                    r = task - (TX + 2) + NG;
+                    k = lane + 1;
+                } else {
+                    if (lane >= 2 * TX) continue;
+                    r = (lane >> 1) + NG;
+                    k = TY + 1 + (lane & 1);
+                }
 #pragma unroll
                 for (int v = 0; v < NV; ++v)
                     sm.sy[v][r - NG][k - 1] = fast::slope(sm.w[v][r][k - 1], sm.w[v][r][k], sm.w[v][r][k + 1],
@@ -157,12 +204,17 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
     // rho, vy, vx, vz, By, Bx, Bz, p, psi, C of physics.py:376-379)
     constexpr int rot[NV] = {0, 2, 1, 3, 5, 4, 6, 7, 8, 9};
     const float igm1 = 1.0f / float(g.gamma - 1.0), half_ich = ch > 0.0 ? float(0.5 / ch) : 0.f;
-    for (int f = t; f < NFX + NFY; f += NT) {
+    // 32-lane tasks on one row each: TX+1 rows of x faces, TX rows of y faces
+    // (columns 0..31), one task for the last y face (column 32) of every row
+    constexpr int NFTASK = (TX + 1) + TX + 1;
+    static_assert(NFX + NFY == 32 * (2 * TX + 1) + TX, "face count");
+    for (int f = t; f < 32 * NFTASK; f += NT) {
+        const int task = f >> 5, lane = f & 31;
+        if (task == NFTASK - 1 && lane >= TX) continue;
         R wl[NV], wr[NV], fl[NV];
-        const bool xf = f < NFX;
-        const int h = xf ? f : f - NFX;
-        const int a = xf ? h / TY : h / (TY + 1);
-        const int c = xf ? h % TY : h % (TY + 1);
+        const bool xf = task <= TX;
+        const int a = xf ? task : (task < NFTASK - 1 ? task - (TX + 1) : lane);
+        const int c = xf ? lane : (task < NFTASK - 1 ? lane : TY);
         if constexpr (kFast<R>) {
             if (xf) {
 #pragma unroll
@@ -331,6 +383,7 @@ __device__ __forceinline__ void rk_stage_tile(const StageParams &p, TileSmem<R, 
             if (sm.nonfinite) atomicOr(&ctl->flags, AMHD_FLAG_NONFINITE);
         }
     }
+    return true;
 }
 
 // resident CTAs per SM the register budget is shaped for (float32 path)
@@ -338,13 +391,18 @@ template <typename R, int TX>
 constexpr int kMinBlocks = kFast<R> ? (TX == 4 ? 6 : (TX == 8 ? 3 : 1)) : 1;
 
 template <typename R, int TX, int STAGE>
-__global__ void __launch_bounds__(TX * TY, (kMinBlocks<R, TX>)) rk_stage_kernel(const StageParams p)
+__global__ void __launch_bounds__(TX * TY, (kMinBlocks<R, TX>)) rk_stage_kernel(const __grid_constant__ StageParams p)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     TileSmem<R, TX> &sm = *reinterpret_cast<TileSmem<R, TX> *>(smem_raw);
+    uint32_t phase = 0;
+    if (p.use_tma) {
+        if (threadIdx.x == 0) tma::mbar_init(&sm.mbar, 1);
+        __syncthreads();
+    }
     for (int pos = blockIdx.x; pos < p.n_tiles; pos += gridDim.x) {
         const int tile = p.tile_order ? p.tile_order[pos] : pos;
-        rk_stage_tile<R, TX, STAGE>(p, sm, tile);
+        if (!rk_stage_tile<R, TX, STAGE>(p, sm, tile, phase)) return;
         __syncthreads();  // shared memory is reused by the next tile
     }
 }

@@ -1,6 +1,7 @@
 // amhd_launch.h -- host-side launch interface between the C ABI (amhd_capi.cu)
 // and the per-precision kernel translation units (amhd_f64.cu, amhd_f32.cu).
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -8,8 +9,14 @@
 
 namespace amhd {
 
-// arguments of one fused RK stage launch over a list of (instance, tile)
+// arguments of one fused RK stage launch over a list of (instance, tile);
+// passed by value as a __grid_constant__ kernel parameter (the tensor map
+// must live there or in global memory for the TMA unit to read it)
 struct StageParams {
+    CUtensorMap tmap;              // single grid: tensor map of uin (when use_tma)
+    const CUtensorMap *tmaps;      // ensemble: 3 maps per instance (U, U1, U2), device memory
+    int32_t use_tma;               // stage the tile + halo with TMA
+    int32_t in_buf;                // ensemble: which of the 3 maps is uin
     const void *uin;               // stage input state (stencil source)
     const void *u0;                // step base state U0
     void *uout;                    // stage output (may alias u0 on stage 3)
@@ -53,6 +60,9 @@ struct Launch {
     static cudaError_t bflux(const amhd_grid &g, const R *U, double *out, cudaStream_t s);
     static cudaError_t bflux_accum(const amhd_grid &g, const R *U, amhd_control *ctl, double dt, cudaStream_t s);
 };
+
+// tensor map of one state buffer for tiles of tile_x rows (0 on success)
+int encode_state_map(CUtensorMap *map, const void *base, int dtype, int pitch, int64_t var_stride, int tile_x);
 
 cudaError_t launch_control_resume(amhd_control *ctl, int n, double snap_t, cudaStream_t s);
 cudaError_t launch_diag_finish(const amhd_grid &g, double x0, const double *rows, double *out, cudaStream_t s);

@@ -130,7 +130,7 @@ class _GridView:
 
 class Ensemble:
     def __init__(self, configs: Sequence[Config], tile_x: int = 8, order: str = "instance", ctas: int = 0,
-                 device=None):
+                 device=None, use_tma: bool = True):
         if not configs:
             raise ValueError("empty ensemble")
         precs = {c.precision for c in configs}
@@ -147,6 +147,7 @@ class Ensemble:
         self.n = len(self.configs)
         self.tile_x = int(tile_x)
         self.ctas = int(ctas)
+        self.use_tma = bool(use_tma)
         self.layouts, off = pack_layout(self.configs, self.code)
         self.total = off
         self.U = torch.zeros(off, dtype=self.dtype, device=self.device)
@@ -179,6 +180,13 @@ class Ensemble:
         self.inst_dev = torch.from_numpy(raw).to(self.device)
         self.tile_inst = torch.from_numpy(tile_inst).to(self.device)
         self.tile_order = torch.from_numpy(tile_order).to(self.device)
+        self.tmaps_dev = None
+        if self.use_tma:
+            # TMA descriptors of every instance's box in U, U1, U2 for this tile shape
+            maps = torch.empty(3 * self.n * 128, dtype=torch.uint8)
+            _lib.call("amhd_ensemble_tensormaps", ctypes.byref(table), self.n, self.code, self.tile_x,
+                      self.U.data_ptr(), self.U1.data_ptr(), self.U2.data_ptr(), maps.data_ptr())
+            self.tmaps_dev = maps.to(self.device)
         self._graphs = {}
 
     def _grid(self, k: int) -> _lib.Grid:
@@ -223,7 +231,8 @@ class Ensemble:
         _lib.call("amhd_ensemble_advance", self.inst_dev.data_ptr(), self.n, self.tile_inst.data_ptr(),
                   self.tile_order.data_ptr(), self.n_tiles, self.code, self.tile_x, self.U.data_ptr(),
                   self.U1.data_ptr(), self.U2.data_ptr(), self.ctl.data_ptr(), int(n),
-                  self.n_tiles if self.ctas < 0 else self.ctas, stream_ptr())
+                  self.n_tiles if self.ctas < 0 else self.ctas,
+                  self.tmaps_dev.data_ptr() if self.tmaps_dev is not None else None, stream_ptr())
 
     def advance(self, n: int, graph: bool = True):
         """n run-loop steps of every active instance (one graph replay)."""

@@ -52,6 +52,10 @@ def parse_args(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--tma", type=int, default=1, help="stage tiles with TMA (1) or 128-bit loads (0)")
+    ap.add_argument("--tile-x", type=int, default=8)
+    ap.add_argument("--ensemble", type=int, default=0,
+                    help="also time the batched shock-interface ensemble of this many instances")
     return ap.parse_args(argv)
 
 
@@ -227,6 +231,9 @@ def run_ours(a, world, rank, local):
     from aeromhd_cuda_b200.solver import MHDSolver
 
     n = a.n
+    _lib.call("amhd_init")
+    _lib.call("amhd_set_tma", int(a.tma))
+    _lib.call("amhd_set_tiling", int(a.tile_x), 0)
     cfg = ot_config(n, a.precision)
     s = MHDSolver(cfg)
     s.set_primitive(ic.orszag_tang(s))
@@ -325,6 +332,10 @@ def run_ours(a, world, rank, local):
                 "stage_hbm_frac": round(80 * 8 * cells * k64 / ((ms[0] + ms[1] + ms[2]) / 1e3) / 1e9 / hbm, 4)}
         del s64
 
+    ens_line = None
+    if a.ensemble > 0:
+        ens_line = run_ensemble(a, world)
+
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         rate, k, el, cores = cpu_oracle_rate(512, target_s=10.0)
@@ -338,11 +349,40 @@ def run_ours(a, world, rank, local):
         "config": {"workload": f"orszag_tang_{n}x{n}_{a.precision}", "nx": n, "ny": n, "precision": a.precision,
                    "pressure_recovery": "f64", "dt_reduction": "f64",
                    "l2": "inputs larger than L2 (3 state buffers of %.0f MB)" % (10 * (n + 4) * (n + 4) * es / 1e6),
-                   "parallelism": f"replicas x{world}", "tile": "8x32, one CTA per tile"},
+                   "parallelism": f"replicas x{world}", "tile": f"{a.tile_x}x32, one CTA per tile",
+                   "staging": "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * a.steps,
-        "clocks": clk.summary(), "fp64": fp64,
+        "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
     }
     return line
+
+
+def run_ensemble(a, world):
+    """Aggregate zone-updates/s of the uneven shock-interface ensemble (one persistent
+    launch per RK stage, graph-replayed steps)."""
+    import torch
+    from aeromhd_cuda_b200.ensemble import Ensemble, draw_configs
+    from aeromhd_cuda_b200 import _lib
+    cfgs = draw_configs(a.ensemble, seed=0, t_end=3.0, precision=a.precision)
+    ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=0, use_tma=bool(a.tma))
+    ens.initialize()
+    ens.start()
+    k = max(3, a.steps // 2)
+    ens.advance(k)  # warm-up + graph capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ens.advance(k)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    cells = int(ens.cells().sum())
+    ctl = ens.controls()
+    if any(c.flags & _lib.AMHD_FLAG_NONFINITE for c in ctl):
+        raise SystemExit("non-finite state in the ensemble benchmark")
+    return {"value": world * cells * k / (ms / 1e3), "unit": "zone-updates/s", "instances": a.ensemble,
+            "cells": cells, "steps": k, "ms_per_step": ms / k,
+            "schedule": {"tile_x": a.tile_x, "order": "instance", "grid": "persistent"}}
 
 
 def run_reference(a, world, rank):

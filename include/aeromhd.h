@@ -54,6 +54,7 @@ extern "C" {
 #define AMHD_FLAG_NONFINITE 1   /* a non-finite value was written by a step */
 #define AMHD_FLAG_DT_TINY 2     /* dt <= 1e-16 stopped the loop (solver.py:479) */
 #define AMHD_FLAG_PAUSED 4      /* loop paused at a snapshot time (amhd_control.snap_t) */
+#define AMHD_FLAG_TIMEOUT 8     /* a bounded device wait (TMA completion) expired */
 
 /* Grid and physics parameters of one instance (reference Config,
  * config.py:47-89, flattened; dx, dy precomputed as config.py:78-84 does). */
@@ -114,6 +115,9 @@ size_t amhd_control_size(void);
  * otherwise a persistent grid of ctas_per_sm x SM-count CTAs).  Process-wide;
  * chosen by the autotuner.  No counterpart in the reference. */
 int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm);
+/* Stage the tile + halo with TMA (cp.async.bulk.tensor) when on (default) or
+ * with 128-bit loads when off.  Process-wide.  No counterpart in the reference. */
+int amhd_set_tma(int32_t on);
 /* shared memory per CTA and resident CTAs per SM of the stage kernel */
 int amhd_stage_info(int32_t dtype, int32_t tile_x, int32_t *smem_bytes, int32_t *ctas_per_sm, int32_t *sm_count);
 
@@ -232,11 +236,19 @@ typedef struct amhd_instance {
  * tile_inst[tile] is the instance of each tile; tile_order (may be NULL for
  * the identity) is the order in which the persistent CTAs take them
  * (CTA b takes positions b, b + ctas, ...).  ctas is the persistent grid size
- * (0: resident CTAs per SM x SM count).  Capturable in a CUDA graph.
+ * (0: resident CTAs per SM x SM count).  tmaps_dev: device copy of
+ * amhd_ensemble_tensormaps for this tile_x (NULL: 128-bit loads instead of
+ * TMA).  Capturable in a CUDA graph.
  * No counterpart in the reference (one grid per solver there). */
 int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev,
                           const int32_t *tile_order_dev, int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U,
-                          void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas, void *stream);
+                          void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas,
+                          const void *tmaps_dev, void *stream);
+/* Fill maps_host (3 * n_inst CUtensorMap of 128 bytes: U, U1, U2 per
+ * instance) for amhd_ensemble_advance; copy it to device memory (64-byte
+ * aligned) before use.  No counterpart in the reference. */
+int amhd_ensemble_tensormaps(const amhd_instance *inst_host, int32_t n_inst, int32_t dtype, int32_t tile_x,
+                             const void *U, const void *U1, const void *U2, void *maps_host);
 /* amhd_control_init for every instance of the ensemble (inst_host: a host
  * copy of the instance table).  Asynchronous. */
 int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst_dev, int32_t n_inst,

@@ -333,3 +333,19 @@ def test_device_argument_errors(amhd):
     with pytest.raises(amhd.lib.AmhdError):
         amhd.lib.call("amhd_step_ssprk3", s._grid(), bad.data_ptr(), _tensors.ptr(s._U1), _tensors.ptr(s._U2), 0.1,
                       1.0, 1.0, None, _tensors.stream_ptr())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_tma_staging_matches_plain_loads_single_grid(amhd, precision):
+    from aeromhd_cuda_b200 import initial_conditions as ic
+    res = []
+    try:
+        for tma in (1, 0):
+            amhd.lib.call("amhd_set_tma", tma)
+            s = amhd.solver.MHDSolver(ot_cfg(80, precision=precision))
+            s.set_primitive(ic.orszag_tang(s))
+            s.advance(max_steps=7, chunk=7, graph=False)
+            res.append(s.U.clone())
+    finally:
+        amhd.lib.call("amhd_set_tma", 1)
+    assert torch.equal(res[0], res[1])
