@@ -11,7 +11,10 @@ runs a kernel of libaeromhd.so:
     hlld_flux_y(WL, WR, gamma, ch)  physics.py:373-379
     mhd_rankine_hugoniot(...)     physics.py:385-429 (host, once per set-up)
 
-``xp`` is torch, playing the role ``xp = cp`` plays in the reference.
+``xp`` plays the role ``xp = cp`` plays in the reference: torch, with the
+array constructors defaulting to float64 on the current CUDA device (numpy's
+and CuPy's default dtype), so set-up code written for the reference builds
+float64 GPU arrays.
 """
 from __future__ import annotations
 
@@ -22,7 +25,57 @@ from . import _lib
 from ._tensors import as_cuda, make_grid, ptr, stream_ptr
 from .config import FLOOR_PR, FLOOR_RHO, NVAR  # noqa: F401  (re-exported like the reference)
 
-xp = torch
+
+class _TorchXP:
+    """torch namespace whose constructors default to float64 on the GPU (numpy/CuPy defaults)."""
+
+    _F64 = torch.float64
+
+    def __getattr__(self, name):
+        return getattr(torch, name)
+
+    @staticmethod
+    def _dev(device):
+        return device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu")
+
+    def zeros(self, *shape, dtype=None, device=None):
+        return torch.zeros(*shape, dtype=dtype or self._F64, device=self._dev(device))
+
+    def ones(self, *shape, dtype=None, device=None):
+        return torch.ones(*shape, dtype=dtype or self._F64, device=self._dev(device))
+
+    def empty(self, *shape, dtype=None, device=None):
+        return torch.empty(*shape, dtype=dtype or self._F64, device=self._dev(device))
+
+    def full(self, shape, value, dtype=None, device=None):
+        return torch.full(shape, value, dtype=dtype or self._F64, device=self._dev(device))
+
+    def asarray(self, a, dtype=None, device=None):
+        if isinstance(a, torch.Tensor):
+            return a.to(device=self._dev(device), dtype=dtype or a.dtype)
+        arr = np.asarray(a)
+        dt = dtype or (self._F64 if arr.dtype.kind == "f" else None)
+        return torch.as_tensor(arr, dtype=dt, device=self._dev(device))
+
+    def arange(self, *args, dtype=None, device=None):
+        return torch.arange(*args, dtype=dtype, device=self._dev(device))
+
+    def linspace(self, start, stop, num, dtype=None, device=None):
+        return torch.linspace(start, stop, num, dtype=dtype or self._F64, device=self._dev(device))
+
+    def where(self, cond, a, b):
+        def t(v):
+            return v if isinstance(v, torch.Tensor) else torch.tensor(v, dtype=self._F64, device=cond.device)
+        return torch.where(cond, t(a), t(b))
+
+    def maximum(self, a, b):
+        def t(v, ref):
+            return v if isinstance(v, torch.Tensor) else torch.tensor(v, dtype=ref.dtype, device=ref.device)
+        ref = a if isinstance(a, torch.Tensor) else b
+        return torch.maximum(t(a, ref), t(b, ref))
+
+
+xp = _TorchXP()
 
 
 def _state_like(t: torch.Tensor) -> torch.Tensor:
