@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -740,4 +741,63 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
 }
 
 }  // extern "C"
+#pragma GCC visibility pop
+
+// ---------------------------------------------------------------------------
+// Diagnostics without any allocation by the caller or the library.
+//
+// The row pass of amhd_diagnostics needs 7 * nx doubles of scratch.  Here that
+// scratch is a fixed file-scope device array: it is part of the module image,
+// so every GPU that loads this library holds it (AMHD_NOALLOC_MAX_NX * 7 * 8
+// bytes = 896 KiB) until the process exits, and no call ever allocates.
+// In host code `g_noalloc_rows` only names a host-side shadow of the symbol,
+// never a device address; the device address is looked up per device with
+// cudaGetSymbolAddress, on the first call made while that device is current.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_noalloc_rows[7 * AMHD_NOALLOC_MAX_NX];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[kMaxDevices] = {};
+
+int noalloc_rows_ptr(double **out)
+{
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(AMHD_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_rows);
+        if (e != cudaSuccess || !p)
+            return fail(AMHD_ERR_CUDA, "cudaGetSymbolAddress of the diagnostics scratch on device %d: %s", dev,
+                        cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = static_cast<double *>(g_noalloc_ptr[dev]);
+    return AMHD_OK;
+}
+}  // namespace
+
+#pragma GCC visibility push(default)
+extern "C" int amhd_diagnostics_noalloc(const amhd_grid *g, const void *U, double x0, double *out_dev, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !out_dev) return fail(AMHD_ERR_ARG, "NULL argument");
+    if (g->nx > AMHD_NOALLOC_MAX_NX)
+        return fail(AMHD_ERR_ARG, "amhd_diagnostics_noalloc: nx = %d exceeds the fixed scratch limit of %d rows", g->nx,
+                    AMHD_NOALLOC_MAX_NX);
+    double *rows = nullptr;
+    if (int e = noalloc_rows_ptr(&rows)) return e;
+    cudaStream_t s = S(stream);
+    // every one of the 7 * nx scratch entries the finish kernel reads is written by
+    // the row kernel of the same call, so nothing has to be cleared between calls
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::diag_rows(*g, static_cast<const double *>(U), rows, s));
+    else
+        CK(Launch<float>::diag_rows(*g, static_cast<const float *>(U), rows, s));
+    CK(launch_diag_finish(*g, x0, rows, out_dev, s));
+    return AMHD_OK;
+}
 #pragma GCC visibility pop

@@ -217,6 +217,23 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
  * rows_dev: scratch of 4*nx doubles.  Asynchronous. */
 int amhd_diagnostics(const amhd_grid *g, const void *U, double x0, double *out_dev, double *rows_dev, void *stream);
 
+/* The same diagnostics for callers that cannot allocate device memory: a
+ * caller running inside CUDA stream capture (where an allocation is not a
+ * capturable operation), a host framework that owns every device allocation
+ * and hands plugins only their inputs and outputs, or a loop with a strict
+ * time budget that must not risk an allocation synchronising the device.
+ * No counterpart in the reference.  The row scratch is a fixed device array
+ * compiled into this library (room for nx <= AMHD_NOALLOC_MAX_NX interior
+ * rows; larger grids get AMHD_ERR_ARG); it is resident on every GPU that
+ * loads the library until the process exits.  The first call on a device
+ * looks the array up (cudaGetSymbolAddress) and must be made with that
+ * device current and before any stream capture that contains later calls.
+ * All calls share the one array: calls whose kernels may overlap on the GPU
+ * (different streams without ordering) race on it.  out_dev: 7 doubles as
+ * for amhd_diagnostics.  Asynchronous. */
+#define AMHD_NOALLOC_MAX_NX 16384
+int amhd_diagnostics_noalloc(const amhd_grid *g, const void *U, double x0, double *out_dev, void *stream);
+
 /* ---- batched ensemble -------------------------------------------------- */
 /* One entry per instance of the packed ensemble; offsets are element offsets
  * of each instance's state in the three packed state buffers. */
