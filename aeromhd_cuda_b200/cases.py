@@ -1,0 +1,196 @@
+"""The benchmark configurations as runnable cases.
+
+    python -m aeromhd_cuda_b200.cases orszag_tang --n 512 --precision fp32
+    python -m aeromhd_cuda_b200.cases cp_alfven --sizes 32 64 128 256 512 1024
+    python -m aeromhd_cuda_b200.cases shock_interface --nx 2048 --ny 512 --t-end 3
+    python -m aeromhd_cuda_b200.cases brio_wu
+
+Each prints one JSON object (wall time, steps, zone-updates/s and the case's
+accuracy figures).  Errors of the float32 path are measured against a float64
+run of the same case on the GPU (itself bit-exact with the reference's
+float64 arithmetic).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import sys
+import time
+
+import numpy as np
+import torch
+
+from . import initial_conditions as ic
+from .config import Config
+from .solver import MHDSolver
+
+
+def _timed_advance(s: MHDSolver, t_end: float, max_steps: int = 1 << 60, chunk: int = 200):
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.advance(t_end=t_end, max_steps=max_steps, chunk=chunk)
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0
+
+
+def rel_l1(a: torch.Tensor, b: torch.Tensor) -> float:
+    a, b = a.double(), b.double()
+    return float((a - b).abs().sum() / b.abs().sum().clamp_min(1e-300))
+
+
+def interior(s: MHDSolver) -> torch.Tensor:
+    return s.U[:, 2:-2, 2:-2]
+
+
+# --------------------------------------------------------------- Orszag-Tang
+def orszag_tang_config(n: int, precision: str, t_end: float = 0.5, cfl: float = 0.4) -> Config:
+    return Config(nx=n, ny=n, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, t_end=t_end, cfl=cfl, gamma=5.0 / 3.0,
+                  powell_source=False, bc_x_type="periodic", bc_y_type="periodic", precision=precision)
+
+
+def orszag_tang(n: int = 512, t_end: float = 0.5, precisions=("fp32", "fp64")) -> dict:
+    out = {"case": "orszag_tang", "n": n, "t_end": t_end}
+    runs = {}
+    for p in precisions:
+        s = MHDSolver(orszag_tang_config(n, p, t_end))
+        s.set_primitive(ic.orszag_tang(s))
+        wall = _timed_advance(s, t_end)
+        d = s.device_diagnostics()
+        runs[p] = s
+        out[p] = {"steps": s.step, "t": s.t, "wall_s": wall, "zone_updates_per_s": n * n * s.step / wall,
+                  "mass": d["mass"], "energy": d["energy"], "divB_L2": d["divB_L2"]}
+    if "fp32" in runs and "fp64" in runs:
+        a, b = interior(runs["fp32"]), interior(runs["fp64"])
+        names = ("rho", "mx", "my", "mz", "Bx", "By", "Bz", "E", "psi", "rhoC")
+        out["fp32_vs_fp64_rel_l1"] = {names[v]: rel_l1(a[v], b[v]) for v in (0, 1, 2, 4, 5, 7)}
+        out["same_step_count"] = runs["fp32"].step == runs["fp64"].step
+    return out
+
+
+# ------------------------------------------------------------------ CP Alfven
+def cp_alfven(sizes=(32, 64, 128, 256, 512, 1024), precision: str = "fp64", amp: float = 0.1,
+              angle: float = 30.0, cfl: float = 0.4) -> dict:
+    """Circularly polarised Alfven wave, one period; L1 error of B_perp against the exact solution."""
+    lx, ly = ic.cp_alfven_box(angle)
+    out = {"case": "cp_alfven", "precision": precision, "amp": amp, "angle_deg": angle, "sizes": list(sizes),
+           "L1": [], "steps": [], "zone_updates_per_s": []}
+    a = math.radians(angle)
+    for n in sizes:
+        cfg = Config(nx=n, ny=n, x_min=0.0, x_max=lx, y_min=0.0, y_max=ly, t_end=1.0, cfl=cfl, gamma=5.0 / 3.0,
+                     powell_source=False, bc_x_type="periodic", bc_y_type="periodic", precision=precision)
+        s = MHDSolver(cfg)
+        W0 = ic.cp_alfven(s, amp=amp, angle_deg=angle)
+        s.set_primitive(W0)
+        wall = _timed_advance(s, 1.0)
+        from .physics import cons_to_prim
+        W = cons_to_prim(s.U, cfg.gamma).double()
+        # B_perp = -Bx sin(a) + By cos(a), interior
+        bp = (-W[4] * math.sin(a) + W[5] * math.cos(a))[2:-2, 2:-2]
+        bp0 = (-W0[4] * math.sin(a) + W0[5] * math.cos(a))[2:-2, 2:-2]
+        out["L1"].append(float((bp - bp0).abs().mean()))
+        out["steps"].append(s.step)
+        out["zone_updates_per_s"].append(n * n * s.step / wall)
+    L1 = out["L1"]
+    out["orders"] = [math.log(L1[i - 1] / L1[i]) / math.log(sizes[i] / sizes[i - 1]) for i in range(1, len(L1))]
+    out["mean_order"] = float(np.mean(out["orders"])) if out["orders"] else None
+    return out
+
+
+# ------------------------------------------------------------ shock interface
+def shock_interface_config(nx=2048, ny=512, precision="fp32", t_end=3.0, seed=0) -> Config:
+    """Single shock-accelerated interface: [0,4]x[0,1], Mach 3 from x = 0.5, interface at
+    x = 1 + 0.05 cos(2 pi 2 y), rho 1 | 3, p = 1, 2-cell tanh, uniform Bx = 0.1, seeded
+    1e-3 density noise ahead of the shock; outflow in x, periodic in y; GLM + Powell."""
+    return Config(nx=nx, ny=ny, x_min=0.0, x_max=4.0, y_min=0.0, y_max=1.0, t_end=t_end, cfl=0.4, gamma=5.0 / 3.0,
+                  mach=3.0, density_ratio=3.0, interface_x=1.0, shock_x=0.5, perturbation_amp=0.05,
+                  perturbation_mode=2, perturbation_shape="cos", interface_cells=2.0, bx0=0.1, noise_amp=1e-3,
+                  seed=seed, ic="shock_interface", powell_mode="on", bc_x_type="extrapolation",
+                  bc_y_type="periodic", diag_interval=200, snapshot_times=[], precision=precision)
+
+
+def shock_interface(nx=2048, ny=512, t_end=3.0, precisions=("fp32", "fp64"), diag_every=0.25) -> dict:
+    out = {"case": "shock_interface", "nx": nx, "ny": ny, "t_end": t_end}
+    runs = {}
+    for p in precisions:
+        cfg = shock_interface_config(nx, ny, p, t_end)
+        s = MHDSolver(cfg)
+        s.initialize()
+        d0 = s.device_diagnostics()
+        hist = {"t": [0.0], "mixing_width": [d0["mixing_width_integral"]], "divB_L2": [d0["divB_L2"]],
+                "mass": [d0["mass"]], "energy": [d0["energy"]]}
+        wall = 0.0
+        tt = 0.0
+        while tt < t_end - 1e-12:
+            tt = min(t_end, tt + diag_every)
+            wall += _timed_advance(s, tt)
+            d = s.device_diagnostics()
+            hist["t"].append(s.t)
+            hist["mixing_width"].append(d["mixing_width_integral"])
+            hist["divB_L2"].append(d["divB_L2"])
+            hist["mass"].append(d["mass"])
+            hist["energy"].append(d["energy"])
+        ebnd = s._cumulative_boundary_energy
+        runs[p] = (s, hist)
+        out[p] = {"steps": s.step, "t": s.t, "wall_s": wall, "zone_updates_per_s": nx * ny * s.step / wall,
+                  "history": hist,
+                  "mass_drift_rel": (hist["mass"][-1] - hist["mass"][0]) / hist["mass"][0],
+                  "energy_drift_rel_raw": (hist["energy"][-1] - hist["energy"][0]) / hist["energy"][0],
+                  "boundary_energy": ebnd,
+                  "energy_drift_rel_corrected": (hist["energy"][-1] - ebnd - hist["energy"][0]) / hist["energy"][0]}
+    if "fp32" in runs and "fp64" in runs:
+        (a, ha), (b, hb) = runs["fp32"], runs["fp64"]
+        mwa, mwb = np.array(ha["mixing_width"]), np.array(hb["mixing_width"])
+        out["fp32_vs_fp64"] = {
+            "rel_l1_rho_final": rel_l1(interior(a)[0], interior(b)[0]),
+            "mixing_width_max_abs_diff_over_peak": float(np.max(np.abs(mwa - mwb)) / max(np.max(np.abs(mwb)), 1e-300)),
+        }
+    return out
+
+
+# ------------------------------------------------------------------ Brio-Wu
+def brio_wu(nx: int = 800, precision: str = "fp64", cfl: float = 0.3, limiter: str = "vanleer") -> dict:
+    cfg = Config(nx=nx, ny=4, x_min=0.0, x_max=1.0, y_min=0.0, y_max=0.05, t_end=0.1, cfl=cfl, gamma=2.0,
+                 B_transverse=0.0, powell_source=False, use_char_bc=False, bc_x_type="extrapolation",
+                 bc_y_type="periodic", precision=precision, limiter=limiter)
+    s = MHDSolver(cfg)
+    s.set_primitive(ic.brio_wu(s))
+    wall = _timed_advance(s, 0.1)
+    from .physics import cons_to_prim
+    W = cons_to_prim(s.U, cfg.gamma).double().cpu().numpy()
+    rho, by, vx = W[0, 2:-2, 2], W[5, 2:-2, 2], W[1, 2:-2, 2]
+    checks = {"rho_min_in_(0.1,0.2)": bool(0.1 < rho.min() < 0.2), "rho_max_in_(0.9,1.05)": bool(0.9 < rho.max() < 1.05),
+              "levels>10": bool(len(np.unique(np.round(rho, 2))) > 10), "By_sign_change": bool(np.any(by[:-1] * by[1:] < 0)),
+              "rho_min<0.18": bool(rho.min() < 0.18), "vx_range>0.5": bool(vx.max() - vx.min() > 0.5)}
+    return {"case": "brio_wu", "nx": nx, "cfl": cfl, "limiter": limiter, "precision": precision, "steps": s.step,
+            "wall_s": wall, "rho_range": [float(rho.min()), float(rho.max())], "checks": checks,
+            "passed": all(checks.values())}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["orszag_tang", "cp_alfven", "shock_interface", "brio_wu"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--nx", type=int, default=2048)
+    ap.add_argument("--ny", type=int, default=512)
+    ap.add_argument("--t-end", type=float, default=None)
+    ap.add_argument("--sizes", type=int, nargs="*", default=[32, 64, 128, 256, 512, 1024])
+    ap.add_argument("--precision", default=None)
+    ap.add_argument("--cfl", type=float, default=None)
+    ap.add_argument("--limiter", default="vanleer")
+    a = ap.parse_args(argv)
+    precs = (a.precision,) if a.precision else ("fp32", "fp64")
+    if a.case == "orszag_tang":
+        r = orszag_tang(a.n, a.t_end or 0.5, precs)
+    elif a.case == "cp_alfven":
+        r = {p: cp_alfven(tuple(a.sizes), p) for p in precs}
+    elif a.case == "shock_interface":
+        r = shock_interface(a.nx, a.ny, a.t_end or 3.0, precs)
+    else:
+        r = {p: brio_wu(precision=p, cfl=a.cfl or 0.3, limiter=a.limiter) for p in precs}
+    print(json.dumps(r))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

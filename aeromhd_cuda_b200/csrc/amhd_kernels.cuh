@@ -316,10 +316,19 @@ __device__ __forceinline__ bool rk_stage_tile(const StageParams &p, TileSmem<R, 
                     out[v] = b0 + dtr * rhs[v];
                 } else {
                     R us = uin[v * vs + gi];
-                    if (STAGE == 2)
-                        out[v] = R(0.75) * b0 + R(0.25) * (us + dtr * rhs[v]);
-                    else
-                        out[v] = R(1.0 / 3.0) * b0 + R(2.0 / 3.0) * (us + dtr * rhs[v]);
+                    if constexpr (kFast<R>) {
+                        // increment form of the same combination: in float32 the weights
+                        // 1/3 and 2/3 round to a sum of 1 + 3e-8, which as a weighted
+                        // average would scale the state every step (a mass drift);
+                        // U0 + w ((U* - U0) + dt R) has no such bias (U* - U0 is exact)
+                        const float w = STAGE == 2 ? 0.25f : float(2.0 / 3.0);
+                        out[v] = b0 + w * ((us - b0) + dtr * rhs[v]);
+                    } else {
+                        if (STAGE == 2)
+                            out[v] = R(0.75) * b0 + R(0.25) * (us + dtr * rhs[v]);
+                        else
+                            out[v] = R(1.0 / 3.0) * b0 + R(2.0 / 3.0) * (us + dtr * rhs[v]);
+                    }
                 }
             }
             // enforce_scalar_bounds, solver.py:199-204
