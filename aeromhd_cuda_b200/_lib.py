@@ -84,7 +84,26 @@ _SIGS = {
     "amhd_ensemble_advance": ([_P, _I32, _P, _P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _I32, _P, _P], _c.c_int),
     "amhd_ensemble_tensormaps": ([_P, _I32, _I32, _I32, _P, _P, _P, _P], _c.c_int),
     "amhd_set_tma": ([_I32], _c.c_int),
+    "amhd_ensemble_continue": ([_P, _P, _I32, _I32, _P, _P, _D, _P], _c.c_int),
     "amhd_ensemble_init": ([_P, _P, _I32, _I32, _P, _P, _D, _I64, _P], _c.c_int),
+    "amhd_nn_last_error": ([], _c.c_char_p),
+    "amhd_nn_gemm": ([_I32, _I32, _I32, _I32, _I32, _P, _I32, _P, _I32, _P, _I32, _c.c_float, _c.c_float, _I32, _P],
+                     _c.c_int),
+    "amhd_nn_im2col3": ([_P, _I32, _I32, _I32, _I32, _P, _P], _c.c_int),
+    "amhd_nn_col2im3": ([_P, _I32, _I32, _I32, _I32, _P, _P], _c.c_int),
+    "amhd_nn_cast_bf16": ([_P, _P, _I64, _P], _c.c_int),
+    "amhd_nn_bias_act": ([_P, _P, _I32, _I64, _I32, _P], _c.c_int),
+    "amhd_nn_relu_bwd": ([_P, _P, _I64, _P], _c.c_int),
+    "amhd_nn_bias_grad": ([_P, _I32, _I64, _P, _P], _c.c_int),
+    "amhd_nn_pool2": ([_P, _I32, _I32, _I32, _P, _I32, _P], _c.c_int),
+    "amhd_nn_up2": ([_P, _I32, _I32, _I32, _P, _I32, _P], _c.c_int),
+    "amhd_nn_axpy": ([_P, _P, _c.c_float, _I64, _P], _c.c_int),
+    "amhd_nn_mse": ([_P, _P, _I64, _P, _P, _P], _c.c_int),
+    "amhd_nn_adam": ([_P, _P, _P, _P, _P, _I64, _c.c_float, _c.c_float, _c.c_float, _c.c_float, _I32, _c.c_float, _P],
+                     _c.c_int),
+    "amhd_nn_restrict": ([_c.POINTER(Grid), _P, _I32, _P, _I64, _I32, _I32, _P], _c.c_int),
+    "amhd_nn_pack": ([_c.POINTER(Grid), _P, _P, _P, _P, _I64, _I32, _P], _c.c_int),
+    "amhd_nn_apply": ([_c.POINTER(Grid), _P, _P, _P, _I64, _I32, _P], _c.c_int),
 }
 
 _lib = None
@@ -118,7 +137,10 @@ def check(rc: int) -> None:
 
 
 def call(name: str, *args) -> None:
-    check(getattr(lib(), name)(*args))
+    rc = getattr(lib(), name)(*args)
+    if rc != AMHD_OK and name.startswith("amhd_nn_"):
+        raise AmhdError(rc, lib().amhd_nn_last_error().decode(errors="replace"))
+    check(rc)
 
 
 def padded_layout(nx: int, ny: int, dtype_code: int):

@@ -29,6 +29,7 @@ UNITS = {
     "amhd_f64.cu": ["-fmad=false"],
     "amhd_f32.cu": [],
     "amhd_capi.cu": [],
+    "amhd_nn.cu": [],
 }
 
 

@@ -17,8 +17,11 @@ behaviour is what you get when you leave them alone):
                    "shock_interface" (a uniform-Bx shocked interface, see
                    ``initial_conditions.shock_interface``).
 ``bx0``, ``shock_x``, ``perturbation_shape``, ``interface_cells``,
-``noise_amp``, ``seed``, ``b1``, ``b_mode``
-                   parameters of the "shock_interface" initial condition.
+``noise_amp``, ``seed``, ``b1``, ``b_mode``, ``ic_frame``
+                   parameters of the "shock_interface" initial condition
+                   (``ic_frame`` "lab": unshocked gas at rest; "post_shock":
+                   the frame of the shocked gas, which keeps the mixing layer
+                   near where the shock meets it).
 """
 from __future__ import annotations
 
@@ -111,6 +114,7 @@ class Config:
     interface_cells: Optional[float] = None
     noise_amp: float = 0.0
     seed: int = 0
+    ic_frame: str = "lab"
 
     @property
     def dx(self) -> float:

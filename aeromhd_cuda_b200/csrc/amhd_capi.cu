@@ -709,6 +709,25 @@ int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst
     return AMHD_OK;
 }
 
+int amhd_ensemble_continue(const amhd_instance *inst_host, const amhd_instance *inst_dev, int32_t n_inst,
+                           int32_t dtype, void *U, amhd_control *ctl_dev, double t_end, void *stream)
+{
+    if (!inst_host || !inst_dev || !U || !ctl_dev || n_inst <= 0) return fail(AMHD_ERR_ARG, "bad ensemble arguments");
+    cudaStream_t s = S(stream);
+    const size_t es = elem_size(dtype);
+    CK(launch_control_retarget(ctl_dev, n_inst, t_end, s));
+    for (int k = 0; k < n_inst; ++k) {
+        const amhd_grid *g = &inst_host[k].grid;
+        if (int e = check_grid(g)) return fail(e, "instance %d: %s", k, g_err.c_str());
+        void *Uk = static_cast<char *>(U) + (size_t)inst_host[k].offset * es;
+        CK(run_dt_reduce(g, Uk, 0, ctl_dev + k, s));
+    }
+    amhd_instance dummy;
+    memset(&dummy, 0, sizeof dummy);
+    CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 0, 0, s));
+    return AMHD_OK;
+}
+
 int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev,
                           const int32_t *tile_order_dev, int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U,
                           void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas,

@@ -81,6 +81,22 @@ cudaError_t launch_control_resume(amhd_control *ctl, int n, double snap_t, cudaS
     return cudaGetLastError();
 }
 
+__global__ void control_retarget_kernel(amhd_control *ctl, int n, double t_end)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    ctl[k].t_end = t_end;
+    ctl[k].active = 1;
+    ctl[k].flags &= ~(AMHD_FLAG_DT_TINY | AMHD_FLAG_PAUSED);
+    for (int q = 0; q < 4; ++q) ctl[k].red[q] = 0ull;
+}
+
+cudaError_t launch_control_retarget(amhd_control *ctl, int n, double t_end, cudaStream_t s)
+{
+    control_retarget_kernel<<<(n + 127) / 128, 128, 0, s>>>(ctl, n, t_end);
+    return cudaGetLastError();
+}
+
 int device_sm_count()
 {
     int dev = 0, n = 0;

@@ -132,8 +132,8 @@ __device__ __forceinline__ void side_flux(const FSide &s, float bxf, float bx2, 
     f[9] = mx * s.c;
 }
 
-// star state of one side (physics.py:122-154), reciprocals shared
-__device__ __forceinline__ void star(FSide &s, float S, float SM, float ptS, float bxf, float bx2, float eps_rel)
+// star-state transverse quantities of one side (physics.py:122-146), reciprocals shared
+__device__ __forceinline__ void star(FSide &s, float S, float SM, float bxf, float bx2, float eps_rel)
 {
     float dsm = S - SM;
     if (fabsf(dsm) < 1e-14f) dsm = 1e-14f;
@@ -151,6 +151,17 @@ __device__ __forceinline__ void star(FSide &s, float S, float SM, float ptS, flo
     const float tb = (rds * s.dS - bx2) * idn;
     s.bys = s.by * tb;
     s.bzs = s.bz * tb;
+}
+
+// total energy, v.B and their star values (physics.py:146-154): only the side
+// whose fan holds x/t = 0 needs them
+__device__ __forceinline__ void side_energy(FSide &s, float bxf, float igm1)
+{
+    s.vb = s.vx * bxf + s.vy * s.by + s.vz * s.bz;
+    s.e = s.p * igm1 + 0.5f * s.rho * (s.vx * s.vx + s.vy * s.vy + s.vz * s.vz) + 0.5f * s.bm2;
+}
+__device__ __forceinline__ void star_energy(FSide &s, float S, float SM, float ptS, float bxf)
+{
     s.vbs = SM * bxf + s.vys * s.bys + s.vzs * s.bzs;
     s.es = ((S - s.vx) * s.e - s.pt * s.vx + ptS * SM + bxf * (s.vb - s.vbs)) * s.idsm;
 }
@@ -188,21 +199,15 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
     if (SM > SR - 1e-14f) SM = SR - 1e-14f;
     const float ptS = L.pt + rdl * (SM - L.vx);
 
-    L.vb = L.vx * bxf + L.vy * L.by + L.vz * L.bz;
-    R.vb = R.vx * bxf + R.vy * R.by + R.vz * R.bz;
-    L.e = L.p * igm1 + 0.5f * L.rho * (L.vx * L.vx + L.vy * L.vy + L.vz * L.vz) + 0.5f * L.bm2;
-    R.e = R.p * igm1 + 0.5f * R.rho * (R.vx * R.vx + R.vy * R.vy + R.vz * R.vz) + 0.5f * R.bm2;
-    if (SL >= 0.f) {
-        side_flux(L, bxf, bx2, psif, ch, f);
-        return;
-    }
-    if (SR <= 0.f) {
-        side_flux(R, bxf, bx2, psif, ch, f);
+    if (SL >= 0.f || SR <= 0.f) {  // supersonic: the upwind side's flux (only without GLM)
+        FSide &U = SL >= 0.f ? L : R;
+        side_energy(U, bxf, igm1);
+        side_flux(U, bxf, bx2, psif, ch, f);
         return;
     }
     const float eps_rel = 1e-8f * fmaxf(fabsf(ptS), 1.f);
-    star(L, SL, SM, ptS, bxf, bx2, eps_rel);
-    star(R, SR, SM, ptS, bxf, bx2, eps_rel);
+    star(L, SL, SM, bxf, bx2, eps_rel);
+    star(R, SR, SM, bxf, bx2, eps_rel);
     const float abx = fabsf(bxf);
     float SAL = SM - abx * fminf(L.isq, 1e14f);
     float SAR = SM + abx * fminf(R.isq, 1e14f);
@@ -211,8 +216,10 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
 
     const bool left = (SAL >= 0.f) || (SM >= 0.f);
     const bool dstar = left ? !(SAL >= 0.f) : (SAR >= 0.f);
-    const FSide &K = left ? L : R;
+    FSide &K = left ? L : R;
     const float S = left ? SL : SR;
+    side_energy(K, bxf, igm1);
+    star_energy(K, S, SM, ptS, bxf);
     side_flux(K, bxf, bx2, psif, ch, f);
     // + S (U* - U)
     f[0] += S * (K.rs - K.rho);
@@ -233,7 +240,7 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
         const float byds = (L.sq * R.bys + R.sq * L.bys + sqq * (R.vys - L.vys)) * idds;
         const float bzds = (L.sq * R.bzs + R.sq * L.bzs + sqq * (R.vzs - L.vzs)) * idds;
         const float vbds = SM * bxf + vyds * byds + vzds * bzds;
-        const float eds = left ? (L.es - L.sq * (L.vbs - vbds) * sbx) : (R.es + R.sq * (R.vbs - vbds) * sbx);
+        const float eds = left ? (K.es - K.sq * (K.vbs - vbds) * sbx) : (K.es + K.sq * (K.vbs - vbds) * sbx);
         const float SA = left ? SAL : SAR;
         // + SA (U** - U*)
         f[2] += SA * K.rs * (vyds - K.vys);

@@ -65,6 +65,7 @@ struct Launch {
 int encode_state_map(CUtensorMap *map, const void *base, int dtype, int pitch, int64_t var_stride, int tile_x);
 
 cudaError_t launch_control_resume(amhd_control *ctl, int n, double snap_t, cudaStream_t s);
+cudaError_t launch_control_retarget(amhd_control *ctl, int n, double t_end, cudaStream_t s);
 cudaError_t launch_diag_finish(const amhd_grid &g, double x0, const double *rows, double *out, cudaStream_t s);
 int device_sm_count();
 

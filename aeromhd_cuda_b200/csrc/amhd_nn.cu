@@ -1,0 +1,577 @@
+// amhd_nn.cu -- kernels of the learned coarse-grid corrector: a BF16
+// tensor-core GEMM (mma.sync m16n8k16, FP32 accumulation) that carries every
+// convolution (im2col form), and the element-wise, pooling, loss and Adam
+// kernels of its training and inference.
+//
+// Activations are FP32 in [C][B*H*W] layout (channel-major: the output of a
+// GEMM W[Cout][K] x col[K][N] is the next layer's input as is); GEMM operands
+// are BF16, weights keep an FP32 master copy for Adam.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+
+#include "aeromhd.h"
+
+namespace {
+
+thread_local std::string g_nn_err;
+
+int nn_fail(int code, const char *fmt, ...)
+{
+    char buf[256];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_nn_err = buf;
+    return code;
+}
+
+#define NNCK(call)                                                                                   \
+    do {                                                                                             \
+        cudaError_t e__ = (call);                                                                    \
+        if (e__ != cudaSuccess) return nn_fail(AMHD_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e__)); \
+    } while (0)
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+inline int blocks_for(int64_t n, int threads = 256)
+{
+    int64_t b = (n + threads - 1) / threads;
+    if (b > 148 * 32) b = 148 * 32;
+    return (int)(b < 1 ? 1 : b);
+}
+
+using bf16 = __nv_bfloat16;
+
+// ---------------------------------------------------------------------------
+// GEMM: C[M][N] = alpha * op(A) op(B) (+ beta * C), op(A) = A (row-major
+// [M][K], lda) or A^T (A stored [K][M]); op(B) = B ([K][N]) or B^T (B stored
+// [N][K]).  64x64x32 CTA tiles, 4 warps of 32x32, split-K over gridDim.z
+// (then the partial products are added atomically into C, which the caller
+// has scaled by beta beforehand).
+// ---------------------------------------------------------------------------
+constexpr int GBM = 64, GBN = 64, GBK = 32, GPAD = 8;
+
+__device__ __forceinline__ void mma_bf16(float d[4], const uint32_t a[4], const uint32_t b[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(128) gemm_bf16_kernel(int transA, int transB, int M, int N, int K, const bf16 *A,
+                                                        int lda, const bf16 *B, int ldb, float *C, int ldc,
+                                                        float alpha, float beta, int k_per_split)
+{
+    __shared__ __align__(16) bf16 As[GBM][GBK + GPAD];
+    __shared__ __align__(16) bf16 Bs[GBN][GBK + GPAD];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int m0 = blockIdx.y * GBM, n0 = blockIdx.x * GBN;
+    const int kbeg = blockIdx.z * k_per_split;
+    const int kend = min(K, kbeg + k_per_split);
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
+    const bf16 zero = __float2bfloat16(0.f);
+
+    for (int k0 = kbeg; k0 < kend; k0 += GBK) {
+        for (int e = tid; e < GBM * GBK; e += 128) {
+            int mm, kk;
+            if (!transA) {
+                mm = e / GBK;
+                kk = e % GBK;
+            } else {
+                kk = e / GBM;
+                mm = e % GBM;
+            }
+            const int gm = m0 + mm, gk = k0 + kk;
+            bf16 v = zero;
+            if (gm < M && gk < kend) v = transA ? A[(int64_t)gk * lda + gm] : A[(int64_t)gm * lda + gk];
+            As[mm][kk] = v;
+        }
+        for (int e = tid; e < GBN * GBK; e += 128) {
+            int nn, kk;
+            if (!transB) {
+                kk = e / GBN;
+                nn = e % GBN;
+            } else {
+                nn = e / GBK;
+                kk = e % GBK;
+            }
+            const int gn = n0 + nn, gk = k0 + kk;
+            bf16 v = zero;
+            if (gn < N && gk < kend) v = transB ? B[(int64_t)gn * ldb + gk] : B[(int64_t)gk * ldb + gn];
+            Bs[nn][kk] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < GBK; ks += 16) {
+            uint32_t a[2][4], b[4][2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+                const int r = wm + mi * 16 + g;
+                a[mi][0] = *reinterpret_cast<const uint32_t *>(&As[r][ks + 2 * t4]);
+                a[mi][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][ks + 2 * t4]);
+                a[mi][2] = *reinterpret_cast<const uint32_t *>(&As[r][ks + 8 + 2 * t4]);
+                a[mi][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][ks + 8 + 2 * t4]);
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) {
+                const int c = wn + ni * 8 + g;
+                b[ni][0] = *reinterpret_cast<const uint32_t *>(&Bs[c][ks + 2 * t4]);
+                b[ni][1] = *reinterpret_cast<const uint32_t *>(&Bs[c][ks + 8 + 2 * t4]);
+            }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], a[mi], b[ni]);
+        }
+        __syncthreads();
+    }
+    const bool split = gridDim.z > 1;
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int row = m0 + wm + mi * 16 + g + (r >= 2 ? 8 : 0);
+                const int col = n0 + wn + ni * 8 + 2 * t4 + (r & 1);
+                if (row < M && col < N) {
+                    float *p = &C[(int64_t)row * ldc + col];
+                    const float v = alpha * acc[mi][ni][r];
+                    if (split)
+                        atomicAdd(p, v);
+                    else
+                        *p = (beta != 0.f) ? v + beta * (*p) : v;
+                }
+            }
+}
+
+__global__ void scale_kernel(float *C, int M, int N, int ldc, float beta)
+{
+    const int64_t n = (int64_t)M * N;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        float *p = &C[(k / N) * ldc + k % N];
+        *p = beta == 0.f ? 0.f : beta * *p;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// convolution helpers, activations [C][B][H][W] (FP32) / columns (BF16)
+// ---------------------------------------------------------------------------
+__global__ void im2col3_kernel(const float *X, int C, int B, int H, int W, bf16 *col)
+{
+    const int64_t N = (int64_t)B * H * W;
+    const int64_t total = (int64_t)C * 9 * N;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t n = k % N;
+        const int row = (int)(k / N);
+        const int c = row / 9, tap = row % 9, dy = tap / 3 - 1, dx = tap % 3 - 1;
+        const int w = (int)(n % W), h = (int)((n / W) % H);
+        const int64_t b = n / ((int64_t)H * W);
+        const int hh = h + dy, ww = w + dx;
+        float v = 0.f;
+        if (hh >= 0 && hh < H && ww >= 0 && ww < W) v = X[((int64_t)c * B + b) * H * W + (int64_t)hh * W + ww];
+        col[k] = __float2bfloat16(v);
+    }
+}
+
+// dX[c][b][h][w] = sum over taps of dcol[c*9+tap][output pixel that read (h,w) through that tap]
+__global__ void col2im3_kernel(const float *dcol, int C, int B, int H, int W, float *dX)
+{
+    const int64_t N = (int64_t)B * H * W;
+    const int64_t total = (int64_t)C * N;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int c = (int)(k / N);
+        const int64_t n = k % N;
+        const int w = (int)(n % W), h = (int)((n / W) % H);
+        const int64_t b = n / ((int64_t)H * W);
+        float s = 0.f;
+#pragma unroll
+        for (int tap = 0; tap < 9; ++tap) {
+            const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+            const int ho = h - dy, wo = w - dx;
+            if (ho >= 0 && ho < H && wo >= 0 && wo < W)
+                s += dcol[(int64_t)(c * 9 + tap) * N + (b * H + ho) * W + wo];
+        }
+        dX[k] = s;
+    }
+}
+
+__global__ void cast_bf16_kernel(const float *x, bf16 *y, int64_t n)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        y[k] = __float2bfloat16(x[k]);
+}
+
+__global__ void bias_act_kernel(float *Y, const float *bias, int C, int64_t N, int relu)
+{
+    const int64_t total = (int64_t)C * N;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        float v = Y[k] + bias[k / N];
+        Y[k] = relu ? fmaxf(v, 0.f) : v;
+    }
+}
+
+__global__ void relu_bwd_kernel(float *dY, const float *Y, int64_t n)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        if (!(Y[k] > 0.f)) dY[k] = 0.f;
+}
+
+// db[c] = sum_n dY[c][n]; one block per channel, fixed reduction order
+__global__ void bias_grad_kernel(const float *dY, int64_t N, float *db)
+{
+    __shared__ float red[256];
+    const int c = blockIdx.x;
+    float s = 0.f;
+    for (int64_t n = threadIdx.x; n < N; n += blockDim.x) s += dY[(int64_t)c * N + n];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) db[c] = red[0];
+}
+
+// 2x2 average pooling: X [C*B][H][W] -> Y [C*B][H/2][W/2]
+__global__ void pool2_kernel(const float *X, int CB, int H, int W, float *Y)
+{
+    const int h2 = H / 2, w2 = W / 2;
+    const int64_t total = (int64_t)CB * h2 * w2;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int w = (int)(k % w2), h = (int)((k / w2) % h2);
+        const int64_t p = k / ((int64_t)h2 * w2);
+        const float *x = X + p * H * W + (int64_t)(2 * h) * W + 2 * w;
+        Y[k] = 0.25f * (x[0] + x[1] + x[W] + x[W + 1]);
+    }
+}
+
+__global__ void pool2_bwd_kernel(const float *dY, int CB, int H, int W, float *dX)
+{
+    const int64_t total = (int64_t)CB * H * W;
+    const int h2 = H / 2, w2 = W / 2;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int w = (int)(k % W), h = (int)((k / W) % H);
+        const int64_t p = k / ((int64_t)H * W);
+        dX[k] = 0.25f * dY[p * h2 * w2 + (int64_t)(h / 2) * w2 + w / 2];
+    }
+}
+
+// nearest 2x upsampling: X [C*B][h][w] -> Y [C*B][2h][2w]
+__global__ void up2_kernel(const float *X, int CB, int h, int w, float *Y)
+{
+    const int H = 2 * h, W = 2 * w;
+    const int64_t total = (int64_t)CB * H * W;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(k % W), y = (int)((k / W) % H);
+        const int64_t p = k / ((int64_t)H * W);
+        Y[k] = X[p * h * w + (int64_t)(y / 2) * w + x / 2];
+    }
+}
+
+__global__ void up2_bwd_kernel(const float *dY, int CB, int h, int w, float *dX)
+{
+    const int64_t total = (int64_t)CB * h * w;
+    const int W = 2 * w;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(k % w), y = (int)((k / w) % h);
+        const int64_t p = k / ((int64_t)h * w);
+        const float *d = dY + p * 4 * h * w + (int64_t)(2 * y) * W + 2 * x;
+        dX[k] = d[0] + d[1] + d[W] + d[W + 1];
+    }
+}
+
+__global__ void axpy_kernel(float *y, const float *x, float a, int64_t n)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        y[k] += a * x[k];
+}
+
+// grad = 2 (pred - target) / n ; loss partials summed per block then atomically
+__global__ void mse_kernel(const float *pred, const float *target, int64_t n, float *grad, float *loss)
+{
+    __shared__ float red[256];
+    float s = 0.f;
+    const float inv = 2.f / (float)n;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const float d = pred[k] - target[k];
+        if (grad) grad[k] = inv * d;
+        s += d * d;
+    }
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && loss) atomicAdd(loss, red[0] / (float)n);
+}
+
+__global__ void adam_kernel(float *w, const float *g, float *m, float *v, bf16 *wb, int64_t n, float lr, float b1,
+                            float b2, float eps, float c1, float c2, float wd)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        const float gk = g[k] + wd * w[k];
+        const float mk = b1 * m[k] + (1.f - b1) * gk;
+        const float vk = b2 * v[k] + (1.f - b2) * gk * gk;
+        m[k] = mk;
+        v[k] = vk;
+        const float wk = w[k] - lr * (mk * c1) / (sqrtf(vk * c2) + eps);
+        w[k] = wk;
+        if (wb) wb[k] = __float2bfloat16(wk);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// solver <-> network data movement
+// ---------------------------------------------------------------------------
+// coarse interior cell (i, j) = mean of the fine interior cells [f i, f i + f) x [f j, f j + f)
+template <typename R>
+__global__ void restrict_kernel(const R *Uf, int pitch_f, int64_t vs_f, int nxc, int nyc, int f, float *out,
+                                int64_t out_vs, int b, int B)
+{
+    const int64_t total = (int64_t)10 * nxc * nyc;
+    const float inv = 1.f / (float)(f * f);
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(k % nyc), i = (int)((k / nyc) % nxc), v = (int)(k / ((int64_t)nxc * nyc));
+        double s = 0.0;
+        for (int a = 0; a < f; ++a)
+            for (int c = 0; c < f; ++c)
+                s += (double)Uf[v * vs_f + (int64_t)(2 + f * i + a) * pitch_f + 2 + f * j + c];
+        out[(int64_t)v * out_vs + ((int64_t)b * nxc + i) * nyc + j] = (float)(s * inv);
+    }
+}
+
+// pack a solver state's interior into the network input x[v][b][i][j] = (U - mean_v) / std_v
+template <typename R>
+__global__ void pack_kernel(const R *U, int pitch, int64_t vs, int nx, int ny, const float *mean, const float *istd,
+                            float *x, int64_t x_vs, int b)
+{
+    const int64_t total = (int64_t)10 * nx * ny;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(k % ny), i = (int)((k / ny) % nx), v = (int)(k / ((int64_t)nx * ny));
+        const float u = (float)U[v * vs + (int64_t)(i + 2) * pitch + j + 2];
+        x[(int64_t)v * x_vs + ((int64_t)b * nx + i) * ny + j] = (u - mean[v]) * istd[v];
+    }
+}
+
+// U_interior += scale_v * y[v][b][i][j] (the network's correction), then the caller refreshes ghosts
+template <typename R>
+__global__ void apply_kernel(R *U, int pitch, int64_t vs, int nx, int ny, const float *scale, const float *y,
+                             int64_t y_vs, int b)
+{
+    const int64_t total = (int64_t)10 * nx * ny;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(k % ny), i = (int)((k / ny) % nx), v = (int)(k / ((int64_t)nx * ny));
+        R *u = &U[v * vs + (int64_t)(i + 2) * pitch + j + 2];
+        *u = (R)((float)*u + scale[v] * y[(int64_t)v * y_vs + ((int64_t)b * nx + i) * ny + j]);
+    }
+}
+
+}  // namespace
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+const char *amhd_nn_last_error(void) { return g_nn_err.c_str(); }
+
+int amhd_nn_gemm(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K, const void *A, int32_t lda,
+                 const void *B, int32_t ldb, float *C, int32_t ldc, float alpha, float beta, int32_t splits,
+                 void *stream)
+{
+    if (M < 0 || N < 0 || K < 0 || !A || !B || !C) return nn_fail(AMHD_ERR_ARG, "bad gemm arguments");
+    if (M == 0 || N == 0) return AMHD_OK;
+    if (splits < 1) splits = 1;
+    int kps = (K + splits - 1) / splits;
+    kps = (kps + GBK - 1) / GBK * GBK;
+    if (kps < GBK) kps = GBK;
+    splits = K > 0 ? (K + kps - 1) / kps : 1;
+    cudaStream_t s = S(stream);
+    if (splits > 1 || K == 0) {
+        scale_kernel<<<blocks_for((int64_t)M * N), 256, 0, s>>>(C, M, N, ldc, beta);
+        NNCK(cudaGetLastError());
+        if (K == 0) return AMHD_OK;
+    }
+    dim3 grid((N + GBN - 1) / GBN, (M + GBM - 1) / GBM, splits);
+    gemm_bf16_kernel<<<grid, 128, 0, s>>>(transA, transB, M, N, K, static_cast<const bf16 *>(A), lda,
+                                          static_cast<const bf16 *>(B), ldb, C, ldc, alpha,
+                                          splits > 1 ? 0.f : beta, kps);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_im2col3(const float *X, int32_t C, int32_t B, int32_t H, int32_t W, void *col, void *stream)
+{
+    if (!X || !col || C <= 0 || B <= 0 || H <= 0 || W <= 0) return nn_fail(AMHD_ERR_ARG, "bad im2col arguments");
+    im2col3_kernel<<<blocks_for((int64_t)C * 9 * B * H * W), 256, 0, S(stream)>>>(X, C, B, H, W,
+                                                                                 static_cast<bf16 *>(col));
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_col2im3(const float *dcol, int32_t C, int32_t B, int32_t H, int32_t W, float *dX, void *stream)
+{
+    if (!dcol || !dX || C <= 0 || B <= 0 || H <= 0 || W <= 0) return nn_fail(AMHD_ERR_ARG, "bad col2im arguments");
+    col2im3_kernel<<<blocks_for((int64_t)C * B * H * W), 256, 0, S(stream)>>>(dcol, C, B, H, W, dX);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_cast_bf16(const float *x, void *y, int64_t n, void *stream)
+{
+    if (n < 0 || (n && (!x || !y))) return nn_fail(AMHD_ERR_ARG, "bad cast arguments");
+    if (n) cast_bf16_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(x, static_cast<bf16 *>(y), n);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_bias_act(float *Y, const float *bias, int32_t C, int64_t N, int32_t relu, void *stream)
+{
+    if (!Y || !bias || C <= 0 || N < 0) return nn_fail(AMHD_ERR_ARG, "bad bias arguments");
+    bias_act_kernel<<<blocks_for((int64_t)C * N), 256, 0, S(stream)>>>(Y, bias, C, N, relu);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_relu_bwd(float *dY, const float *Y, int64_t n, void *stream)
+{
+    if (!dY || !Y || n < 0) return nn_fail(AMHD_ERR_ARG, "bad relu arguments");
+    relu_bwd_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(dY, Y, n);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_bias_grad(const float *dY, int32_t C, int64_t N, float *db, void *stream)
+{
+    if (!dY || !db || C <= 0 || N <= 0) return nn_fail(AMHD_ERR_ARG, "bad bias-grad arguments");
+    bias_grad_kernel<<<C, 256, 0, S(stream)>>>(dY, N, db);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_pool2(const float *X, int32_t CB, int32_t H, int32_t W, float *Y, int32_t backward, void *stream)
+{
+    if (!X || !Y || CB <= 0 || H < 2 || W < 2 || (H & 1) || (W & 1)) return nn_fail(AMHD_ERR_ARG, "bad pool arguments");
+    if (backward)
+        pool2_bwd_kernel<<<blocks_for((int64_t)CB * H * W), 256, 0, S(stream)>>>(X, CB, H, W, Y);
+    else
+        pool2_kernel<<<blocks_for((int64_t)CB * H * W / 4), 256, 0, S(stream)>>>(X, CB, H, W, Y);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_up2(const float *X, int32_t CB, int32_t h, int32_t w, float *Y, int32_t backward, void *stream)
+{
+    if (!X || !Y || CB <= 0 || h <= 0 || w <= 0) return nn_fail(AMHD_ERR_ARG, "bad upsample arguments");
+    if (backward)
+        up2_bwd_kernel<<<blocks_for((int64_t)CB * h * w), 256, 0, S(stream)>>>(X, CB, h, w, Y);
+    else
+        up2_kernel<<<blocks_for((int64_t)CB * 4 * h * w), 256, 0, S(stream)>>>(X, CB, h, w, Y);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_axpy(float *y, const float *x, float a, int64_t n, void *stream)
+{
+    if (!y || !x || n < 0) return nn_fail(AMHD_ERR_ARG, "bad axpy arguments");
+    if (n) axpy_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(y, x, a, n);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_mse(const float *pred, const float *target, int64_t n, float *grad, float *loss, void *stream)
+{
+    if (!pred || !target || n <= 0) return nn_fail(AMHD_ERR_ARG, "bad mse arguments");
+    mse_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(pred, target, n, grad, loss);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_adam(float *w, const float *g, float *m, float *v, void *w_bf16, int64_t n, float lr, float beta1,
+                 float beta2, float eps, int32_t t, float weight_decay, void *stream)
+{
+    if (!w || !g || !m || !v || n < 0 || t < 1) return nn_fail(AMHD_ERR_ARG, "bad adam arguments");
+    const float c1 = 1.f / (1.f - powf(beta1, (float)t)), c2 = 1.f / (1.f - powf(beta2, (float)t));
+    if (n) adam_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(w, g, m, v, static_cast<bf16 *>(w_bf16), n, lr, beta1,
+                                                             beta2, eps, c1, c2, weight_decay);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_restrict(const amhd_grid *fine, const void *Uf, int32_t factor, float *out, int64_t out_vs, int32_t b,
+                     int32_t B, void *stream)
+{
+    if (!fine || !Uf || !out || factor < 1 || fine->nx % factor || fine->ny % factor)
+        return nn_fail(AMHD_ERR_ARG, "bad restriction arguments");
+    const int nxc = fine->nx / factor, nyc = fine->ny / factor;
+    const int64_t n = (int64_t)10 * nxc * nyc;
+    if (fine->dtype == AMHD_F64)
+        restrict_kernel<double><<<blocks_for(n), 256, 0, S(stream)>>>(static_cast<const double *>(Uf), fine->pitch,
+                                                                       fine->var_stride, nxc, nyc, factor, out, out_vs,
+                                                                       b, B);
+    else
+        restrict_kernel<float><<<blocks_for(n), 256, 0, S(stream)>>>(static_cast<const float *>(Uf), fine->pitch,
+                                                                      fine->var_stride, nxc, nyc, factor, out, out_vs,
+                                                                      b, B);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_pack(const amhd_grid *g, const void *U, const float *mean, const float *istd, float *x, int64_t x_vs,
+                 int32_t b, void *stream)
+{
+    if (!g || !U || !mean || !istd || !x) return nn_fail(AMHD_ERR_ARG, "bad pack arguments");
+    const int64_t n = (int64_t)10 * g->nx * g->ny;
+    if (g->dtype == AMHD_F64)
+        pack_kernel<double><<<blocks_for(n), 256, 0, S(stream)>>>(static_cast<const double *>(U), g->pitch,
+                                                                   g->var_stride, g->nx, g->ny, mean, istd, x, x_vs, b);
+    else
+        pack_kernel<float><<<blocks_for(n), 256, 0, S(stream)>>>(static_cast<const float *>(U), g->pitch,
+                                                                  g->var_stride, g->nx, g->ny, mean, istd, x, x_vs, b);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_apply(const amhd_grid *g, void *U, const float *scale, const float *y, int64_t y_vs, int32_t b,
+                  void *stream)
+{
+    if (!g || !U || !scale || !y) return nn_fail(AMHD_ERR_ARG, "bad apply arguments");
+    const int64_t n = (int64_t)10 * g->nx * g->ny;
+    if (g->dtype == AMHD_F64)
+        apply_kernel<double><<<blocks_for(n), 256, 0, S(stream)>>>(static_cast<double *>(U), g->pitch, g->var_stride,
+                                                                    g->nx, g->ny, scale, y, y_vs, b);
+    else
+        apply_kernel<float><<<blocks_for(n), 256, 0, S(stream)>>>(static_cast<float *>(U), g->pitch, g->var_stride,
+                                                                   g->nx, g->ny, scale, y, y_vs, b);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

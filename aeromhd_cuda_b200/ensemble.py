@@ -227,6 +227,11 @@ class Ensemble:
         _lib.call("amhd_ensemble_init", ctypes.byref(self._table), self.inst_dev.data_ptr(), self.n, self.code,
                   self.U.data_ptr(), self.ctl.data_ptr(), t_end, int(max_steps), stream_ptr())
 
+    def continue_to(self, t_end: float):
+        """Keep every instance's t and step; run on to a new end time."""
+        _lib.call("amhd_ensemble_continue", ctypes.byref(self._table), self.inst_dev.data_ptr(), self.n, self.code,
+                  self.U.data_ptr(), self.ctl.data_ptr(), float(t_end), stream_ptr())
+
     def _advance_eager(self, n: int):
         _lib.call("amhd_ensemble_advance", self.inst_dev.data_ptr(), self.n, self.tile_inst.data_ptr(),
                   self.tile_order.data_ptr(), self.n_tiles, self.code, self.tile_x, self.U.data_ptr(),

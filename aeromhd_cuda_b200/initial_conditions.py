@@ -105,6 +105,8 @@ def shock_interface(solver):
     W[iPR] = _sel(post, p2, p1)
     W[iBX] = cfg.bx0 + cfg.b1 * torch.sin(2 * np.pi * cfg.b_mode * yy / ly)
     W[iCLR] = _sel(post, 0.0, phi)
+    if cfg.ic_frame == "post_shock":
+        W[iVX] -= vx2
     return W, rh
 
 

@@ -261,6 +261,12 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
                           const int32_t *tile_order_dev, int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U,
                           void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas,
                           const void *tmaps_dev, void *stream);
+/* Continue every instance from its current t and step to a new t_end: dt,
+ * ch and the loop flags are recomputed from the current states (as
+ * amhd_ensemble_init does, but keeping t, step, flags and the boundary
+ * energy).  Asynchronous.  No counterpart in the reference. */
+int amhd_ensemble_continue(const amhd_instance *inst_host, const amhd_instance *inst_dev, int32_t n_inst,
+                           int32_t dtype, void *U, amhd_control *ctl_dev, double t_end, void *stream);
 /* Fill maps_host (3 * n_inst CUtensorMap of 128 bytes: U, U1, U2 per
  * instance) for amhd_ensemble_advance; copy it to device memory (64-byte
  * aligned) before use.  No counterpart in the reference. */
@@ -271,6 +277,53 @@ int amhd_ensemble_tensormaps(const amhd_instance *inst_host, int32_t n_inst, int
 int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst_dev, int32_t n_inst,
                        int32_t dtype, void *U, amhd_control *ctl_dev, double t_end, int64_t max_steps,
                        void *stream);
+
+/* ---- learned coarse-grid corrector ------------------------------------- */
+/* Kernels of the convolutional corrector's training and inference; none has a
+ * counterpart in the reference.  Activations are float32 [C][B*H*W]
+ * (channel-major), GEMM operands bfloat16, accumulation float32. */
+const char *amhd_nn_last_error(void);
+/* C[M][N] = alpha op(A) op(B) + beta C on the BF16 tensor cores (mma.sync
+ * m16n8k16, FP32 accumulate).  op(A) = A ([M][K], lda) or, transA, A^T (A
+ * stored [K][M]); op(B) = B ([K][N]) or, transB, B^T (B stored [N][K]).
+ * splits > 1 divides K over CTAs and accumulates atomically. */
+int amhd_nn_gemm(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K, const void *A, int32_t lda,
+                 const void *B, int32_t ldb, float *C, int32_t ldc, float alpha, float beta, int32_t splits,
+                 void *stream);
+/* 3x3 zero-padded convolution columns: col[c*9+tap][b,h,w] (BF16) of X[c][b][h][w] */
+int amhd_nn_im2col3(const float *X, int32_t C, int32_t B, int32_t H, int32_t W, void *col, void *stream);
+/* adjoint of im2col3: dX[c][b][h][w] = sum over taps of dcol (gather, fixed order) */
+int amhd_nn_col2im3(const float *dcol, int32_t C, int32_t B, int32_t H, int32_t W, float *dX, void *stream);
+int amhd_nn_cast_bf16(const float *x, void *y, int64_t n, void *stream);
+/* Y[c][n] = act(Y[c][n] + bias[c]), act = ReLU if relu else identity */
+int amhd_nn_bias_act(float *Y, const float *bias, int32_t C, int64_t N, int32_t relu, void *stream);
+/* dY *= (Y > 0) */
+int amhd_nn_relu_bwd(float *dY, const float *Y, int64_t n, void *stream);
+/* db[c] = sum_n dY[c][n] */
+int amhd_nn_bias_grad(const float *dY, int32_t C, int64_t N, float *db, void *stream);
+/* 2x2 average pooling of [CB][H][W] (backward: its adjoint into [CB][H][W]) */
+int amhd_nn_pool2(const float *X, int32_t CB, int32_t H, int32_t W, float *Y, int32_t backward, void *stream);
+/* nearest 2x upsampling of [CB][h][w] (backward: its adjoint into [CB][h][w]) */
+int amhd_nn_up2(const float *X, int32_t CB, int32_t h, int32_t w, float *Y, int32_t backward, void *stream);
+/* y += a x */
+int amhd_nn_axpy(float *y, const float *x, float a, int64_t n, void *stream);
+/* grad = 2 (pred - target) / n (if grad), *loss += mean squared error (if loss) */
+int amhd_nn_mse(const float *pred, const float *target, int64_t n, float *grad, float *loss, void *stream);
+/* Adam with bias correction (step t >= 1) and decoupled-into-gradient weight
+ * decay; refreshes the BF16 copy w_bf16 (may be NULL) */
+int amhd_nn_adam(float *w, const float *g, float *m, float *v, void *w_bf16, int64_t n, float lr, float beta1,
+                 float beta2, float eps, int32_t t, float weight_decay, void *stream);
+/* factor x factor block average of a fine state's interior (float64 sums)
+ * into sample b of out[10][B][nx/f][ny/f] (plane stride out_vs) */
+int amhd_nn_restrict(const amhd_grid *fine, const void *Uf, int32_t factor, float *out, int64_t out_vs, int32_t b,
+                     int32_t B, void *stream);
+/* network input: x[v][b][i][j] = (U_interior - mean[v]) * istd[v] */
+int amhd_nn_pack(const amhd_grid *g, const void *U, const float *mean, const float *istd, float *x, int64_t x_vs,
+                 int32_t b, void *stream);
+/* corrector output applied: U_interior[v] += scale[v] * y[v][b][i][j]
+ * (ghost cells are left to amhd_apply_bc) */
+int amhd_nn_apply(const amhd_grid *g, void *U, const float *scale, const float *y, int64_t y_vs, int32_t b,
+                  void *stream);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,148 @@
+"""Corrector kernels on the GPU against float32 references: the BF16 GEMM in
+every transpose/split variant against a float matmul of the same BF16-rounded
+operands; the full network's output and every parameter gradient against the
+CPU autograd oracle (tests/nn_oracle.py); Adam against torch.optim.Adam; and
+the solver <-> network data movement."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def bf(t):
+    return t.to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("transA,transB", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K,splits", [(37, 91, 53, 1), (128, 300, 700, 4), (10, 4096, 288, 1), (64, 64, 5000, 7)])
+def test_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import stream_ptr
+    g = torch.Generator(device="cuda").manual_seed(M * N + K)
+    A = bf(torch.randn((K, M) if transA else (M, K), device="cuda", generator=g))
+    B = bf(torch.randn((N, K) if transB else (K, N), device="cuda", generator=g))
+    C = torch.randn((M, N), device="cuda", generator=g)
+    C0 = C.clone()
+    _lib.call("amhd_nn_gemm", transA, transB, M, N, K, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1],
+              C.data_ptr(), N, 0.5, 2.0, splits, stream_ptr())
+    opA = A.float().t() if transA else A.float()
+    opB = B.float().t() if transB else B.float()
+    ref = 0.5 * (opA.double() @ opB.double()) + 2.0 * C0.double()
+    err = float((C.double() - ref).abs().max() / ref.abs().max())
+    assert err < 2e-6, err
+
+
+def _net_and_oracle(H=32, W=16, B=2, seed=5):
+    import nn_oracle
+    from aeromhd_cuda_b200.corrector import Corrector, architecture, init_params
+    p = init_params(architecture(), seed)
+    # make the last layer non-trivial so that gradients are well conditioned
+    p["out"]["w"] *= 10.0
+    for v in p.values():
+        v["b"].normal_(0, 0.05, generator=torch.Generator().manual_seed(seed + 1))
+    # round weights to bf16 so both sides use identical operand values
+    for v in p.values():
+        v["w"] = v["w"].to(torch.bfloat16).float()
+    net = Corrector(H, W, params=p)
+    gen = torch.Generator().manual_seed(seed + 2)
+    x = torch.randn(B, 10, H, W, generator=gen).to(torch.bfloat16).float()
+    tgt = torch.randn(B, 10, H, W, generator=gen)
+    return net, p, x, tgt, nn_oracle
+
+
+def test_network_forward_and_gradients_match_cpu_oracle():
+    net, p, x, tgt, O = _net_and_oracle()
+    B, H, W = x.shape[0], x.shape[2], x.shape[3]
+    # oracle
+    leaf = {k: {"w": v["w"].clone().requires_grad_(True), "b": v["b"].clone().requires_grad_(True)}
+            for k, v in p.items()}
+    y_ref = O.forward(leaf, x)
+    loss_ref = ((y_ref - tgt) ** 2).mean()
+    loss_ref.backward()
+    # GPU kernels
+    xg = O.from_nchw(x).cuda()
+    tg = O.from_nchw(tgt).cuda()
+    y = net.forward(xg, B)
+    y_cpu = O.to_nchw(y.cpu(), B, H, W)
+    rel = float((y_cpu - y_ref.detach()).norm() / y_ref.detach().norm())
+    assert rel < 3e-2, rel
+    dout = torch.empty_like(y)
+    loss = torch.zeros(1, device="cuda")
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import stream_ptr
+    _lib.call("amhd_nn_mse", y.data_ptr(), tg.data_ptr(), y.numel(), dout.data_ptr(), loss.data_ptr(), stream_ptr())
+    assert abs(float(loss) - float(loss_ref)) / float(loss_ref) < 3e-2
+    net.backward(dout, B)
+    worst = {}
+    for s in net.specs:
+        gw = net.p[s.name]["gw"].cpu().reshape(leaf[s.name]["w"].shape)
+        gb = net.p[s.name]["gb"].cpu()
+        rw = leaf[s.name]["w"].grad
+        rb = leaf[s.name]["b"].grad
+        worst[s.name] = (float((gw - rw).norm() / rw.norm().clamp_min(1e-30)),
+                         float((gb - rb).norm() / rb.norm().clamp_min(1e-30)))
+    bad = {k: v for k, v in worst.items() if max(v) > 6e-2}
+    assert not bad, worst
+
+
+def test_adam_matches_torch_adam():
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import stream_ptr
+    g = torch.Generator().manual_seed(0)
+    w0 = torch.randn(1000, generator=g)
+    grads = [torch.randn(1000, generator=g) for _ in range(4)]
+    wr = w0.clone().requires_grad_(True)
+    opt = torch.optim.Adam([wr], lr=1e-2, betas=(0.9, 0.999), eps=1e-8)
+    w, m, v = w0.cuda(), torch.zeros(1000, device="cuda"), torch.zeros(1000, device="cuda")
+    for t, gr in enumerate(grads, 1):
+        wr.grad = gr.clone()
+        opt.step()
+        gg = gr.cuda()
+        _lib.call("amhd_nn_adam", w.data_ptr(), gg.data_ptr(), m.data_ptr(), v.data_ptr(), None, 1000, 1e-2, 0.9,
+                  0.999, 1e-8, t, 0.0, stream_ptr())
+    assert torch.allclose(w.cpu(), wr.detach(), atol=1e-6, rtol=1e-5)
+
+
+def test_restrict_pack_apply():
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import make_grid, padded_state, stream_ptr
+    f = 4
+    _, Uf = padded_state(64, 32, torch.float32)
+    Uf.copy_(torch.randn(Uf.shape, device="cuda"))
+    out = torch.empty((10, 16, 8), device="cuda")
+    _lib.call("amhd_nn_restrict", make_grid(Uf, 1.4), Uf.data_ptr(), f, out.data_ptr(), 128, 0, 1, stream_ptr())
+    ref = Uf[:, 2:-2, 2:-2].double().reshape(10, 16, 4, 8, 4).mean(dim=(2, 4))
+    assert torch.allclose(out.double(), ref, atol=1e-6)
+    _, Uc = padded_state(16, 8, torch.float64)
+    Uc.copy_(torch.randn(Uc.shape, device="cuda", dtype=torch.float64))
+    mean = torch.arange(10, device="cuda", dtype=torch.float32)
+    istd = torch.full((10,), 0.5, device="cuda")
+    x = torch.empty((10, 128), device="cuda")
+    g = make_grid(Uc, 1.4)
+    _lib.call("amhd_nn_pack", g, Uc.data_ptr(), mean.data_ptr(), istd.data_ptr(), x.data_ptr(), 128, 0, stream_ptr())
+    assert torch.allclose(x.double(), ((Uc[:, 2:-2, 2:-2] - mean.double().view(10, 1, 1)) * 0.5).reshape(10, 128),
+                          atol=1e-5)
+    before = Uc.clone()
+    y = torch.randn((10, 128), device="cuda")
+    scale = torch.linspace(1, 2, 10, device="cuda")
+    _lib.call("amhd_nn_apply", g, Uc.data_ptr(), scale.data_ptr(), y.data_ptr(), 128, 0, stream_ptr())
+    exp = before[:, 2:-2, 2:-2] + (scale.view(10, 1) * y).double().reshape(10, 16, 8)
+    assert torch.allclose(Uc[:, 2:-2, 2:-2], exp, atol=1e-5)
+    assert torch.equal(Uc[:, :2], before[:, :2])   # ghosts untouched
+
+
+def test_training_reduces_the_loss_on_a_fixed_batch():
+    from aeromhd_cuda_b200.corrector import Corrector
+    import nn_oracle as O
+    torch.manual_seed(0)
+    H, W, B = 32, 16, 4
+    x = torch.randn(B, 10, H, W)
+    tgt = 0.3 * torch.tanh(x.roll(1, dims=2))       # a smooth learnable map
+    net = Corrector(H, W, seed=2)
+    xg, tg = O.from_nchw(x).cuda(), O.from_nchw(tgt).cuda()
+    first = float(net.loss(xg, tg, B))
+    for _ in range(60):
+        net.train_step(xg, tg, B, lr=3e-3)
+    last = float(net.loss(xg, tg, B))
+    assert last < 0.5 * first, (first, last)
