@@ -95,8 +95,15 @@ class Normaliser:
         ts = T.transpose(0, 1).reshape(10, -1) if T.dim() == 4 else T.permute(2, 0, 1, 3, 4).reshape(10, -1)
         self.in_mean = xs.mean(1)
         self.in_std = xs.std(1).clamp_min(1e-6)
-        self.out_std = ts.std(1).clamp_min(1e-8)
-        self.out_max = (ts.abs().amax(1) / self.out_std)
+        tstd = ts.std(1)
+        # channels the fine solution never corrects (e.g. m_z, B_z of these runs) get no correction
+        self.active = tstd > 1e-7 * tstd.max().clamp_min(1e-30)
+        self.out_std = torch.where(self.active, tstd, torch.ones_like(tstd))
+        self.out_max = (ts.abs().amax(1) / self.out_std).clamp_min(1.0)
+
+    @property
+    def out_scale(self) -> torch.Tensor:
+        return torch.where(self.active, self.out_std, torch.zeros_like(self.out_std))
 
     def inputs(self, X: torch.Tensor) -> torch.Tensor:
         """[S][10][H][W] -> normalised [10][S*H*W]"""
@@ -119,7 +126,7 @@ def train(X: torch.Tensor, Y: torch.Tensor, train_seeds: Sequence[int], val_seed
     tva = T[:, list(val_seeds)].reshape(-1, 10, H, W)
     norm = Normaliser(tr, ttr)
     net = Corrector(H, W, seed=seed, device=X.device)
-    net.set_normalisation(norm.in_mean, norm.in_std, norm.out_std)
+    net.set_normalisation(norm.in_mean, norm.in_std, norm.out_scale)
     gen = torch.Generator(device="cpu").manual_seed(seed)
     hist = {"epoch": [], "train_loss": [], "val_loss": [], "wall_s": []}
     n = tr.shape[0]
@@ -198,13 +205,9 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], apply_every
                     ctl = e.controls()
                     steps = np.array([c.step for c in ctl])
                     due = np.nonzero((steps // apply_every > last // apply_every) & ~fallback)[0]
-                    for i in due:
-                        st = e.state(i)
-                        g = e._grid(i)
-                        ok = _apply_guarded(net, norm, st, g, corr_sigma)
-                        if not ok:
-                            fallback[i] = True
-                        _lib.call("amhd_apply_bc", g, ptr(st), stream_ptr())
+                    if len(due):
+                        ok = _apply_batch(net, norm, e, due, corr_sigma)
+                        fallback[due[~ok]] = True
                     last = steps
                     if len(due):
                         e.continue_to(ts)
@@ -253,24 +256,33 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], apply_every
     return out
 
 
-def _apply_guarded(net: Corrector, norm: Normaliser, st: torch.Tensor, g, corr_sigma: float) -> bool:
-    """Apply the correction unless it is non-finite or far outside the training range."""
+def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma: float) -> np.ndarray:
+    """One forward pass over the instances `idx`; each gets its correction unless it is
+    non-finite or far outside the training range (then it is marked for fallback).
+    Ghost cells are refreshed afterwards."""
     N = net.H * net.W
-    x = net._buf("eval.x", (10, N))
-    _lib.call("amhd_nn_pack", g, ptr(st), ptr(net.in_mean), ptr(net.in_istd), ptr(x), N, 0, stream_ptr())
-    y = net.forward(x, 1)
-    lim = (norm.out_max * corr_sigma).view(10, 1)
-    if not bool(torch.isfinite(y).all()) or bool((y.abs() > lim).any()):
-        return False
-    _lib.call("amhd_nn_apply", g, ptr(st), ptr(net.out_scale), ptr(y), N, 0, stream_ptr())
-    return True
+    B = len(idx)
+    x = net._buf("eval.x", (10, B * N))
+    for b, i in enumerate(idx):
+        _lib.call("amhd_nn_pack", e._grid(i), ptr(e.state(i)), ptr(net.in_mean), ptr(net.in_istd), ptr(x), B * N,
+                  int(b), stream_ptr())
+    y = net.forward(x, B)
+    lim = (norm.out_max * corr_sigma).view(10, 1, 1)
+    yb = y.view(10, B, N)
+    good = (torch.isfinite(yb).all(dim=2).all(dim=0) & (yb.abs() <= lim).all(dim=2).all(dim=0)).cpu().numpy()
+    for b, i in enumerate(idx):
+        g = e._grid(i)
+        if good[b]:
+            _lib.call("amhd_nn_apply", g, ptr(e.state(i)), ptr(net.out_scale), ptr(y), B * N, int(b), stream_ptr())
+        _lib.call("amhd_apply_bc", g, ptr(e.state(i)), stream_ptr())
+    return good
 
 
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--train-seeds", type=int, default=100)
     ap.add_argument("--test-seeds", type=int, default=64)
-    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--nyc", type=int, default=64)

@@ -72,7 +72,7 @@ def test_network_forward_and_gradients_match_cpu_oracle():
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200._tensors import stream_ptr
     _lib.call("amhd_nn_mse", y.data_ptr(), tg.data_ptr(), y.numel(), dout.data_ptr(), loss.data_ptr(), stream_ptr())
-    assert abs(float(loss) - float(loss_ref)) / float(loss_ref) < 3e-2
+    assert abs(float(loss) - float(loss_ref.detach())) / float(loss_ref.detach()) < 3e-2
     net.backward(dout, B)
     worst = {}
     for s in net.specs:
@@ -142,7 +142,7 @@ def test_training_reduces_the_loss_on_a_fixed_batch():
     net = Corrector(H, W, seed=2)
     xg, tg = O.from_nchw(x).cuda(), O.from_nchw(tgt).cuda()
     first = float(net.loss(xg, tg, B))
-    for _ in range(60):
+    for _ in range(250):
         net.train_step(xg, tg, B, lr=3e-3)
     last = float(net.loss(xg, tg, B))
-    assert last < 0.5 * first, (first, last)
+    assert last < 0.4 * first, (first, last)
