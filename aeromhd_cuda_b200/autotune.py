@@ -1,10 +1,12 @@
-"""Autotuner for the fused stage kernel: tile shape, work order and grid size.
+"""Autotuner for the fused stage kernel: kernel and work shape, work order and grid size.
 
-The stage kernel's cost depends on the tile shape (tile_x rows x 32 columns:
-halo re-reads and the share of faces computed twice fall with the tile size,
-while registers, shared memory and wave quantisation favour small tiles on
-small grids), on the persistent grid size, and for an ensemble on the order
-in which CTAs take the (instance, tile) work items.  The tuner times a few
+The stage kernel's cost depends on the kernel and its work shape (tiled:
+tile_x rows x 32 columns per CTA -- halo re-reads and the share of faces
+computed twice fall with the tile size, while registers, shared memory and
+wave quantisation favour small tiles on small grids; warp-marching, tile_x
+negative: -tile_x rows x 28 columns per warp -- longer items amortise the
+4-row start-up, shorter ones balance better), on the persistent grid size,
+and for an ensemble on the order in which CTAs take the work items.  The tuner times a few
 steps of every candidate on the GPU, on a scratch copy of the state, and keeps
 the fastest; results are cached per problem signature (process memory and an
 optional JSON file).
@@ -19,7 +21,7 @@ import os
 from dataclasses import asdict, dataclass
 from typing import Callable, Dict, Iterable, List, Optional, Sequence
 
-TILE_XS = (4, 8, 16)
+TILE_XS = (4, 8, 16, -16, -32, -64)
 ORDERS = ("instance", "interleave", "largest_first")
 GRIDS = (-1, 0)  # -1: one CTA per tile; 0: persistent (resident CTAs per SM x SMs)
 
@@ -46,12 +48,12 @@ def candidates(ensemble: bool, precision: str = "fp32", tile_xs: Sequence[int] =
 
 def choose(timings: Dict[Candidate, float], rel_tie: float = 0.01) -> Candidate:
     """Fastest candidate; within rel_tie of the best, prefer the simplest
-    (instance order, one CTA per tile, then the smaller tile)."""
+    (instance order, one CTA per tile, the tiled kernel, then the smaller tile)."""
     if not timings:
         raise ValueError("no timings")
     best = min(timings.values())
     near = [c for c, t in timings.items() if t <= best * (1.0 + rel_tie)]
-    return sorted(near, key=lambda c: (c.order != "instance", c.ctas != -1, c.tile_x))[0]
+    return sorted(near, key=lambda c: (c.order != "instance", c.ctas != -1, c.tile_x < 0, abs(c.tile_x)))[0]
 
 
 def signature(precision: str, sizes: Iterable[tuple], device_name: str = "") -> str:

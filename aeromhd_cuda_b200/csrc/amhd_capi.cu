@@ -93,8 +93,13 @@ amhd_instance single_instance(const amhd_grid *g, int tile_x)
     in.grid = *g;
     in.offset = 0;
     in.first_tile = 0;
-    in.tiles_x = (g->nx + tile_x - 1) / tile_x;
-    in.tiles_y = (g->ny + kTY - 1) / kTY;
+    if (is_march(tile_x)) {
+        in.tiles_x = (g->nx - tile_x - 1) / -tile_x;
+        in.tiles_y = (g->ny + kMarchCols - 1) / kMarchCols;
+    } else {
+        in.tiles_x = (g->nx + tile_x - 1) / tile_x;
+        in.tiles_y = (g->ny + kTY - 1) / kTY;
+    }
     return in;
 }
 
@@ -116,7 +121,7 @@ void set_input(StageParams &p, const void *uin, const amhd_grid *g, int tile_x)
 {
     p.uin = uin;
     p.use_tma = 0;
-    if (g_use_tma && encode_state_map(&p.tmap, uin, g->dtype, g->pitch, g->var_stride, tile_x) == 0) p.use_tma = 1;
+    if (g_use_tma && !is_march(tile_x) && encode_state_map(&p.tmap, uin, g->dtype, g->pitch, g->var_stride, tile_x) == 0) p.use_tma = 1;
 }
 
 cudaError_t run_stage(int dtype, int stage, int tile_x, const StageParams &p, int grid, cudaStream_t s)
@@ -269,7 +274,7 @@ int amhd_padded_layout(int32_t nx, int32_t ny, int32_t dtype, int32_t *pitch, in
 
 int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm)
 {
-    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16");
+    if (!valid_geometry(tile_x)) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8, 16 or -1024..-4 (marching rows)");
     if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(AMHD_ERR_ARG, "ctas_per_sm out of range");
     g_tile_x = tile_x;
     g_ctas_per_sm = ctas_per_sm;
@@ -286,7 +291,7 @@ int amhd_ensemble_tensormaps(const amhd_instance *inst_host, int32_t n_inst, int
                              const void *U, const void *U1, const void *U2, void *maps_host)
 {
     if (!inst_host || n_inst <= 0 || !U || !U1 || !U2 || !maps_host) return fail(AMHD_ERR_ARG, "bad arguments");
-    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16");
+    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16 (the marching kernel takes no tensor maps)");
     const size_t es = elem_size(dtype);
     CUtensorMap *maps = static_cast<CUtensorMap *>(maps_host);
     const void *bufs[3] = {U, U1, U2};
@@ -306,7 +311,7 @@ int amhd_ensemble_tensormaps(const amhd_instance *inst_host, int32_t n_inst, int
 
 int amhd_stage_info(int32_t dtype, int32_t tile_x, int32_t *smem_bytes, int32_t *ctas_per_sm, int32_t *sm_count)
 {
-    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16");
+    if (!valid_geometry(tile_x)) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8, 16 or -1024..-4 (marching rows)");
     if (dtype != AMHD_F32 && dtype != AMHD_F64) return fail(AMHD_ERR_ARG, "unknown dtype %d", dtype);
     if (smem_bytes)
         *smem_bytes = (int32_t)(dtype == AMHD_F64 ? Launch<double>::stage_smem(tile_x) : Launch<float>::stage_smem(tile_x));
@@ -736,7 +741,7 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
     if (!inst_dev || !tile_inst_dev || !U || !U1 || !U2 || !ctl_dev || n_inst <= 0 || n_tiles <= 0)
         return fail(AMHD_ERR_ARG, "bad ensemble arguments");
     if (dtype != AMHD_F32 && dtype != AMHD_F64) return fail(AMHD_ERR_ARG, "unknown dtype %d", dtype);
-    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16");
+    if (!valid_geometry(tile_x)) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8, 16 or -1024..-4 (marching rows)");
     cudaStream_t s = S(stream);
     int grid = ctas;
     if (grid <= 0) {

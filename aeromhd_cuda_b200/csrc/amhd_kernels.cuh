@@ -72,6 +72,144 @@ __device__ __forceinline__ const amhd_instance &inst_of(const StageParams &p, in
 // ---------------------------------------------------------------------------
 // fused RK stage; STAGE 1..3 (solver.py:319-329), STAGE 0 = compute_rhs (R out)
 // ---------------------------------------------------------------------------
+// does interior index i (of n) feed a ghost cell? (see ghost_targets)
+__device__ __forceinline__ bool feeds_ghosts(int i, int n, int bc)
+{
+    return bc == AMHD_BC_PERIODIC ? (i < 2 * NG || i >= n) : (i == NG || i == NG + n - 1);
+}
+
+// Copy boundary cell (i, j) of U, which this thread has just written, into
+// every ghost cell that copies it (apply_bc, solver.py:158-197; psi is zero in
+// the x-ghost rows of a non-periodic x boundary).  Few cells take this path;
+// it stays out of line so that its registers do not weigh on the caller.
+template <typename R>
+__device__ __noinline__ void push_ghosts(const amhd_grid g, R *U, int i, int j)
+{
+    int gx[4], gy[4];
+    const int nxg = ghost_targets(i, g.nx, g.bc_x, gx);
+    const int nyg = ghost_targets(j, g.ny, g.bc_y, gy);
+    const bool zero_psi_x = g.bc_x != AMHD_BC_PERIODIC;
+    const int64_t vs = g.var_stride;
+    const int pitch = g.pitch;
+    for (int v = 0; v < NV; ++v) {
+        const R val = U[v * vs + (int64_t)i * pitch + j];
+        for (int m = 0; m < nyg; ++m) U[v * vs + (int64_t)i * pitch + gy[m]] = val;
+        const R ox = (v == PSI && zero_psi_x) ? R(0) : val;
+        for (int n = 0; n < nxg; ++n) {
+            U[v * vs + (int64_t)gx[n] * pitch + j] = ox;
+            for (int m = 0; m < nyg; ++m) U[v * vs + (int64_t)gx[n] * pitch + gy[m]] = ox;
+        }
+    }
+}
+
+// cell values the Powell source needs (solver.py:242-266): Bx at i, i-1, i+1;
+// By at j, j-1, j+1; v and Bz at the cell
+template <typename R>
+struct PowellIn {
+    R bxc, bxm, bxp, byc, bym, byp, vx, vy, vz, bzc;
+};
+
+// Everything after the face fluxes for one interior cell (i, j): flux divergence,
+// Powell source, SSP-RK3 combination (solver.py:319-329), scalar clamp
+// (solver.py:199-204), psi damping (:331-333), CFL quantities of the new state
+// (stage 3, max-accumulated into q), then the cell and every ghost cell that
+// copies it (apply_bc, solver.py:158-197).  STAGE 0 writes the right-hand side
+// instead.  powell_in() gives the Powell inputs; base_at(v) / in_at(v) the
+// cell's value of U0 / of the stage input in plane v.
+template <typename R, int STAGE, typename PowellFn, typename BaseFn, typename InFn>
+__device__ __forceinline__ void update_cell(const StageParams &p, const amhd_grid &g, R *uout, int i, int j,
+                                            const R fxl[NV], const R fxr[NV], const R fyl[NV], const R fyr[NV],
+                                            PowellFn powell_in, BaseFn base_at, InFn in_at, double dt, double ch,
+                                            double decay, unsigned long long q[4], bool &bad)
+{
+    const int64_t vs = g.var_stride;
+    const int pitch = g.pitch;
+    const int64_t gi = (int64_t)i * pitch + j;
+    R rhs[NV];
+    const R dx = R(g.dx), dy = R(g.dy);
+    if constexpr (kFast<R>) {
+        const float idx = float(1.0 / g.dx), idy = float(1.0 / g.dy);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) rhs[v] = -(fxr[v] - fxl[v]) * idx - (fyr[v] - fyl[v]) * idy;
+    } else {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            R r0 = R(0);
+            r0 -= (fxr[v] - fxl[v]) / dx;
+            r0 -= (fyr[v] - fyl[v]) / dy;
+            rhs[v] = r0;
+        }
+    }
+    if (g.powell) {
+        // _compute_powell_source, solver.py:242-266 (centred face-average divB)
+        const PowellIn<R> pw = powell_in();
+        R divb = (R(0.5) * (pw.bxc + pw.bxp) - R(0.5) * (pw.bxm + pw.bxc)) / dx +
+                 (R(0.5) * (pw.byc + pw.byp) - R(0.5) * (pw.bym + pw.byc)) / dy;
+        R vb = pw.vx * pw.bxc + pw.vy * pw.byc + pw.vz * pw.bzc;
+        rhs[MX] += -divb * pw.bxc;
+        rhs[MY] += -divb * pw.byc;
+        rhs[MZ] += -divb * pw.bzc;
+        rhs[BX] += -divb * pw.vx;
+        rhs[BY] += -divb * pw.vy;
+        rhs[BZ] += -divb * pw.vz;
+        rhs[EN] += -divb * vb;
+        rhs[RHO] += R(0);  // the reference adds a zero source to these slots too
+        rhs[PSI] += R(0);
+        rhs[RHOC] += R(0);
+    }
+    R out[NV];
+    if (STAGE == 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) out[v] = rhs[v];
+    } else {
+        const R dtr = R(dt);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            R b0 = base_at(v);
+            if (STAGE == 1) {
+                out[v] = b0 + dtr * rhs[v];
+            } else {
+                R us = in_at(v);
+                if constexpr (kFast<R>) {
+                    // increment form of the same combination: in float32 the weights
+                    // 1/3 and 2/3 round to a sum of 1 + 3e-8, which as a weighted
+                    // average would scale the state every step (a mass drift);
+                    // U0 + w ((U* - U0) + dt R) has no such bias (U* - U0 is exact)
+                    const float w = STAGE == 2 ? 0.25f : float(2.0 / 3.0);
+                    out[v] = b0 + w * ((us - b0) + dtr * rhs[v]);
+                } else {
+                    if (STAGE == 2)
+                        out[v] = R(0.75) * b0 + R(0.25) * (us + dtr * rhs[v]);
+                    else
+                        out[v] = R(1.0 / 3.0) * b0 + R(2.0 / 3.0) * (us + dtr * rhs[v]);
+                }
+            }
+        }
+        // enforce_scalar_bounds, solver.py:199-204
+        R rho = np_max(out[RHO], R(FLOOR_RHO));
+        R cc = np_min(np_max(out[RHOC] / rho, R(0)), R(1));
+        out[RHOC] = rho * cc;
+        if (STAGE == 3) {
+            if (ch > 0.0) out[PSI] *= R(decay);  // solver.py:331-333
+            if (p.fuse_dt) {
+                double qd[4];
+                if constexpr (kFast<R>)
+                    fast::cfl_quantities(out, g.gamma, qd);
+                else
+                    cfl_quantities(out, g.gamma, qd);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) q[k] = umax64(q[k], ord_bits(qd[k]));
+            }
+#pragma unroll
+            for (int v = 0; v < NV; ++v) bad |= !isfinite((double)out[v]);
+        }
+    }
+    // write the cell, then every ghost that copies it (apply_bc, solver.py:158-197)
+#pragma unroll
+    for (int v = 0; v < NV; ++v) uout[v * vs + gi] = out[v];
+    if (STAGE != 0 && (feeds_ghosts(i, g.nx, g.bc_x) || feeds_ghosts(j, g.ny, g.bc_y))) push_ghosts(g, uout, i, j);
+}
+
 // returns false when the CTA must stop (a TMA transfer did not complete)
 template <typename R, int TX, int STAGE>
 __device__ __forceinline__ bool rk_stage_tile(const StageParams &p, TileSmem<R, TX> &sm, int tile, uint32_t &phase)
@@ -266,105 +404,24 @@ __device__ __forceinline__ bool rk_stage_tile(const StageParams &p, TileSmem<R, 
     unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
     bool bad = false;
     if (valid) {
-        const int64_t gi = (int64_t)i * pitch + j;
-        R rhs[NV];
-        const R dx = R(g.dx), dy = R(g.dy);
-        if constexpr (kFast<R>) {
-            const float idx = float(1.0 / g.dx), idy = float(1.0 / g.dy);
-#pragma unroll
-            for (int v = 0; v < NV; ++v)
-                rhs[v] = -(sm.fx[v][a + 1][c] - sm.fx[v][a][c]) * idx - (sm.fy[v][a][c + 1] - sm.fy[v][a][c]) * idy;
-        } else {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                R r0 = R(0);
-                r0 -= (sm.fx[v][a + 1][c] - sm.fx[v][a][c]) / dx;
-                r0 -= (sm.fy[v][a][c + 1] - sm.fy[v][a][c]) / dy;
-                rhs[v] = r0;
-            }
-        }
-        if (g.powell) {
-            // _compute_powell_source, solver.py:242-266 (centred face-average divB)
-            const int hr = a + NG, hc = c + NG;
-            R bxc = sm.w[BX][hr][hc], byc = sm.w[BY][hr][hc];
-            R divb = (R(0.5) * (bxc + sm.w[BX][hr + 1][hc]) - R(0.5) * (sm.w[BX][hr - 1][hc] + bxc)) / dx +
-                     (R(0.5) * (byc + sm.w[BY][hr][hc + 1]) - R(0.5) * (sm.w[BY][hr][hc - 1] + byc)) / dy;
-            R vx = sm.w[IVX][hr][hc], vy = sm.w[IVY][hr][hc], vz = sm.w[IVZ][hr][hc];
-            R bzc = sm.w[BZ][hr][hc];
-            R vb = vx * bxc + vy * byc + vz * bzc;
-            rhs[MX] += -divb * bxc;
-            rhs[MY] += -divb * byc;
-            rhs[MZ] += -divb * bzc;
-            rhs[BX] += -divb * vx;
-            rhs[BY] += -divb * vy;
-            rhs[BZ] += -divb * vz;
-            rhs[EN] += -divb * vb;
-            rhs[RHO] += R(0);  // the reference adds a zero source to these slots too
-            rhs[PSI] += R(0);
-            rhs[RHOC] += R(0);
-        }
-        R out[NV];
-        if (STAGE == 0) {
-#pragma unroll
-            for (int v = 0; v < NV; ++v) out[v] = rhs[v];
-        } else {
-            const R dtr = R(dt);
-#pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                R b0 = u0[v * vs + gi];
-                if (STAGE == 1) {
-                    out[v] = b0 + dtr * rhs[v];
-                } else {
-                    R us = uin[v * vs + gi];
-                    if constexpr (kFast<R>) {
-                        // increment form of the same combination: in float32 the weights
-                        // 1/3 and 2/3 round to a sum of 1 + 3e-8, which as a weighted
-                        // average would scale the state every step (a mass drift);
-                        // U0 + w ((U* - U0) + dt R) has no such bias (U* - U0 is exact)
-                        const float w = STAGE == 2 ? 0.25f : float(2.0 / 3.0);
-                        out[v] = b0 + w * ((us - b0) + dtr * rhs[v]);
-                    } else {
-                        if (STAGE == 2)
-                            out[v] = R(0.75) * b0 + R(0.25) * (us + dtr * rhs[v]);
-                        else
-                            out[v] = R(1.0 / 3.0) * b0 + R(2.0 / 3.0) * (us + dtr * rhs[v]);
-                    }
-                }
-            }
-            // enforce_scalar_bounds, solver.py:199-204
-            R rho = np_max(out[RHO], R(FLOOR_RHO));
-            R cc = np_min(np_max(out[RHOC] / rho, R(0)), R(1));
-            out[RHOC] = rho * cc;
-            if (STAGE == 3) {
-                if (ch > 0.0) out[PSI] *= R(decay);  // solver.py:331-333
-                if (p.fuse_dt) {
-                    double qd[4];
-                    if constexpr (kFast<R>)
-                        fast::cfl_quantities(out, g.gamma, qd);
-                    else
-                        cfl_quantities(out, g.gamma, qd);
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) q[k] = ord_bits(qd[k]);
-                }
-#pragma unroll
-                for (int v = 0; v < NV; ++v) bad |= !isfinite((double)out[v]);
-            }
-        }
-        // write the cell and every ghost that copies it (apply_bc, solver.py:158-197)
-        int gx[4], gy[4];
-        const int nxg = (STAGE == 0) ? 0 : ghost_targets(i, g.nx, g.bc_x, gx);
-        const int nyg = (STAGE == 0) ? 0 : ghost_targets(j, g.ny, g.bc_y, gy);
-        const bool zero_psi_x = g.bc_x != AMHD_BC_PERIODIC;
+        R fxl[NV], fxr[NV], fyl[NV], fyr[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            uout[v * vs + gi] = out[v];
-            for (int m = 0; m < nyg; ++m) uout[v * vs + (int64_t)i * pitch + gy[m]] = out[v];
-            const R ox = (v == PSI && zero_psi_x) ? R(0) : out[v];
-            for (int n = 0; n < nxg; ++n) {
-                uout[v * vs + (int64_t)gx[n] * pitch + j] = ox;
-                for (int m = 0; m < nyg; ++m) uout[v * vs + (int64_t)gx[n] * pitch + gy[m]] = ox;
-            }
+            fxl[v] = sm.fx[v][a][c];
+            fxr[v] = sm.fx[v][a + 1][c];
+            fyl[v] = sm.fy[v][a][c];
+            fyr[v] = sm.fy[v][a][c + 1];
         }
+        const int hr = a + NG, hc = c + NG;
+        auto pw = [&]() {
+            return PowellIn<R>{sm.w[BX][hr][hc],  sm.w[BX][hr - 1][hc], sm.w[BX][hr + 1][hc], sm.w[BY][hr][hc],
+                               sm.w[BY][hr][hc - 1], sm.w[BY][hr][hc + 1], sm.w[IVX][hr][hc], sm.w[IVY][hr][hc],
+                               sm.w[IVZ][hr][hc], sm.w[BZ][hr][hc]};
+        };
+        const int64_t gi = (int64_t)i * pitch + j;
+        auto base_at = [&](int v) { return u0[v * vs + gi]; };
+        auto in_at = [&](int v) { return uin[v * vs + gi]; };
+        update_cell<R, STAGE>(p, g, uout, i, j, fxl, fxr, fyl, fyr, pw, base_at, in_at, dt, ch, decay, q, bad);
     }
     if (STAGE == 3) {
         // block reduction of the CFL maxima and of the non-finite flag
@@ -413,6 +470,268 @@ __global__ void __launch_bounds__(TX * TY, (kMinBlocks<R, TX>)) rk_stage_kernel(
         const int tile = p.tile_order ? p.tile_order[pos] : pos;
         if (!rk_stage_tile<R, TX, STAGE>(p, sm, tile, phase)) return;
         __syncthreads();  // shared memory is reused by the next tile
+    }
+}
+
+// ---------------------------------------------------------------------------
+// warp-marching RK stage.  One warp owns a work item of kMarchCols interior
+// columns x march_rows rows; lane l holds column (first - 2 + l), so the 32
+// lanes cover the item's columns plus a 2-column halo on each side.  The warp
+// walks the rows in x order: each row of the input state is fetched once
+// (cp.async, one row ahead) and converted to primitives once, the x-slope and
+// the flux through the face below the current row are carried from the
+// previous row, and y-neighbours come from the adjacent lanes (warp shuffles).
+// No CTA barrier: the warps of a CTA run independently.  The per-cell
+// arithmetic is the tiled kernel's (same functions, same operation order), so
+// float64 results are identical to it.
+// ---------------------------------------------------------------------------
+template <typename R>
+__device__ __forceinline__ void to_prim(const R u[NV], double gamma, R w[NV])
+{
+    if constexpr (kFast<R>)
+        fast::cons_to_prim(u, gamma, w);
+    else
+        cons_to_prim_cell(u, gamma, w);
+}
+
+template <typename R>
+__device__ __forceinline__ R cell_slope(R wm, R w0, R wp, int limiter)
+{
+    if constexpr (kFast<R>)
+        return fast::slope(wm, w0, wp, limiter);
+    else
+        return limited_slope(wm, w0, wp, limiter);
+}
+
+// HLLD flux of one face from its reconstructed states (slot order of an x face)
+template <typename R>
+__device__ __forceinline__ void face_flux(R wl[NV], R wr[NV], R gam, float igm1, R chr, float half_ich, R f[NV])
+{
+    if constexpr (kFast<R>) {
+        fast::hlld(wl, wr, gam, igm1, chr, half_ich, f);
+    } else {
+        // floors of physics.py:331-334 (slot 7 is p in both orders)
+        wl[RHO] = np_max(wl[RHO], R(FLOOR_RHO));
+        wr[RHO] = np_max(wr[RHO], R(FLOOR_RHO));
+        wl[IPR] = np_max(wl[IPR], R(FLOOR_PR));
+        wr[IPR] = np_max(wr[IPR], R(FLOOR_PR));
+        hlld_flux(wl, wr, gam, chr, f);
+    }
+}
+
+// per-warp shared memory of the marching kernel, [var][lane] (conflict-free);
+// every entry but fy is private to its lane
+template <typename R>
+struct MarchSmem {
+    R raw[4][NV][32];  // conserved stage-input rows i-1 .. i+2 (cp.async), row r in slot r & 3
+    R base[2][NV][32]; // U0 rows i, i+1 when U0 is not the stage input, row r in slot r & 1
+    R sx[NV][32];      // limited x-slope of the current row
+    R fx[2][NV][32];   // x-face fluxes by face parity: face i-1/2 in [i & 1], i+1/2 in [(i + 1) & 1]
+    R fy[2][NV][32];   // flux through each lane's left y face, by row parity (read by the lane on the left)
+};
+
+// asynchronous copy of one row of the state (this lane's column) into shared memory
+template <typename R>
+__device__ __forceinline__ void fetch_row(R (*dst)[32], const R *u, int64_t vs, int64_t gi, int lane)
+{
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(&dst[v][lane]);
+        if constexpr (sizeof(R) == 4)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(u + v * vs + gi) : "memory");
+        else
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(u + v * vs + gi) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void fetch_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <typename R, int STAGE>
+__device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &ms, int item, int lane,
+                                           unsigned long long q[4], bool &bad, amhd_control *&ctl_out)
+{
+    int ii;
+    const amhd_instance &in = inst_of(p, item, ii);
+    const amhd_grid g = in.grid;
+    amhd_control *ctl = p.ctl ? p.ctl + ii : nullptr;
+    ctl_out = ctl;
+    double dt = p.dt, ch = p.ch, decay = p.decay;
+    if (p.use_ctl) {
+        if (!ctl->active) return;
+        dt = ctl->dt;
+        ch = ctl->ch;
+        decay = ctl->decay;
+    }
+    const int local = item - in.first_tile;
+    const int strip = local % in.tiles_y, chunk = local / in.tiles_y;
+    const int j = kMarchCols * strip + lane;  // storage column of this lane (first interior column - 2 + lane)
+    const int jl = min(j, g.pitch - 1);       // lanes past the padded row load a cell they do not use
+    const int ib = NG + chunk * p.march_rows;
+    const int ie = min(ib + p.march_rows, NG + g.nx);
+    const int64_t vs = g.var_stride;
+    const int pitch = g.pitch;
+    const R *uin = reinterpret_cast<const R *>(p.uin) + in.offset;
+    const R *u0 = reinterpret_cast<const R *>(p.u0) + in.offset;
+    R *uout = reinterpret_cast<R *>(p.uout) + in.offset;
+    const bool out_lane = lane >= NG && lane < NG + kMarchCols && j < NG + g.ny;
+    // U0 comes from its own buffer unless it is the stage input (stage 1 of a step)
+    const bool own_base = STAGE >= 1 && p.u0 != p.uin;
+
+    const R gam = R(g.gamma), chr = R(ch);
+    const int lim = g.limiter;
+    const float igm1 = 1.0f / float(g.gamma - 1.0), half_ich = ch > 0.0 ? float(0.5 / ch) : 0.f;
+    constexpr int rot[NV] = {0, 2, 1, 3, 5, 4, 6, 7, 8, 9};
+
+    // prologue: rows ib-2 .. ib+1 give the x-slope of row ib and the flux
+    // through face ib-1/2
+#pragma unroll 1
+    for (int r = ib - 2; r <= ib + 1; ++r) fetch_row(ms.raw[r & 3], uin, vs, (int64_t)r * pitch + jl, lane);
+    if (own_base) fetch_row(ms.base[ib & 1], u0, vs, (int64_t)ib * pitch + jl, lane);
+    fetch_wait();
+    R w0[NV], w1[NV], bxm;
+    {
+        R u[NV], wa[NV], wb[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) u[v] = ms.raw[(ib - 2) & 3][v][lane];
+        to_prim(u, g.gamma, wa);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) u[v] = ms.raw[(ib - 1) & 3][v][lane];
+        to_prim(u, g.gamma, wb);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) u[v] = ms.raw[ib & 3][v][lane];
+        to_prim(u, g.gamma, w0);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) u[v] = ms.raw[(ib + 1) & 3][v][lane];
+        to_prim(u, g.gamma, w1);
+        R wl[NV], wr[NV], f[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            const R sm1 = cell_slope(wa[v], wb[v], w0[v], lim);
+            const R s0 = cell_slope(wb[v], w0[v], w1[v], lim);
+            ms.sx[v][lane] = s0;
+            wl[v] = wb[v] + R(0.5) * sm1;
+            wr[v] = w0[v] - R(0.5) * s0;
+        }
+        face_flux(wl, wr, gam, igm1, chr, half_ich, f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) ms.fx[ib & 1][v][lane] = f[v];
+        bxm = wb[BX];
+    }
+    // row ib+2 replaces row ib-2, whose values the prologue has used
+    fetch_row(ms.raw[(ib + 2) & 3], uin, vs, (int64_t)(ib + 2) * pitch + jl, lane);
+
+    for (int i = ib; i < ie; ++i) {
+        const int par = i & 1;
+        fetch_wait();  // row i+2 of the input and U0 of row i have landed
+        // one row ahead: row i+3 replaces row i-1 (done with since the last
+        // iteration), and U0 of row i+1 replaces that of row i-1
+        if (i + 1 < ie) {
+            fetch_row(ms.raw[(i + 3) & 3], uin, vs, (int64_t)(i + 3) * pitch + jl, lane);
+            if (own_base) fetch_row(ms.base[par ^ 1], u0, vs, (int64_t)(i + 1) * pitch + jl, lane);
+        }
+        // y: slope of this lane's cell of row i from its lane neighbours, and
+        // the flux through the face on the cell's left (rotated slot order of
+        // physics.py:376-379); the right face is the next lane's left face
+        __syncwarp();  // the left neighbour has read ms.fy[par] of row i-2
+        R bym = R(0), byp = R(0);
+        {
+            R wl[NV], wr[NV], f[NV];
+#pragma unroll
+            for (int k = 0; k < NV; ++k) {
+                const int v = rot[k];
+                const R wm = __shfl_up_sync(0xffffffffu, w0[v], 1);
+                const R wp = __shfl_down_sync(0xffffffffu, w0[v], 1);
+                const R sy = cell_slope(wm, w0[v], wp, lim);
+                wr[k] = w0[v] - R(0.5) * sy;
+                wl[k] = __shfl_up_sync(0xffffffffu, w0[v] + R(0.5) * sy, 1);
+                if (v == BY) {
+                    bym = wm;
+                    byp = wp;
+                }
+            }
+            face_flux(wl, wr, gam, igm1, chr, half_ich, f);
+#pragma unroll
+            for (int k = 0; k < NV; ++k) ms.fy[par][rot[k]][lane] = f[k];
+        }
+        // x: primitives of row i+2, slope of row i+1 and the flux through face i+1/2
+        R w2[NV];
+        {
+            R u[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u[v] = ms.raw[(i + 2) & 3][v][lane];
+            to_prim(u, g.gamma, w2);
+            R wl[NV], wr[NV], f[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const R s1 = cell_slope(w0[v], w1[v], w2[v], lim);
+                wl[v] = w0[v] + R(0.5) * ms.sx[v][lane];
+                wr[v] = w1[v] - R(0.5) * s1;
+                ms.sx[v][lane] = s1;
+            }
+            face_flux(wl, wr, gam, igm1, chr, half_ich, f);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) ms.fx[par ^ 1][v][lane] = f[v];
+        }
+        __syncwarp();  // every lane's y-face flux of row i is in ms.fy[par]
+        if (out_lane) {
+            R fxl[NV], fxr[NV], fyl[NV], fyr[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                fxl[v] = ms.fx[par][v][lane];
+                fxr[v] = ms.fx[par ^ 1][v][lane];
+                fyl[v] = ms.fy[par][v][lane];
+                fyr[v] = ms.fy[par][v][lane + 1];  // output lanes stop at 29
+            }
+            auto pw = [&]() {
+                return PowellIn<R>{w0[BX], bxm, w1[BX], w0[BY], bym, byp, w0[IVX], w0[IVY], w0[IVZ], w0[BZ]};
+            };
+            const int slot = i & 3;
+            auto in_at = [&](int v) { return ms.raw[slot][v][lane]; };
+            auto base_at = [&](int v) { return own_base ? ms.base[par][v][lane] : ms.raw[slot][v][lane]; };
+            update_cell<R, STAGE>(p, g, uout, i, j, fxl, fxr, fyl, fyr, pw, base_at, in_at, dt, ch, decay, q, bad);
+        }
+        bxm = w0[BX];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+            w0[v] = w1[v];
+            w1[v] = w2[v];
+        }
+    }
+    __syncwarp();  // the next item reuses the shared rows
+}
+
+// resident CTAs of kMarchThreads per SM the register budget is shaped for
+template <typename R>
+constexpr int kMarchMinBlocks = kFast<R> ? 4 : 2;
+
+template <typename R, int STAGE>
+__global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R>)) march_stage_kernel(
+    const __grid_constant__ StageParams p)
+{
+    extern __shared__ __align__(16) unsigned char march_smem[];
+    MarchSmem<R> &ms = reinterpret_cast<MarchSmem<R> *>(march_smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int n_warps = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+    for (int pos = warp; pos < p.n_tiles; pos += n_warps) {
+        const int item = p.tile_order ? p.tile_order[pos] : pos;
+        unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
+        bool bad = false;
+        amhd_control *ctl = nullptr;
+        march_item<R, STAGE>(p, ms, item, lane, q, bad, ctl);
+        if (STAGE == 3 && ctl != nullptr) {
+            // warp reduction of the CFL maxima and of the non-finite flag of the item
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                for (int o = 16; o > 0; o >>= 1) q[k] = umax64(q[k], __shfl_xor_sync(0xffffffffu, q[k], o));
+            const unsigned any_bad = __any_sync(0xffffffffu, bad);
+            if (lane == 0) {
+                if (p.fuse_dt)
+                    for (int k = 0; k < 4; ++k)
+                        if (q[k]) atomicMax(reinterpret_cast<unsigned long long *>(&ctl->red[k]), q[k]);
+                if (any_bad) atomicOr(&ctl->flags, AMHD_FLAG_NONFINITE);
+            }
+        }
     }
 }
 

@@ -29,7 +29,19 @@ struct StageParams {
     double dt, ch, decay;          // host scalars when !use_ctl
     int32_t use_ctl;               // take dt / ch / decay / active from ctl
     int32_t fuse_dt;               // stage 3: accumulate the CFL reduction
+    int32_t march_rows;            // warp-marching kernel: rows of one work item
 };
+
+// Work geometry of the stage kernels, passed around as one int "tile_x":
+// 4, 8, 16 -- the tiled kernel (tile_x x 32 cells per CTA);
+// -1024 .. -4 -- the warp-marching kernel, -tile_x rows x kMarchCols columns per warp.
+constexpr int kMarchCols = 28;     // 32 lanes minus a 2-column halo on each side
+constexpr int kMarchThreads = 128; // 4 independent warps per CTA
+inline bool is_march(int tile_x) { return tile_x < 0; }
+inline bool valid_geometry(int tile_x)
+{
+    return tile_x == 4 || tile_x == 8 || tile_x == 16 || (tile_x <= -4 && tile_x >= -1024);
+}
 
 struct Layout {
     int32_t nxt, nyt, pitch;

@@ -15,8 +15,12 @@ static inline int elem_blocks(int64_t n, int threads = 256)
 }
 
 template <typename R>
+constexpr size_t kMarchSmem = sizeof(MarchSmem<R>) * (kMarchThreads / 32);
+
+template <typename R>
 size_t Launch<R>::stage_smem(int tile_x)
 {
+    if (is_march(tile_x)) return kMarchSmem<R>;
     switch (tile_x) {
     case 4: return sizeof(TileSmem<R, 4>);
     case 8: return sizeof(TileSmem<R, 8>);
@@ -83,11 +87,40 @@ static cudaError_t launch_stage_tx(int stage, const StageParams &p, int grid, cu
     }
 }
 
+template <typename R, int ST>
+static cudaError_t launch_march_t(const StageParams &p, int grid, cudaStream_t s)
+{
+    static bool configured = false;  // shared-memory opt-in, once per process
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(march_stage_kernel<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)kMarchSmem<R>);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    march_stage_kernel<R, ST><<<grid, kMarchThreads, kMarchSmem<R>, s>>>(p);
+    return cudaGetLastError();
+}
+
 template <typename R>
 cudaError_t Launch<R>::stage(int stage, int tile_x, const StageParams &p, int grid, cudaStream_t s)
 {
-    if (grid <= 0) grid = p.n_tiles;
     if (p.n_tiles <= 0) return cudaSuccess;
+    if (is_march(tile_x)) {
+        // grid counts CTAs of kMarchThreads / 32 warps; one warp per work item at a time
+        const int wpc = kMarchThreads / 32;
+        const int need = (p.n_tiles + wpc - 1) / wpc;
+        if (grid <= 0 || grid > need) grid = need;
+        StageParams q = p;
+        q.march_rows = -tile_x;
+        switch (stage) {
+        case 0: return launch_march_t<R, 0>(q, grid, s);
+        case 1: return launch_march_t<R, 1>(q, grid, s);
+        case 2: return launch_march_t<R, 2>(q, grid, s);
+        case 3: return launch_march_t<R, 3>(q, grid, s);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    if (grid <= 0) grid = p.n_tiles;
     switch (tile_x) {
     case 4: return launch_stage_tx<R, 4>(stage, p, grid, s);
     case 8: return launch_stage_tx<R, 8>(stage, p, grid, s);
@@ -110,6 +143,15 @@ static int ctas_per_sm_t()
 template <typename R>
 int Launch<R>::stage_ctas_per_sm(int tile_x)
 {
+    if (is_march(tile_x)) {
+        int n = 0;
+        cudaFuncSetAttribute(march_stage_kernel<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kMarchSmem<R>);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, march_stage_kernel<R, 3>, kMarchThreads,
+                                                          kMarchSmem<R>) != cudaSuccess)
+            return 1;
+        return n > 0 ? n : 1;
+    }
     switch (tile_x) {
     case 4: return ctas_per_sm_t<R, 4>();
     case 8: return ctas_per_sm_t<R, 8>();

@@ -66,8 +66,24 @@ def pack_layout(configs: Sequence[Config], dtype_code: int):
     return layouts, off
 
 
+MARCH_COLS = 28  # interior columns of one warp-marching work item (32 lanes minus a 2-column halo each side)
+
+
+def valid_geometry(tile_x: int) -> bool:
+    """4, 8, 16: tiled stage kernel; -1024..-4: warp-marching kernel, -tile_x rows per item."""
+    return tile_x in (4, 8, 16) or -1024 <= tile_x <= -4
+
+
+def work_shape(tile_x: int) -> tuple:
+    """(rows, columns) of one work item of the stage kernel for this geometry."""
+    if not valid_geometry(tile_x):
+        raise ValueError("tile_x must be 4, 8, 16 (tiled kernel) or -1024..-4 (marching kernel rows)")
+    return (tile_x, 32) if tile_x > 0 else (-tile_x, MARCH_COLS)
+
+
 def tile_counts(configs: Sequence[Config], tile_x: int) -> np.ndarray:
-    return np.array([((c.nx + tile_x - 1) // tile_x) * ((c.ny + 31) // 32) for c in configs], dtype=np.int64)
+    r, c_ = work_shape(tile_x)
+    return np.array([((c.nx + r - 1) // r) * ((c.ny + c_ - 1) // c_) for c in configs], dtype=np.int64)
 
 
 def work_list(counts: Sequence[int], order: str = "instance"):
@@ -159,10 +175,12 @@ class Ensemble:
 
     # -------------------------------------------------------- schedule
     def set_schedule(self, tile_x: int, order: str = "instance", ctas: int = 0):
-        """Tile shape, work-list order and persistent grid size (chosen by autotune).
-        ctas: 0 = resident CTAs per SM x SM count; -1 = one CTA per tile."""
-        if tile_x not in (4, 8, 16):
-            raise ValueError("tile_x must be 4, 8 or 16")
+        """Stage-kernel geometry (tile_x: 4, 8, 16 rows x 32 columns per CTA of the
+        tiled kernel, or negative: -tile_x rows x 28 columns per warp of the
+        marching kernel), work-list order and persistent grid size (chosen by
+        autotune).  ctas: 0 = resident CTAs per SM x SM count; -1 = one CTA
+        per tile."""
+        rows, cols = work_shape(tile_x)
         self.tile_x, self.order, self.ctas = int(tile_x), order, int(ctas)
         counts = tile_counts(self.configs, tile_x)
         tile_order, tile_inst, first = work_list(counts, order)
@@ -171,8 +189,8 @@ class Ensemble:
             inst = table[k]
             inst.grid = self._grid(k)
             inst.offset = off
-            inst.tiles_x = (c.nx + tile_x - 1) // tile_x
-            inst.tiles_y = (c.ny + 31) // 32
+            inst.tiles_x = (c.nx + rows - 1) // rows
+            inst.tiles_y = (c.ny + cols - 1) // cols
             inst.first_tile = int(first[k])
         self.n_tiles = int(counts.sum())
         self._table = table
@@ -181,7 +199,7 @@ class Ensemble:
         self.tile_inst = torch.from_numpy(tile_inst).to(self.device)
         self.tile_order = torch.from_numpy(tile_order).to(self.device)
         self.tmaps_dev = None
-        if self.use_tma:
+        if self.use_tma and tile_x > 0:
             # TMA descriptors of every instance's box in U, U1, U2 for this tile shape
             maps = torch.empty(3 * self.n * 128, dtype=torch.uint8)
             _lib.call("amhd_ensemble_tensormaps", ctypes.byref(table), self.n, self.code, self.tile_x,

@@ -53,7 +53,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--tma", type=int, default=1, help="stage tiles with TMA (1) or 128-bit loads (0)")
-    ap.add_argument("--tile-x", type=int, default=8)
+    ap.add_argument("--tile-x", type=int, default=8,
+                    help="stage kernel geometry: 4, 8, 16 (tiled kernel rows) or negative (warp-marching rows)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also time the batched shock-interface ensemble of this many instances")
     return ap.parse_args(argv)
@@ -76,9 +77,19 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def profile_traffic():
+def stage_kernel_name(tile_x):
+    return "march_stage_kernel" if tile_x < 0 else "rk_stage_kernel"
+
+
+def stage_geometry(tile_x):
+    if tile_x < 0:
+        return f"warp-marching, {-tile_x} rows x 28 columns per warp, cp.async row staging"
+    return f"tiled, {tile_x}x32 cells per CTA"
+
+
+def profile_traffic(tile_x):
     """dram bytes per stage-kernel step from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "rk_stage_kernel_traffic.txt")
+    path = os.path.join(ROOT, "profiles", stage_kernel_name(tile_x) + "_traffic.txt")
     try:
         vals = {}
         for line in open(path):
@@ -270,7 +281,7 @@ def run_ours(a, world, rank, local):
     stage_ms = prof[0] + prof[1] + prof[2]
     alg_bytes_step = 80 * es * cells
     achieved = alg_bytes_step * a.steps / (stage_ms / 1e3) / 1e9
-    tr = profile_traffic()
+    tr = profile_traffic(a.tile_x)
     traffic = None
     if tr.get("precision") == a.precision and tr.get("n"):
         try:
@@ -279,7 +290,7 @@ def run_ours(a, world, rank, local):
             traffic = None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": hbm_kind,
-                "kernel": "rk_stage_kernel (3 launches/step)",
+                "kernel": stage_kernel_name(a.tile_x) + " (3 launches/step)",
                 "algorithmic_bytes_per_step": alg_bytes_step,
                 "ms_per_step": {"stage1": prof[0] / a.steps, "stage2": prof[1] / a.steps,
                                 "stage3_fused_dt": prof[2] / a.steps, "finalize": prof[3] / a.steps}}
@@ -349,8 +360,9 @@ def run_ours(a, world, rank, local):
         "config": {"workload": f"orszag_tang_{n}x{n}_{a.precision}", "nx": n, "ny": n, "precision": a.precision,
                    "pressure_recovery": "f64", "dt_reduction": "f64",
                    "l2": "inputs larger than L2 (3 state buffers of %.0f MB)" % (10 * (n + 4) * (n + 4) * es / 1e6),
-                   "parallelism": f"replicas x{world}", "tile": f"{a.tile_x}x32, one CTA per tile",
-                   "staging": "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads"},
+                   "parallelism": f"replicas x{world}", "stage_kernel": stage_geometry(a.tile_x),
+                   "staging": ("cp.async rows" if a.tile_x < 0 else
+                               "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads")},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * a.steps,
         "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
     }

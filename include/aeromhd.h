@@ -110,15 +110,21 @@ int amhd_init(void);
  * pitch and rows per plane (multiples the kernels' tiles need). */
 int amhd_padded_layout(int32_t nx, int32_t ny, int32_t dtype, int32_t *pitch, int32_t *rows);
 size_t amhd_control_size(void);
-/* Tiling of the fused stage kernel for single-grid calls: tile_x (x rows per
- * 32-column tile: 4, 8 or 16) and ctas_per_sm (0: one CTA per tile,
- * otherwise a persistent grid of ctas_per_sm x SM-count CTAs).  Process-wide;
- * chosen by the autotuner.  No counterpart in the reference. */
+/* Stage kernel and its work shape for single-grid calls.  tile_x 4, 8 or 16:
+ * the tiled kernel, tile_x x 32 cells per CTA staged in shared memory;
+ * tile_x from -1024 to -4: the warp-marching kernel, one warp per item of
+ * -tile_x rows x 28 columns, walking the rows with the x-slopes and x-face
+ * fluxes carried from row to row (no CTA barriers).  ctas_per_sm: 0 = one CTA
+ * per tile (tiled) / per 4 items (marching), otherwise a persistent grid of
+ * ctas_per_sm x SM-count CTAs.  Both kernels compute the same arithmetic
+ * (identical float64 results).  Process-wide; chosen by the autotuner.  The
+ * same tile_x values are accepted by amhd_stage_info and
+ * amhd_ensemble_advance.  No counterpart in the reference. */
 int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm);
 /* Stage the tile + halo with TMA (cp.async.bulk.tensor) when on (default) or
  * with 128-bit loads when off.  Process-wide.  No counterpart in the reference. */
 int amhd_set_tma(int32_t on);
-/* shared memory per CTA and resident CTAs per SM of the stage kernel */
+/* shared memory per CTA and resident CTAs per SM of the stage kernel of this geometry */
 int amhd_stage_info(int32_t dtype, int32_t tile_x, int32_t *smem_bytes, int32_t *ctas_per_sm, int32_t *sm_count);
 
 /* ---- physics.py ------------------------------------------------------- */

@@ -66,13 +66,18 @@ def test_shard_balances_cells_and_covers_everything():
 
 def test_candidates_and_choice():
     ens = candidates(True, "fp32")
-    assert Candidate(8, "interleave", 0) in ens and len(ens) == 3 * 3 * 2
+    assert Candidate(8, "interleave", 0) in ens and len(ens) == 6 * 3 * 2
+    assert Candidate(-32, "instance", 0) in ens  # warp-marching kernel, 32 rows per item
     assert all(c.tile_x != 16 for c in candidates(True, "fp64"))
     assert all(c.order == "instance" for c in candidates(False, "fp32"))
     t = {Candidate(8, "instance", -1): 1.0, Candidate(4, "instance", -1): 1.005, Candidate(16, "interleave", 0): 0.5}
     assert choose(t) == Candidate(16, "interleave", 0)
     t = {Candidate(8, "instance", -1): 1.0, Candidate(4, "instance", -1): 1.005, Candidate(16, "interleave", 0): 1.2}
     assert choose(t) == Candidate(4, "instance", -1)  # tie within 1%: simplest, then smaller tile
+    t = {Candidate(8, "instance", -1): 1.0, Candidate(-32, "instance", -1): 1.004}
+    assert choose(t) == Candidate(8, "instance", -1)  # tie: the tiled kernel
+    t = {Candidate(8, "instance", -1): 1.0, Candidate(-32, "instance", -1): 0.7}
+    assert choose(t) == Candidate(-32, "instance", -1)
 
 
 def test_tune_uses_cache(tmp_path):
@@ -81,7 +86,7 @@ def test_tune_uses_cache(tmp_path):
 
     def run(c):
         calls.append(c)
-        return {4: 3.0, 8: 1.0, 16: 2.0}[c.tile_x]
+        return {4: 3.0, 8: 1.0, 16: 2.0}.get(c.tile_x, 4.0)
 
     key = signature("fp32", [(128, 32), (512, 128)], "B200")
     assert key == signature("fp32", [(512, 128), (128, 32)], "B200")
@@ -91,3 +96,15 @@ def test_tune_uses_cache(tmp_path):
     n = len(calls)
     best2, t2 = tune(run, candidates(False), key, Cache(path))   # fresh cache object reads the file
     assert best2 == best and t2 == {} and len(calls) == n
+
+
+def test_work_shapes_and_counts():
+    from aeromhd_cuda_b200.config import Config
+    from aeromhd_cuda_b200.ensemble import work_shape
+    assert work_shape(8) == (8, 32) and work_shape(-32) == (32, 28)
+    for bad in (0, 3, 5, -3, 32, -2000):
+        with pytest.raises(ValueError):
+            work_shape(bad)
+    cfgs = [Config(nx=100, ny=60), Config(nx=64, ny=28)]
+    assert list(tile_counts(cfgs, 8)) == [13 * 2, 8 * 1]
+    assert list(tile_counts(cfgs, -32)) == [4 * 3, 2 * 1]

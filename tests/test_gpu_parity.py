@@ -88,7 +88,8 @@ def step_cfg(bcx, bcy, By, **kw):
              powell_source=True, bc_x_type=bcx, bc_y_type=bcy, glm_alpha=1.5, **kw)
 
 
-@pytest.mark.parametrize("tile_x", [8, 4, 16])
+# 4, 8, 16: tiled kernel; negative: warp-marching kernel with that many rows per work item
+@pytest.mark.parametrize("tile_x", [8, 4, 16, -4, -6, -64])
 @pytest.mark.parametrize("k", range(len(STEP_CASES)))
 def test_three_steps_bit_exact(amhd, k, tile_x):
     g = golden("steps.npz")
@@ -349,3 +350,55 @@ def test_tma_staging_matches_plain_loads_single_grid(amhd, precision):
     finally:
         amhd.lib.call("amhd_set_tma", 1)
     assert torch.equal(res[0], res[1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape,rows", [((80, 80), -8), ((75, 61), -5), ((64, 130), -32), ((33, 29), -4)])
+def test_marching_kernel_matches_tiled(amhd, precision, shape, rows):
+    """Warp-marching stage kernel vs the tiled one on odd shapes (strips of 28
+    columns and chunks of rows that do not divide the grid): identical bits in
+    float64; in float32 the two compile the same arithmetic with different
+    FMA contraction, so the bar is 1e-6 relative."""
+    from aeromhd_cuda_b200 import initial_conditions as ic
+    nx, ny = shape
+    res = []
+    try:
+        for tx in (8, rows):
+            amhd.lib.call("amhd_set_tiling", tx, 0)
+            cfg = C(nx=nx, ny=ny, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, t_end=0.5, cfl=0.4,
+                    gamma=5.0 / 3.0, powell_source=False, bc_x_type="periodic", bc_y_type="periodic",
+                    precision=precision)
+            s = amhd.solver.MHDSolver(cfg)
+            s.set_primitive(ic.orszag_tang(s))
+            s.advance(max_steps=9, chunk=9, graph=False)
+            res.append((s.U.clone(), s.t))
+    finally:
+        amhd.lib.call("amhd_set_tiling", 8, 0)
+    (a, ta), (b, tb) = res
+    if precision == "fp64":
+        assert ta == tb
+        assert torch.equal(a, b)
+    else:
+        assert abs(ta - tb) <= 1e-6 * ta
+        assert rel_l1(np_(b), np_(a)) < 1e-6
+
+
+@pytest.mark.parametrize("bcx", ["extrapolation", "characteristic"])
+def test_marching_kernel_rmi_device_loop_bit_exact(amhd, bcx):
+    """Shocked-interface problem (outflow / characteristic x boundaries, Powell
+    source on) on the marching kernel against the tiled kernel, 25 device-loop
+    steps in float64."""
+    res = []
+    try:
+        for tx in (8, -16):
+            amhd.lib.call("amhd_set_tiling", tx, 0)
+            cfg = C(nx=96, ny=40, B_transverse=0.3, glm_ch=0.0, bc_x_type=bcx, t_end=1.0)
+            s = amhd.solver.MHDSolver(cfg)
+            s.initialize()
+            s.advance(max_steps=25, chunk=25, graph=False)
+            res.append((s.U.clone(), s.t, s._cumulative_boundary_energy))
+    finally:
+        amhd.lib.call("amhd_set_tiling", 8, 0)
+    (a, ta, ea), (b, tb, eb) = res
+    assert ta == tb and ea == eb
+    assert torch.equal(a, b)
