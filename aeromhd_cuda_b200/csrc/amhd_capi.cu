@@ -156,11 +156,12 @@ cudaError_t run_dt_reduce(const amhd_grid *g, const void *A, int from_prim, amhd
 int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instance *insts, const int32_t *tile_inst,
                  int n_tiles, int tile_x, int grid, void *U, void *U1, void *U2, amhd_control *ctl, int use_ctl,
                  double dt, double ch, double decay, int fuse_dt, cudaStream_t s, const int32_t *tile_order = nullptr,
-                 const CUtensorMap *tmaps = nullptr)
+                 const CUtensorMap *tmaps = nullptr, int n_inst = 1)
 {
     StageParams p;
     memset(&p, 0, sizeof p);
     p.inst = insts;
+    p.n_inst = n_inst;
     p.one = one;
     p.tile_inst = tile_inst;
     p.tile_order = tile_order;
@@ -757,7 +758,7 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
     memset(&dummy, 0, sizeof dummy);
     for (int k = 0; k < n_steps; ++k) {
         if (int e = three_stages(&gdt, dummy, inst_dev, tile_inst_dev, n_tiles, tile_x, grid, U, U1, U2, ctl_dev, 1, 0,
-                                 0, 1, 1, s, tile_order_dev, static_cast<const CUtensorMap *>(tmaps_dev)))
+                                 0, 1, 1, s, tile_order_dev, static_cast<const CUtensorMap *>(tmaps_dev), n_inst))
             return e;
         CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 1, 0, s));
     }

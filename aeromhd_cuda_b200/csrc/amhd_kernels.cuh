@@ -114,13 +114,15 @@ struct PowellIn {
 // (solver.py:199-204), psi damping (:331-333), CFL quantities of the new state
 // (stage 3, max-accumulated into q), then the cell and every ghost cell that
 // copies it (apply_bc, solver.py:158-197).  STAGE 0 writes the right-hand side
-// instead.  powell_in() gives the Powell inputs; base_at(v) / in_at(v) the
-// cell's value of U0 / of the stage input in plane v.
-template <typename R, int STAGE, typename PowellFn, typename BaseFn, typename InFn>
-__device__ __forceinline__ void update_cell(const StageParams &p, const amhd_grid &g, R *uout, int i, int j,
-                                            const R fxl[NV], const R fxr[NV], const R fyl[NV], const R fyr[NV],
-                                            PowellFn powell_in, BaseFn base_at, InFn in_at, double dt, double ch,
-                                            double decay, unsigned long long q[4], bool &bad)
+// instead.  dfx / dfy: flux differences (face +1/2 minus face -1/2) in x and
+// y; powell_in() gives the Powell inputs; base_at(v) / in_at(v) the cell's
+// value of U0 / of the stage input in plane v.  Without PUSH the caller fills
+// the ghost cells afterwards (march_bc_fill_kernel).
+template <typename R, int STAGE, bool PUSH = true, typename PowellFn, typename BaseFn, typename InFn>
+__device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_grid &g, R *uout, int i, int j,
+                                              const R dfx[NV], const R dfy[NV], PowellFn powell_in, BaseFn base_at,
+                                              InFn in_at, double dt, double ch, double decay, unsigned long long q[4],
+                                              bool &bad)
 {
     const int64_t vs = g.var_stride;
     const int pitch = g.pitch;
@@ -130,13 +132,13 @@ __device__ __forceinline__ void update_cell(const StageParams &p, const amhd_gri
     if constexpr (kFast<R>) {
         const float idx = float(1.0 / g.dx), idy = float(1.0 / g.dy);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) rhs[v] = -(fxr[v] - fxl[v]) * idx - (fyr[v] - fyl[v]) * idy;
+        for (int v = 0; v < NV; ++v) rhs[v] = -dfx[v] * idx - dfy[v] * idy;
     } else {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             R r0 = R(0);
-            r0 -= (fxr[v] - fxl[v]) / dx;
-            r0 -= (fyr[v] - fyl[v]) / dy;
+            r0 -= dfx[v] / dx;
+            r0 -= dfy[v] / dy;
             rhs[v] = r0;
         }
     }
@@ -207,7 +209,24 @@ __device__ __forceinline__ void update_cell(const StageParams &p, const amhd_gri
     // write the cell, then every ghost that copies it (apply_bc, solver.py:158-197)
 #pragma unroll
     for (int v = 0; v < NV; ++v) uout[v * vs + gi] = out[v];
-    if (STAGE != 0 && (feeds_ghosts(i, g.nx, g.bc_x) || feeds_ghosts(j, g.ny, g.bc_y))) push_ghosts(g, uout, i, j);
+    if (PUSH && STAGE != 0 && (feeds_ghosts(i, g.nx, g.bc_x) || feeds_ghosts(j, g.ny, g.bc_y)))
+        push_ghosts(g, uout, i, j);
+}
+
+// the same from the four face fluxes
+template <typename R, int STAGE, typename PowellFn, typename BaseFn, typename InFn>
+__device__ __forceinline__ void update_cell(const StageParams &p, const amhd_grid &g, R *uout, int i, int j,
+                                            const R fxl[NV], const R fxr[NV], const R fyl[NV], const R fyr[NV],
+                                            PowellFn powell_in, BaseFn base_at, InFn in_at, double dt, double ch,
+                                            double decay, unsigned long long q[4], bool &bad)
+{
+    R dfx[NV], dfy[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        dfx[v] = fxr[v] - fxl[v];
+        dfy[v] = fyr[v] - fyl[v];
+    }
+    update_cell_d<R, STAGE>(p, g, uout, i, j, dfx, dfy, powell_in, base_at, in_at, dt, ch, decay, q, bad);
 }
 
 // returns false when the CTA must stop (a TMA transfer did not complete)
@@ -523,11 +542,11 @@ __device__ __forceinline__ void face_flux(R wl[NV], R wr[NV], R gam, float igm1,
 // every entry but fy is private to its lane
 template <typename R>
 struct MarchSmem {
-    R raw[4][NV][32];  // conserved stage-input rows i-1 .. i+2 (cp.async), row r in slot r & 3
-    R base[2][NV][32]; // U0 rows i, i+1 when U0 is not the stage input, row r in slot r & 1
+    R raw[3][NV][32];  // conserved stage-input rows i .. i+2 (cp.async), row r in slot r % 3
+    R base[NV][32];    // U0 of row i when U0 is not the stage input
     R sx[NV][32];      // limited x-slope of the current row
-    R fx[2][NV][32];   // x-face fluxes by face parity: face i-1/2 in [i & 1], i+1/2 in [(i + 1) & 1]
-    R fy[2][NV][32];   // flux through each lane's left y face, by row parity (read by the lane on the left)
+    R fx[NV][32];      // flux through the x face below the current row
+    R fy[NV][32];      // flux through each lane's left y face of the current row (read by the lane on the left)
 };
 
 // asynchronous copy of one row of the state (this lane's column) into shared memory
@@ -582,59 +601,45 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
     const float igm1 = 1.0f / float(g.gamma - 1.0), half_ich = ch > 0.0 ? float(0.5 / ch) : 0.f;
     constexpr int rot[NV] = {0, 2, 1, 3, 5, 4, 6, 7, 8, 9};
 
-    // prologue: rows ib-2 .. ib+1 give the x-slope of row ib and the flux
-    // through face ib-1/2
-#pragma unroll 1
-    for (int r = ib - 2; r <= ib + 1; ++r) fetch_row(ms.raw[r & 3], uin, vs, (int64_t)r * pitch + jl, lane);
-    if (own_base) fetch_row(ms.base[ib & 1], u0, vs, (int64_t)ib * pitch + jl, lane);
+    // Rows ib-2 .. ib are fetched up front and row ib+1 behind them.  The walk
+    // starts one row early: iteration ib-1 only computes the flux through face
+    // ib-1/2 (no y faces, no update), so the x-face code is not repeated in a
+    // prologue.  Input row r lives in slot r % 3; each iteration fetches the
+    // input row three ahead and the next row of U0 once it is done with the
+    // slots they replace, and waits for them just before the x faces.
+    int s0 = (ib - 2) % 3;  // slot of row i (ib-2 here)
+    const int s1i = s0 == 2 ? 0 : s0 + 1, s2i = s1i == 2 ? 0 : s1i + 1;
+    fetch_row(ms.raw[s0], uin, vs, (int64_t)(ib - 2) * pitch + jl, lane);
+    fetch_row(ms.raw[s1i], uin, vs, (int64_t)(ib - 1) * pitch + jl, lane);
+    fetch_row(ms.raw[s2i], uin, vs, (int64_t)ib * pitch + jl, lane);
     fetch_wait();
-    R w0[NV], w1[NV], bxm;
+    R w0[NV], w1[NV], bxm = R(0);
     {
-        R u[NV], wa[NV], wb[NV];
+        R u[NV], wa[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) u[v] = ms.raw[(ib - 2) & 3][v][lane];
+        for (int v = 0; v < NV; ++v) u[v] = ms.raw[s0][v][lane];
         to_prim(u, g.gamma, wa);
+        fetch_row(ms.raw[s0], uin, vs, (int64_t)(ib + 1) * pitch + jl, lane);  // row ib-2 is converted
 #pragma unroll
-        for (int v = 0; v < NV; ++v) u[v] = ms.raw[(ib - 1) & 3][v][lane];
-        to_prim(u, g.gamma, wb);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) u[v] = ms.raw[ib & 3][v][lane];
+        for (int v = 0; v < NV; ++v) u[v] = ms.raw[s1i][v][lane];
         to_prim(u, g.gamma, w0);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) u[v] = ms.raw[(ib + 1) & 3][v][lane];
+        for (int v = 0; v < NV; ++v) u[v] = ms.raw[s2i][v][lane];
         to_prim(u, g.gamma, w1);
-        R wl[NV], wr[NV], f[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-            const R sm1 = cell_slope(wa[v], wb[v], w0[v], lim);
-            const R s0 = cell_slope(wb[v], w0[v], w1[v], lim);
-            ms.sx[v][lane] = s0;
-            wl[v] = wb[v] + R(0.5) * sm1;
-            wr[v] = w0[v] - R(0.5) * s0;
-        }
-        face_flux(wl, wr, gam, igm1, chr, half_ich, f);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) ms.fx[ib & 1][v][lane] = f[v];
-        bxm = wb[BX];
+        for (int v = 0; v < NV; ++v) ms.sx[v][lane] = cell_slope(wa[v], w0[v], w1[v], lim);  // row ib-1
     }
-    // row ib+2 replaces row ib-2, whose values the prologue has used
-    fetch_row(ms.raw[(ib + 2) & 3], uin, vs, (int64_t)(ib + 2) * pitch + jl, lane);
+    s0 = s1i;  // slot of row ib-1
 
-    for (int i = ib; i < ie; ++i) {
-        const int par = i & 1;
-        fetch_wait();  // row i+2 of the input and U0 of row i have landed
-        // one row ahead: row i+3 replaces row i-1 (done with since the last
-        // iteration), and U0 of row i+1 replaces that of row i-1
-        if (i + 1 < ie) {
-            fetch_row(ms.raw[(i + 3) & 3], uin, vs, (int64_t)(i + 3) * pitch + jl, lane);
-            if (own_base) fetch_row(ms.base[par ^ 1], u0, vs, (int64_t)(i + 1) * pitch + jl, lane);
-        }
-        // y: slope of this lane's cell of row i from its lane neighbours, and
-        // the flux through the face on the cell's left (rotated slot order of
-        // physics.py:376-379); the right face is the next lane's left face
-        __syncwarp();  // the left neighbour has read ms.fy[par] of row i-2
+    for (int i = ib - 1; i < ie; ++i) {
+        const bool full = i >= ib;  // warp-uniform: iteration ib-1 only prepares face ib-1/2
+        const int s2 = s0 == 0 ? 2 : s0 - 1;  // slot of row i+2 (== (i + 2) % 3)
+        __syncwarp();  // the left neighbour has read ms.fy of row i-1
         R bym = R(0), byp = R(0);
-        {
+        if (full) {
+            // y: slope of this lane's cell of row i from its lane neighbours, and
+            // the flux through the face on the cell's left (rotated slot order of
+            // physics.py:376-379); the right face is the next lane's left face
             R wl[NV], wr[NV], f[NV];
 #pragma unroll
             for (int k = 0; k < NV; ++k) {
@@ -651,16 +656,17 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
             }
             face_flux(wl, wr, gam, igm1, chr, half_ich, f);
 #pragma unroll
-            for (int k = 0; k < NV; ++k) ms.fy[par][rot[k]][lane] = f[k];
+            for (int k = 0; k < NV; ++k) ms.fy[rot[k]][lane] = f[k];
         }
-        // x: primitives of row i+2, slope of row i+1 and the flux through face i+1/2
-        R w2[NV];
+        // x: primitives of row i+2, slope of row i+1, flux through face i+1/2 and
+        // the x-flux difference of row i
+        fetch_wait();  // input row i+2 and U0 of row i have landed
+        R w2[NV], dfx[NV];
         {
-            R u[NV];
+            R u[NV], wl[NV], wr[NV], f[NV];
 #pragma unroll
-            for (int v = 0; v < NV; ++v) u[v] = ms.raw[(i + 2) & 3][v][lane];
+            for (int v = 0; v < NV; ++v) u[v] = ms.raw[s2][v][lane];
             to_prim(u, g.gamma, w2);
-            R wl[NV], wr[NV], f[NV];
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 const R s1 = cell_slope(w0[v], w1[v], w2[v], lim);
@@ -670,26 +676,32 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
             }
             face_flux(wl, wr, gam, igm1, chr, half_ich, f);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) ms.fx[par ^ 1][v][lane] = f[v];
-        }
-        __syncwarp();  // every lane's y-face flux of row i is in ms.fy[par]
-        if (out_lane) {
-            R fxl[NV], fxr[NV], fyl[NV], fyr[NV];
-#pragma unroll
             for (int v = 0; v < NV; ++v) {
-                fxl[v] = ms.fx[par][v][lane];
-                fxr[v] = ms.fx[par ^ 1][v][lane];
-                fyl[v] = ms.fy[par][v][lane];
-                fyr[v] = ms.fy[par][v][lane + 1];  // output lanes stop at 29
+                dfx[v] = f[v] - ms.fx[v][lane];
+                ms.fx[v][lane] = f[v];
             }
-            auto pw = [&]() {
-                return PowellIn<R>{w0[BX], bxm, w1[BX], w0[BY], bym, byp, w0[IVX], w0[IVY], w0[IVZ], w0[BZ]};
-            };
-            const int slot = i & 3;
-            auto in_at = [&](int v) { return ms.raw[slot][v][lane]; };
-            auto base_at = [&](int v) { return own_base ? ms.base[par][v][lane] : ms.raw[slot][v][lane]; };
-            update_cell<R, STAGE>(p, g, uout, i, j, fxl, fxr, fyl, fyr, pw, base_at, in_at, dt, ch, decay, q, bad);
         }
+        if (full) {
+            __syncwarp();  // every lane's y-face flux of row i is in ms.fy
+            if (out_lane) {
+                R dfy[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) dfy[v] = ms.fy[v][lane + 1] - ms.fy[v][lane];  // output lanes stop at 29
+                auto pw = [&]() {
+                    return PowellIn<R>{w0[BX], bxm, w1[BX], w0[BY], bym, byp, w0[IVX], w0[IVY], w0[IVZ], w0[BZ]};
+                };
+                const int slot = s0;
+                auto in_at = [&](int v) { return ms.raw[slot][v][lane]; };
+                auto base_at = [&](int v) { return own_base ? ms.base[v][lane] : ms.raw[slot][v][lane]; };
+                update_cell_d<R, STAGE, false>(p, g, uout, i, j, dfx, dfy, pw, base_at, in_at, dt, ch, decay, q, bad);
+            }
+        }
+        // rows done with: input row i (slot s0) -> row i+3; U0 of row i -> row i+1
+        if (i + 1 < ie) {
+            fetch_row(ms.raw[s0], uin, vs, (int64_t)(i + 3) * pitch + jl, lane);
+            if (own_base) fetch_row(ms.base, u0, vs, (int64_t)(i + 1) * pitch + jl, lane);
+        }
+        s0 = s0 == 2 ? 0 : s0 + 1;
         bxm = w0[BX];
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -701,11 +713,12 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
 }
 
 // resident CTAs of kMarchThreads per SM the register budget is shaped for
-template <typename R>
-constexpr int kMarchMinBlocks = kFast<R> ? 4 : 2;
+// (float32: stage 3 carries the CFL maxima and keeps a larger budget)
+template <typename R, int STAGE>
+constexpr int kMarchMinBlocks = kFast<R> ? (STAGE == 3 ? 4 : 5) : 2;
 
 template <typename R, int STAGE>
-__global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R>)) march_stage_kernel(
+__global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) march_stage_kernel(
     const __grid_constant__ StageParams p)
 {
     extern __shared__ __align__(16) unsigned char march_smem[];
@@ -740,13 +753,12 @@ __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R>)) march_sta
 // interior source, so one pass in any order reproduces the reference.
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void bc_fill_kernel(const amhd_grid g, R *U)
+__device__ __forceinline__ void fill_ghosts(const amhd_grid &g, R *U, int64_t first, int64_t step)
 {
     const int nxt = g.nx + 2 * NG, nyt = g.ny + 2 * NG;
     const int64_t n_rows = 4LL * nyt;  // x-ghost rows, full length
     const int64_t n_total = n_rows + 4LL * g.nx;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n_total;
-         k += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t k = first; k < n_total; k += step) {
         int i, j;
         if (k < n_rows) {
             const int r = (int)(k / nyt);
@@ -766,6 +778,24 @@ __global__ void bc_fill_kernel(const amhd_grid g, R *U)
             U[v * g.var_stride + (int64_t)i * g.pitch + j] = val;
         }
     }
+}
+
+template <typename R>
+__global__ void bc_fill_kernel(const amhd_grid g, R *U)
+{
+    fill_ghosts(g, U, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+// ghost fill of a marching stage's output, every instance of the stage
+// (blockIdx.y = instance); instances whose loop has stopped are skipped
+template <typename R>
+__global__ void march_bc_fill_kernel(const __grid_constant__ StageParams p)
+{
+    const int k = blockIdx.y;
+    const amhd_instance &in = p.inst ? p.inst[k] : p.one;
+    if (p.use_ctl && !p.ctl[k].active) return;
+    fill_ghosts(in.grid, reinterpret_cast<R *>(p.uout) + in.offset, blockIdx.x * (int64_t)blockDim.x + threadIdx.x,
+                (int64_t)gridDim.x * blockDim.x);
 }
 
 // ---------------------------------------------------------------------------

@@ -30,6 +30,7 @@ struct StageParams {
     int32_t use_ctl;               // take dt / ch / decay / active from ctl
     int32_t fuse_dt;               // stage 3: accumulate the CFL reduction
     int32_t march_rows;            // warp-marching kernel: rows of one work item
+    int32_t n_inst;                // instances in inst (ghost fill after a marching stage)
 };
 
 // Work geometry of the stage kernels, passed around as one int "tile_x":

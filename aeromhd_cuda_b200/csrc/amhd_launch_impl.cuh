@@ -112,13 +112,21 @@ cudaError_t Launch<R>::stage(int stage, int tile_x, const StageParams &p, int gr
         if (grid <= 0 || grid > need) grid = need;
         StageParams q = p;
         q.march_rows = -tile_x;
+        cudaError_t e;
         switch (stage) {
         case 0: return launch_march_t<R, 0>(q, grid, s);
-        case 1: return launch_march_t<R, 1>(q, grid, s);
-        case 2: return launch_march_t<R, 2>(q, grid, s);
-        case 3: return launch_march_t<R, 3>(q, grid, s);
+        case 1: e = launch_march_t<R, 1>(q, grid, s); break;
+        case 2: e = launch_march_t<R, 2>(q, grid, s); break;
+        case 3: e = launch_march_t<R, 3>(q, grid, s); break;
         default: return cudaErrorInvalidValue;
         }
+        if (e != cudaSuccess) return e;
+        // the marching kernel leaves the ghost cells of its output to this pass
+        const int n_inst = p.inst ? p.n_inst : 1;
+        if (n_inst <= 0) return cudaErrorInvalidValue;
+        const int per = p.inst ? 8 : elem_blocks(4LL * (p.one.grid.ny + 2 * NG) + 4LL * p.one.grid.nx);
+        march_bc_fill_kernel<R><<<dim3(per, n_inst), 256, 0, s>>>(q);
+        return cudaGetLastError();
     }
     if (grid <= 0) grid = p.n_tiles;
     switch (tile_x) {
