@@ -21,6 +21,8 @@ AMHD_ERR_UNSUPPORTED = -5
 AMHD_F64 = 0
 AMHD_F32 = 1
 LIMITER_CODES = {"vanleer": 0, "minmod": 1}
+# stage-kernel geometry the library starts with (amhd_set_tiling): warp-marching, 16 rows per item
+DEFAULT_TILE_X = -16
 
 AMHD_FLAG_NONFINITE = 1
 AMHD_FLAG_DT_TINY = 2

@@ -39,7 +39,7 @@ int fail(int code, const char *fmt, ...)
 constexpr int kNG = 2;
 constexpr int kTY = 32;
 
-int g_tile_x = 8;
+int g_tile_x = -16;  // warp-marching kernel, 16 rows per work item
 int g_ctas_per_sm = 0;
 int g_use_tma = 1;
 

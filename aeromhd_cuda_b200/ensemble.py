@@ -145,7 +145,7 @@ class _GridView:
 
 
 class Ensemble:
-    def __init__(self, configs: Sequence[Config], tile_x: int = 8, order: str = "instance", ctas: int = 0,
+    def __init__(self, configs: Sequence[Config], tile_x: int = -16, order: str = "instance", ctas: int = 0,
                  device=None, use_tma: bool = True):
         if not configs:
             raise ValueError("empty ensemble")

@@ -44,7 +44,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
@@ -53,7 +53,7 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--tma", type=int, default=1, help="stage tiles with TMA (1) or 128-bit loads (0)")
-    ap.add_argument("--tile-x", type=int, default=8,
+    ap.add_argument("--tile-x", type=int, default=-16,
                     help="stage kernel geometry: 4, 8, 16 (tiled kernel rows) or negative (warp-marching rows)")
     ap.add_argument("--ensemble", type=int, default=0,
                     help="also time the batched shock-interface ensemble of this many instances")
@@ -75,6 +75,11 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def launches_per_step(tile_x):
+    """Kernels of one run-loop step: 3 stages (+ 3 ghost fills with the marching kernel) + finalize."""
+    return 3 + (3 if tile_x < 0 else 0) + 1
 
 
 def stage_kernel_name(tile_x):
@@ -105,7 +110,7 @@ def profile_traffic(tile_x):
 class ClockSampler:
     """NVML clock / throttle-reason sampling during the timed region (read only)."""
 
-    def __init__(self, device_index: int, period_s: float = 0.2):
+    def __init__(self, device_index: int, period_s: float = 0.01):
         self.samples = []
         self.period = period_s
         self._stop = threading.Event()
@@ -363,7 +368,7 @@ def run_ours(a, world, rank, local):
                    "parallelism": f"replicas x{world}", "stage_kernel": stage_geometry(a.tile_x),
                    "staging": ("cp.async rows" if a.tile_x < 0 else
                                "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads")},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * a.steps,
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step(a.tile_x) * a.steps,
         "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
     }
     return line

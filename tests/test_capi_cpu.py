@@ -59,7 +59,11 @@ def test_argument_errors_are_codes_not_crashes(L):
     assert b"2x2" in L.amhd_last_error()
     assert L.amhd_padded_layout(8, 8, 7, ctypes.byref(p), ctypes.byref(r)) == _lib.AMHD_ERR_ARG
     assert L.amhd_set_tiling(5, 0) == _lib.AMHD_ERR_ARG
+    assert L.amhd_set_tiling(-3, 0) == _lib.AMHD_ERR_ARG      # marching items need at least 4 rows
+    assert L.amhd_set_tiling(-2000, 0) == _lib.AMHD_ERR_ARG
     assert L.amhd_set_tiling(8, 0) == _lib.AMHD_OK
+    assert L.amhd_set_tiling(-16, 0) == _lib.AMHD_OK
+    assert L.amhd_set_tiling(_lib.DEFAULT_TILE_X, 0) == _lib.AMHD_OK
     g = _lib.Grid(nx=8, ny=8, pitch=4, dtype=0, var_stride=1000, dx=0.1, dy=0.1, gamma=1.4, cfl=0.3,
                   glm_alpha=1.5)
     # pitch < ny+4 is refused before any device call

@@ -13,18 +13,19 @@ def small_configs(precision, n=6, seed=11):
     return draw_configs(n, seed=seed, t_end=3.0, precision=precision, ny_choices=(32, 64))
 
 
+@pytest.mark.parametrize("tile_x", [8, -16])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-def test_instances_equal_single_grid_runs(precision):
+def test_instances_equal_single_grid_runs(precision, tile_x):
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200.ensemble import Ensemble
     from aeromhd_cuda_b200.solver import MHDSolver
     cfgs = small_configs(precision)
-    ens = Ensemble(cfgs, tile_x=8)
+    ens = Ensemble(cfgs, tile_x=tile_x)
     ens.initialize()
     ens.start(max_steps=12)
     ens.advance(12)
     ctl = ens.controls()
-    _lib.call("amhd_set_tiling", 8, 0)
+    _lib.call("amhd_set_tiling", tile_x, 0)
     for k, c in enumerate(cfgs):
         s = MHDSolver(c)
         s.initialize()

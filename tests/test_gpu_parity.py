@@ -25,7 +25,7 @@ def amhd():
     import aeromhd_cuda_b200.physics as physics
     import aeromhd_cuda_b200.solver as solver
     from aeromhd_cuda_b200 import _lib, config
-    _lib.call("amhd_set_tiling", 8, 0)
+    _lib.call("amhd_set_tiling", _lib.DEFAULT_TILE_X, 0)
     return type("M", (), dict(physics=physics, solver=solver, lib=_lib, config=config))
 
 
@@ -107,7 +107,7 @@ def test_three_steps_bit_exact(amhd, k, tile_x):
         assert np.array_equal(np_(s.U), g[f"U3_{k}"])
         np.testing.assert_allclose(s._cumulative_boundary_energy, g[f"ebnd_{k}"], rtol=1e-12, atol=1e-15)
     finally:
-        amhd.lib.call("amhd_set_tiling", 8, 0)
+        amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, 0)
 
 
 def test_single_routines_bit_exact(amhd):
@@ -373,7 +373,7 @@ def test_marching_kernel_matches_tiled(amhd, precision, shape, rows):
             s.advance(max_steps=9, chunk=9, graph=False)
             res.append((s.U.clone(), s.t))
     finally:
-        amhd.lib.call("amhd_set_tiling", 8, 0)
+        amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, 0)
     (a, ta), (b, tb) = res
     if precision == "fp64":
         assert ta == tb
@@ -398,7 +398,7 @@ def test_marching_kernel_rmi_device_loop_bit_exact(amhd, bcx):
             s.advance(max_steps=25, chunk=25, graph=False)
             res.append((s.U.clone(), s.t, s._cumulative_boundary_energy))
     finally:
-        amhd.lib.call("amhd_set_tiling", 8, 0)
+        amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, 0)
     (a, ta, ea), (b, tb, eb) = res
     assert ta == tb and ea == eb
     assert torch.equal(a, b)
