@@ -83,6 +83,7 @@ _SIGS = {
     "amhd_step_host": ([_c.POINTER(Grid), _P, _P, _P, _P, _P, _D, _D, _c.POINTER(_D), _P], _c.c_int),
     "amhd_diagnostics": ([_c.POINTER(Grid), _P, _D, _P, _P, _P], _c.c_int),
     "amhd_diagnostics_noalloc": ([_c.POINTER(Grid), _P, _D, _P, _P], _c.c_int),
+    "amhd_diagnostics_colour": ([_c.POINTER(Grid), _P, _D, _P, _P, _P, _P], _c.c_int),
     "amhd_ensemble_advance": ([_P, _I32, _P, _P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _I32, _P, _P], _c.c_int),
     "amhd_ensemble_tensormaps": ([_P, _I32, _I32, _I32, _P, _P, _P, _P], _c.c_int),
     "amhd_set_tma": ([_I32], _c.c_int),
@@ -106,6 +107,8 @@ _SIGS = {
     "amhd_nn_restrict": ([_c.POINTER(Grid), _P, _I32, _P, _I64, _I32, _I32, _P], _c.c_int),
     "amhd_nn_pack": ([_c.POINTER(Grid), _P, _P, _P, _P, _I64, _I32, _P], _c.c_int),
     "amhd_nn_apply": ([_c.POINTER(Grid), _P, _P, _P, _I64, _I32, _P], _c.c_int),
+    "amhd_nn_apply_guarded": ([_c.POINTER(Grid), _P, _P, _P, _I64, _I32, _c.c_float, _c.c_float, _P, _P],
+                              _c.c_int),
 }
 
 _lib = None

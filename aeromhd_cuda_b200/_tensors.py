@@ -94,6 +94,15 @@ def control_tensor(n: int = 1, device="cuda") -> torch.Tensor:
     return torch.zeros((n, size), dtype=torch.uint8, device=device)
 
 
+def write_controls(ctl: torch.Tensor, controls) -> None:
+    """List of ctypes Control -> device control blocks (synchronous copy)."""
+    size = ctypes.sizeof(_lib.Control)
+    raw = bytearray(size * len(controls))
+    for k, c in enumerate(controls):
+        raw[k * size:(k + 1) * size] = bytes(c)
+    ctl.copy_(torch.frombuffer(raw, dtype=torch.uint8).view(len(controls), size))
+
+
 def read_controls(ctl: torch.Tensor):
     """Device control blocks -> list of ctypes Control (synchronises)."""
     raw = ctl.cpu().numpy()

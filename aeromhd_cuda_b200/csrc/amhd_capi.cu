@@ -681,6 +681,19 @@ int amhd_diagnostics(const amhd_grid *g, const void *U, double x0, double *out_d
     return AMHD_OK;
 }
 
+int amhd_diagnostics_colour(const amhd_grid *g, const void *U, double x0, const double *rows_dev, double *cp2_dev,
+                            double *pos_dev, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !rows_dev || !cp2_dev || !pos_dev) return fail(AMHD_ERR_ARG, "NULL argument");
+    cudaStream_t s = S(stream);
+    if (g->dtype == AMHD_F64)
+        CK(Launch<double>::diag_colour(*g, static_cast<const double *>(U), x0, rows_dev, cp2_dev, pos_dev, s));
+    else
+        CK(Launch<float>::diag_colour(*g, static_cast<const float *>(U), x0, rows_dev, cp2_dev, pos_dev, s));
+    return AMHD_OK;
+}
+
 int amhd_ensemble_init(const amhd_instance *inst_host, const amhd_instance *inst_dev, int32_t n_inst, int32_t dtype,
                        void *U, amhd_control *ctl_dev, double t_end, int64_t max_steps, void *stream)
 {

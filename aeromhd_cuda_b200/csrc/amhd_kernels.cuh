@@ -961,7 +961,12 @@ __global__ void dt_reduce_kernel(const Layout l, const R *A, int from_prim, doub
             R u[NV];
 #pragma unroll
             for (int v = 0; v < NV; ++v) u[v] = A[v * l.var_stride + c];
-            cfl_quantities(u, gamma, qd);
+            // float32 state: the arithmetic of the stage kernels' fused reduction,
+            // so that a run resumed from a stored state takes the same dt
+            if constexpr (kFast<R>)
+                fast::cfl_quantities(u, gamma, qd);
+            else
+                cfl_quantities(u, gamma, qd);
         }
 #pragma unroll
         for (int m = 0; m < 4; ++m) q[m] = umax64(q[m], ord_bits(qd[m]));
@@ -1113,6 +1118,106 @@ __global__ void finalize_kernel(const amhd_instance *insts, const amhd_instance 
 //   row pass: per interior x-row i, sum_j clip(C), sum_j rho, sum_j E,
 //   sum_j rho w^2 and row maxima of |divB| and stagnation pressure; sum divB^2
 // ---------------------------------------------------------------------------
+// Colour-field diagnostics of solver.py:353-417 that look at the field again
+// after the row sums: the clipped colour C = clip(rhoC / max(rho, floor), 0, 1)
+// in double, as diag_rows_kernel computes it.
+template <typename R>
+__device__ __forceinline__ double clipped_colour(const amhd_grid &g, const R *U, int i, int j)
+{
+    const int64_t c = (int64_t)i * g.pitch + j;
+    const double rho = np_max((double)U[RHO * g.var_stride + c], FLOOR_RHO);
+    const double ri = 1.0 / rho;
+    return fmin(fmax((double)U[RHOC * g.var_stride + c] * ri, 0.0), 1.0);
+}
+
+// numpy's pairwise summation of a short array (n <= 128: eight running sums
+// combined as ((r0+r1)+(r2+r3))+((r4+r5)+(r6+r7)), then the remainder in
+// order; below 8 elements a plain loop), so that a sum the reference takes
+// with numpy.sum comes out with the same bits
+__device__ __forceinline__ double np_pairwise_sum(const double *a, int n)
+{
+    if (n < 8) {
+        double res = 0.0;
+        for (int k = 0; k < n; ++k) res += a[k];
+        return res;
+    }
+    double r[8];
+    for (int k = 0; k < 8; ++k) r[k] = a[k];
+    int k = 8;
+    for (; k < n - (n % 8); k += 8)
+        for (int m = 0; m < 8; ++m) r[m] += a[k + m];
+    double res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+    for (; k < n; ++k) res += a[k];
+    return res;
+}
+
+// one block per interior row: sum over y of (C - Cbar)^2 with Cbar = csum[r] / ny
+// (C_prime_sq of solver.py:360 times ny)
+template <typename R>
+__global__ void diag_colour_rows_kernel(const amhd_grid g, const R *U, const double *csum, double *cp2)
+{
+    const int r = blockIdx.x;
+    const double cbar = csum[r] / g.ny;
+    double s = 0.0;
+    for (int jj = threadIdx.x; jj < g.ny; jj += blockDim.x) {
+        const double d = clipped_colour(g, U, NG + r, NG + jj) - cbar;
+        s += d * d;
+    }
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        cp2[r] = t;
+    }
+}
+
+// One thread per interior column j: the interface position of solver.py:368-383
+// -- |dC/dx| as numpy.gradient takes it along x (central differences inside,
+// one-sided at the two ends), its first maximum over the column, and the
+// |dC/dx|-weighted mean of x over up to 10 rows either side of it; NaN when the
+// column's maximum is <= 1e-6, the window is empty or the weights sum to <= 1e-12.
+template <typename R>
+__global__ void diag_interface_kernel(const amhd_grid g, const R *U, double x0, double *pos)
+{
+    const int nx = g.nx;
+    const double dx = g.dx;
+    for (int jj = blockIdx.x * blockDim.x + threadIdx.x; jj < g.ny; jj += gridDim.x * blockDim.x) {
+        const int j = NG + jj;
+        auto grad = [&](int r) -> double {
+            if (r == 0) return fabs((clipped_colour(g, U, NG + 1, j) - clipped_colour(g, U, NG, j)) / dx);
+            if (r == nx - 1)
+                return fabs((clipped_colour(g, U, NG + nx - 1, j) - clipped_colour(g, U, NG + nx - 2, j)) / dx);
+            return fabs((clipped_colour(g, U, NG + r + 1, j) - clipped_colour(g, U, NG + r - 1, j)) / (2.0 * dx));
+        };
+        double best = -1.0;
+        int ip = 0;
+        for (int r = 0; r < nx; ++r) {
+            const double d = grad(r);
+            if (d > best) {
+                best = d;
+                ip = r;
+            }
+        }
+        double out = __longlong_as_double(0x7ff8000000000000LL);  // NaN
+        const int hw = min(10, min(ip, nx - ip - 1));
+        if (best > 1e-6 && hw > 0) {
+            double wgt[21], xw[21];
+            const int n = 2 * hw + 1;
+            for (int k = 0; k < n; ++k) {
+                const int r = ip - hw + k;
+                wgt[k] = grad(r);
+                xw[k] = (x0 + ((double)r + 0.5) * dx) * wgt[k];
+            }
+            const double ws = np_pairwise_sum(wgt, n);
+            if (ws > 1e-12) out = np_pairwise_sum(xw, n) / ws;
+        }
+        pos[jj] = out;
+    }
+}
+
 template <typename R>
 __global__ void diag_rows_kernel(const amhd_grid g, const R *U, double *rows)
 {

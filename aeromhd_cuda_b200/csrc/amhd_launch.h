@@ -70,6 +70,8 @@ struct Launch {
     static cudaError_t finalize(const amhd_instance *insts, int n_inst, const amhd_instance &one, const R *U,
                                 amhd_control *ctl, int advance, int set_only, cudaStream_t s);
     static cudaError_t diag_rows(const amhd_grid &g, const R *U, double *rows, cudaStream_t s);
+    static cudaError_t diag_colour(const amhd_grid &g, const R *U, double x0, const double *csum, double *cp2,
+                                   double *pos, cudaStream_t s);
     static cudaError_t bflux(const amhd_grid &g, const R *U, double *out, cudaStream_t s);
     static cudaError_t bflux_accum(const amhd_grid &g, const R *U, amhd_control *ctl, double dt, cudaStream_t s);
 };

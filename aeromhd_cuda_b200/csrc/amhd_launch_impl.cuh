@@ -239,6 +239,17 @@ cudaError_t Launch<R>::finalize(const amhd_instance *insts, int n_inst, const am
 }
 
 template <typename R>
+cudaError_t Launch<R>::diag_colour(const amhd_grid &g, const R *U, double x0, const double *csum, double *cp2,
+                                   double *pos, cudaStream_t s)
+{
+    diag_colour_rows_kernel<R><<<g.nx, 256, 0, s>>>(g, U, csum, cp2);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    diag_interface_kernel<R><<<(g.ny + 127) / 128, 128, 0, s>>>(g, U, x0, pos);
+    return cudaGetLastError();
+}
+
+template <typename R>
 cudaError_t Launch<R>::diag_rows(const amhd_grid &g, const R *U, double *rows, cudaStream_t s)
 {
     diag_rows_kernel<R><<<g.nx, 256, 0, s>>>(g, U, rows);

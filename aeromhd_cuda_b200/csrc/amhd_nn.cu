@@ -394,6 +394,45 @@ __global__ void apply_kernel(R *U, int pitch, int64_t vs, int nx, int ny, const 
     }
 }
 
+// The same, cell by cell and kept admissible: U_cell += alpha scale_v y[v] only
+// when the corrected cell is finite and keeps at least min_ratio of its
+// density and of its pressure p = (gamma-1)(E - |m|^2/2rho - |B|^2/2) (float64);
+// otherwise the cell keeps its state and *rejected counts it.
+template <typename R>
+__global__ void apply_guarded_kernel(R *U, int pitch, int64_t vs, int nx, int ny, double gamma, const float *scale,
+                                     const float *y, int64_t y_vs, int b, float alpha, float min_ratio,
+                                     int *rejected)
+{
+    const int64_t total = (int64_t)nx * ny;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(k % ny), i = (int)(k / ny);
+        const int64_t c = (int64_t)(i + 2) * pitch + j + 2;
+        const int64_t yc = ((int64_t)b * nx + i) * ny + j;
+        double u[10], w[10];
+        bool ok = true;
+#pragma unroll
+        for (int v = 0; v < 10; ++v) {
+            u[v] = (double)U[v * vs + c];
+            w[v] = (double)(R)((float)U[v * vs + c] + alpha * scale[v] * y[(int64_t)v * y_vs + yc]);
+            ok = ok && isfinite(w[v]);
+        }
+        auto pressure = [&](const double *s) {
+            const double m2 = s[1] * s[1] + s[2] * s[2] + s[3] * s[3];
+            const double b2 = s[4] * s[4] + s[5] * s[5] + s[6] * s[6];
+            return (gamma - 1.0) * (s[7] - 0.5 * m2 / s[0] - 0.5 * b2);
+        };
+        if (ok) ok = u[0] > 0.0 && w[0] >= (double)min_ratio * u[0];
+        if (ok) ok = pressure(w) >= (double)min_ratio * pressure(u);
+        if (ok) {
+#pragma unroll
+            for (int v = 0; v < 10; ++v) U[v * vs + c] = (R)w[v];
+        } else if (rejected != nullptr) {
+            atomicAdd(rejected, 1);
+        }
+    }
+}
+
 }  // namespace
 
 #pragma GCC visibility push(default)
@@ -569,6 +608,24 @@ int amhd_nn_apply(const amhd_grid *g, void *U, const float *scale, const float *
     else
         apply_kernel<float><<<blocks_for(n), 256, 0, S(stream)>>>(static_cast<float *>(U), g->pitch, g->var_stride,
                                                                    g->nx, g->ny, scale, y, y_vs, b);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_apply_guarded(const amhd_grid *g, void *U, const float *scale, const float *y, int64_t y_vs, int32_t b,
+                          float alpha, float min_ratio, int32_t *rejected_dev, void *stream)
+{
+    if (!g || !U || !scale || !y) return nn_fail(AMHD_ERR_ARG, "bad apply arguments");
+    if (!(min_ratio >= 0.f && min_ratio <= 1.f)) return nn_fail(AMHD_ERR_ARG, "min_ratio must be in [0, 1]");
+    const int64_t n = (int64_t)g->nx * g->ny;
+    if (g->dtype == AMHD_F64)
+        apply_guarded_kernel<double><<<blocks_for(n), 256, 0, S(stream)>>>(
+            static_cast<double *>(U), g->pitch, g->var_stride, g->nx, g->ny, g->gamma, scale, y, y_vs, b, alpha,
+            min_ratio, rejected_dev);
+    else
+        apply_guarded_kernel<float><<<blocks_for(n), 256, 0, S(stream)>>>(
+            static_cast<float *>(U), g->pitch, g->var_stride, g->nx, g->ny, g->gamma, scale, y, y_vs, b, alpha,
+            min_ratio, rejected_dev);
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }

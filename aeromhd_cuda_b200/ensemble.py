@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import _lib, initial_conditions
-from ._tensors import NG, control_tensor, read_controls, stream_ptr, torch_dtype
+from ._tensors import NG, control_tensor, read_controls, stream_ptr, torch_dtype, write_controls
 from .config import Config, bc_x_code, bc_y_code
 from .physics import prim_to_cons
 
@@ -272,6 +272,26 @@ class Ensemble:
 
     def controls(self):
         return read_controls(self.ctl)
+
+    def set_state(self, k: int, U) -> None:
+        """Load instance k's conserved state ([10, nx+4, ny+4], ghosts included)."""
+        v = self.state(k)
+        src = torch.as_tensor(U)
+        if tuple(src.shape) != tuple(v.shape):
+            raise ValueError(f"instance {k}: state must have shape {tuple(v.shape)}, got {tuple(src.shape)}")
+        v.copy_(src.to(device=self.device, dtype=self.dtype))
+        self._graphs = {}
+
+    def resume(self, t, step, e_bnd, t_end: float, max_steps: int = 1 << 62) -> None:
+        """Continue every instance from its own saved time, step count and boundary
+        energy (sequences of length n) toward t_end: dt and ch from the states, as
+        at a loop head."""
+        self.start(t_end=t_end, max_steps=max_steps)
+        ctl = self.controls()
+        for k, c in enumerate(ctl):
+            c.t, c.step, c.e_bnd = float(t[k]), int(step[k]), float(e_bnd[k])
+        write_controls(self.ctl, ctl)
+        self.continue_to(t_end)
 
     def run(self, chunk: int = 50, max_chunks: int = 1 << 30):
         """Advance until every instance reached its end time; returns steps per instance."""

@@ -3,19 +3,23 @@
     python -m aeromhd_cuda_b200.learned --train-seeds 100 --test-seeds 64
 
 Data: shocked-interface runs drawn like the batched ensemble (Mach, density
-ratio, mode, amplitude, field), each run twice from the same parameters --
-coarse (nx x ny) and 4x finer -- as two GPU ensembles; at every snapshot time
-(0.1, 0.2, ... 3.0) the pair (coarse state, fine state restricted onto the
-coarse grid) is kept.  Runs use the frame of the shocked gas so that the
-mixing layer stays in the domain until t = 3.  Seeds split 90/10 into
-training and validation; separate test seeds judge the result.
+ratio, mode, amplitude, field), each on a coarse (nx x ny) and a 4x finer
+grid, as GPU ensembles.  The corrector learns the error the coarse solver
+makes over one correction interval `delta` starting from a good state: at
+every start time t_k (0, 0.1, ... 2.9) the fine state is restricted onto the
+coarse grid (4x4 block averages), the coarse solver advances it by delta, and
+the pair (that coarse state, the fine state at t_k + delta restricted) is
+kept; the target is their difference.  Runs use the frame of the shocked gas
+so that the mixing layer stays in the domain until t = 3.  Seeds split 90/10
+into training and validation; separate test seeds judge the result.
 
-Use: during a coarse run the corrector is applied every `apply_every` coarse
-steps of each instance.  It is judged against the plain fine solve on
-mixing width, spectral energy and div B; an instance falls back to the plain
-fine solve when its corrected run leaves the trusted range (non-finite
-values, corrections far outside the training distribution, div B above a
-tolerance).
+Use: a corrected coarse run adds the corrector's output every `delta` of
+simulated time (all instances of an ensemble together).  It is judged
+against the plain fine solve on mixing width, spectral energy and div B; an
+instance falls back to the plain fine solve when its corrected run leaves the
+trusted range (non-finite or far out-of-range corrections, a correction that
+collapses the time step, a step count far above the plain coarse run's, div B
+above a tolerance).
 
 No counterpart in the reference.
 """
@@ -33,11 +37,13 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._tensors import ptr, stream_ptr
+from ._tensors import ptr, stream_ptr, write_controls
 from .corrector import Corrector
 from .ensemble import Ensemble, draw_configs
 
-T_SNAPS = tuple(round(0.1 * k, 10) for k in range(1, 31))
+T_SNAPS = tuple(round(0.1 * k, 10) for k in range(1, 31))   # evaluation snapshot times
+T_STARTS = tuple(round(0.1 * k, 10) for k in range(0, 30))   # training start times
+DELTA = 0.02                                                 # correction interval (5 per snapshot interval)
 
 
 def paired_configs(seeds: Sequence[int], nyc: int = 64, factor: int = 4, precision: str = "fp32"):
@@ -54,38 +60,55 @@ def _interior(ens: Ensemble, k: int) -> torch.Tensor:
     return ens.state(k)[:, 2:-2, 2:-2]
 
 
-def generate_pairs(seeds: Sequence[int], t_snaps: Sequence[float] = T_SNAPS, nyc: int = 64, factor: int = 4,
-                   precision: str = "fp32", log=print):
-    """Returns (X, Y, wall): X[snap][seed] coarse interiors, Y[snap][seed] restricted fine interiors."""
+def _load_restricted(ef: Ensemble, ec: Ensemble, factor: int, buf: torch.Tensor) -> None:
+    """Every coarse instance := its fine instance restricted (interior) + boundary conditions."""
+    for i in range(ec.n):
+        c = ec.configs[i]
+        _lib.call("amhd_nn_restrict", ef._grid(i), ptr(ef.state(i)), factor, ptr(buf), c.nx * c.ny, 0, 1,
+                  stream_ptr())
+        _interior(ec, i).copy_(buf.view(10, c.nx, c.ny))
+        _lib.call("amhd_apply_bc", ec._grid(i), ptr(ec.state(i)), stream_ptr())
+
+
+def _timed_run(e: Ensemble, wall: dict, key: str) -> None:
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e.run(chunk=64)
+    torch.cuda.synchronize()
+    wall[key] += time.perf_counter() - t0
+
+
+def generate_pairs(seeds: Sequence[int], t_starts: Sequence[float] = T_STARTS, delta: float = DELTA, nyc: int = 64,
+                   factor: int = 4, precision: str = "fp32", log=print):
+    """Returns (X, Y, wall): X[k][seed] = the coarse state after `delta` of coarse
+    evolution from the fine state at t_starts[k] restricted; Y[k][seed] = the fine
+    state at t_starts[k] + delta restricted (interiors, float32)."""
     coarse, fine = paired_configs(seeds, nyc, factor, precision)
     ec, ef = Ensemble(coarse), Ensemble(fine)
-    ec.initialize()
     ef.initialize()
     nxc, nyc_ = coarse[0].nx, coarse[0].ny
     n = len(seeds)
-    X = torch.empty((len(t_snaps), n, 10, nxc, nyc_), dtype=torch.float32, device=ec.device)
+    X = torch.empty((len(t_starts), n, 10, nxc, nyc_), dtype=torch.float32, device=ec.device)
     Y = torch.empty_like(X)
+    buf = torch.empty((10, nxc * nyc_), dtype=torch.float32, device=ec.device)
     wall = {"coarse": 0.0, "fine": 0.0}
-    ec.start(t_end=t_snaps[0])
-    ef.start(t_end=t_snaps[0])
-    plane = nxc * nyc_
-    for k, ts in enumerate(t_snaps):
+    ef.start(t_end=t_starts[0])
+    zeros = [0] * n
+    for k, ts in enumerate(t_starts):
         if k:
-            ec.continue_to(ts)
             ef.continue_to(ts)
-        for name, e in (("coarse", ec), ("fine", ef)):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            e.run(chunk=64)
-            torch.cuda.synchronize()
-            wall[name] += time.perf_counter() - t0
+            _timed_run(ef, wall, "fine")
+        _load_restricted(ef, ec, factor, buf)
+        ec.resume([ts] * n, zeros, [0.0] * n, ts + delta)
+        _timed_run(ec, wall, "coarse")
+        ef.continue_to(ts + delta)
+        _timed_run(ef, wall, "fine")
         for i in range(n):
             X[k, i].copy_(_interior(ec, i))
-            g = ef._grid(i)
-            out = Y[k, i]
-            _lib.call("amhd_nn_restrict", g, ptr(ef.state(i)), factor, ptr(out), plane, 0, 1, stream_ptr())
-        if log and (k % 5 == 4 or k == len(t_snaps) - 1):
-            log(f"  pairs at t={ts:.1f}: {n} seeds, wall coarse {wall['coarse']:.1f}s fine {wall['fine']:.1f}s")
+            _lib.call("amhd_nn_restrict", ef._grid(i), ptr(ef.state(i)), factor, ptr(Y[k, i]), nxc * nyc_, 0, 1,
+                      stream_ptr())
+        if log and (k % 5 == 4 or k == len(t_starts) - 1):
+            log(f"  pairs from t={ts:.1f}: {n} seeds, wall coarse {wall['coarse']:.1f}s fine {wall['fine']:.1f}s")
     return X, Y, wall
 
 
@@ -177,51 +200,115 @@ def _ke_spectrum(U: torch.Tensor) -> torch.Tensor:
     return s
 
 
-def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], apply_every: int = 20, nyc: int = 64,
+def _set_limits(e: Ensemble, cap: np.ndarray, stop: np.ndarray) -> None:
+    """Per-instance step cap for the current interval; instances in `stop` are halted."""
+    ctl = e.controls()
+    for i, c in enumerate(ctl):
+        if stop[i]:
+            c.max_steps = int(c.step)
+            c.active = 0
+        else:
+            c.max_steps = int(cap[i])
+    write_controls(e.ctl, ctl)
+
+
+def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: float = DELTA, nyc: int = 64,
              factor: int = 4, t_snaps: Sequence[float] = T_SNAPS, divb_tol: float = 1.0, corr_sigma: float = 8.0,
-             log=print) -> dict:
+             step_factor: float = 3.0, dt_drop: float = 0.5, max_wall: float = 900.0, alpha: float = 1.0,
+             min_ratio: float = 0.5, runs_in=None, log=print) -> dict:
+    """Fine, coarse and corrected runs of the held-out seeds to every snapshot
+    time.  The corrected run adds the correction every `delta` of simulated
+    time; an instance falls back (stops; its plain fine solve stands in) when
+    a correction is non-finite or far outside the training range, when it makes
+    the next dt drop below dt_drop x its value before the correction, or when
+    the instance needs more than step_factor x the plain coarse run's steps
+    between two snapshots.  max_wall bounds the corrected run's wall time.
+    alpha scales the corrections; cells a correction would leave with less than
+    min_ratio of their density or pressure are not corrected.  runs_in: the
+    fine and coarse results of an earlier call on the same seeds (reused)."""
     coarse, fine = paired_configs(seeds, nyc, factor)
     n = len(seeds)
     runs = {}
     walls = {}
     mw = {name: np.zeros((len(t_snaps), n)) for name in ("fine", "coarse", "corrected")}
     divb = {name: np.zeros((len(t_snaps), n)) for name in ("fine", "coarse", "corrected")}
+    coarse_steps = np.zeros((len(t_snaps), n), dtype=np.int64)
     fallback = np.zeros(n, dtype=bool)
+    reasons = {"range": 0, "dt_drop": 0, "steps": 0, "wall": 0, "divB": 0}
+    n_corr = 0
+    rejected = torch.zeros(1, dtype=torch.int32, device="cuda")
+    cells_corrected = 0
+    if runs_in is not None:
+        runs, walls, coarse_steps = dict(runs_in["runs"]), dict(runs_in["walls"]), runs_in["coarse_steps"]
+        for name in ("fine", "coarse"):
+            mw[name], divb[name] = runs_in["mw"][name], runs_in["divb"][name]
     for name, cfgs in (("fine", fine), ("coarse", coarse), ("corrected", coarse)):
+        if name in runs:
+            continue
         e = Ensemble(cfgs)
         e.initialize()
         e.start(t_end=t_snaps[0])
-        last = np.zeros(n, dtype=np.int64)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
+        t_prev = 0.0
+        pending = None   # instances corrected last and their CFL dt before the correction
         for k, ts in enumerate(t_snaps):
-            if k:
-                e.continue_to(ts)
             if name != "corrected":
+                if k:
+                    e.continue_to(ts)
                 e.run(chunk=64)
+                if name == "coarse":
+                    coarse_steps[k] = [c.step for c in e.controls()]
             else:
-                while True:
-                    e.advance(apply_every)
+                start = np.array([c.step for c in e.controls()], dtype=np.int64)
+                interval = coarse_steps[k] - (coarse_steps[k - 1] if k else 0)
+                cap = start + (step_factor * interval).astype(np.int64) + 40
+                m = max(1, int(round((ts - t_prev) / delta)))
+                for q in range(1, m + 1):
+                    tc = ts if q == m else t_prev + q * (ts - t_prev) / m
+                    e.continue_to(tc)           # dt / ch of the (corrected) states
+                    if pending is not None:
+                        due, dt_before = pending
+                        ctl = e.controls()
+                        dt_after = np.array([ctl[i].dt_cfl for i in due])
+                        drop = (dt_after < dt_drop * dt_before) & ~fallback[due]
+                        fallback[due[drop]] = True
+                        reasons["dt_drop"] += int(drop.sum())
+                        pending = None
+                    _set_limits(e, cap, fallback)
+                    e.run(chunk=32)
                     ctl = e.controls()
-                    steps = np.array([c.step for c in ctl])
-                    due = np.nonzero((steps // apply_every > last // apply_every) & ~fallback)[0]
+                    t_now = np.array([c.t for c in ctl])
+                    over = (t_now < tc * (1 - 1e-12)) & ~fallback
+                    if over.any():
+                        fallback |= over
+                        reasons["steps"] += int(over.sum())
+                    if time.perf_counter() - t0 > max_wall:
+                        left = ~fallback
+                        fallback |= left
+                        reasons["wall"] += int(left.sum())
+                    due = np.nonzero(~fallback)[0]
                     if len(due):
-                        ok = _apply_batch(net, norm, e, due, corr_sigma)
+                        dt_before = np.array([ctl[i].dt_cfl for i in due])
+                        ok = _apply_batch(net, norm, e, due, corr_sigma, alpha, min_ratio, rejected)
+                        n_corr += 1
+                        cells_corrected += int(sum(cfgs[i].nx * cfgs[i].ny for i in due[ok]))
                         fallback[due[~ok]] = True
-                    last = steps
-                    if len(due):
-                        e.continue_to(ts)
-                    if not any(c.active for c in e.controls()):
-                        break
+                        reasons["range"] += int((~ok).sum())
+                        pending = (due[ok], dt_before[ok])
+                t_prev = ts
             for i in range(n):
                 mw[name][k, i], divb[name][k, i] = _mixing_width(e, i)
         torch.cuda.synchronize()
         walls[name] = time.perf_counter() - t0
         runs[name] = e
         if log:
-            log(f"  {name}: {walls[name]:.1f}s")
+            log(f"  {name}: {walls[name]:.1f}s" + (f"  corrections {n_corr}, fallback {int(fallback.sum())}/{n} "
+                                                    f"{reasons}" if name == "corrected" else ""))
     # div B gate on the corrected runs
-    fallback |= (divb["corrected"].max(0) > divb_tol) | ~np.isfinite(mw["corrected"]).all(0)
+    gate = ((divb["corrected"].max(0) > divb_tol) | ~np.isfinite(mw["corrected"]).all(0)) & ~fallback
+    reasons["divB"] += int(gate.sum())
+    fallback |= gate
     # spectral energy at the final time (fine restricted to the coarse grid)
     spec_err = np.zeros((2, n))
     nxc, nycc = coarse[0].nx, coarse[0].ny
@@ -241,7 +328,7 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], apply_every
     err_c, err_k = mw_err("coarse"), mw_err("corrected")
     err_final = np.where(fallback, 0.0, err_k)
     out = {
-        "seeds": list(map(int, seeds)), "apply_every": apply_every,
+        "seeds": list(map(int, seeds)), "correction_interval": delta, "corrections": n_corr,
         "wall_s": walls, "speedup_corrected_vs_fine": walls["fine"] / max(walls["corrected"], 1e-12),
         "mixing_width_err_coarse": {"mean": float(err_c.mean()), "median": float(np.median(err_c)),
                                     "max": float(err_c.max())},
@@ -250,16 +337,25 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], apply_every
         "within_2pct": {"coarse": int((err_c <= 0.02).sum()), "corrected": int((err_k <= 0.02).sum()), "of": n},
         "spectral_energy_err": {"coarse": float(spec_err[0].mean()), "corrected": float(spec_err[1].mean())},
         "divB_L2_final": {k: float(v[-1].mean()) for k, v in divb.items()},
-        "fallback_instances": int(fallback.sum()),
+        "fallback_instances": int(fallback.sum()), "fallback_reasons": reasons, "alpha": alpha,
+        "min_ratio": min_ratio, "cells_not_corrected_fraction": float(rejected.item()) / max(cells_corrected, 1),
+        "speedup_with_fallback_fine_solves": walls["fine"] / max(walls["corrected"] +
+                                                                 fallback.mean() * walls["fine"], 1e-12),
         "mixing_width_err_with_fallback": {"mean": float(err_final.mean()), "max": float(err_final.max())},
     }
+    out["_baseline"] = {"runs": {k: runs[k] for k in ("fine", "coarse")},
+                        "walls": {k: walls[k] for k in ("fine", "coarse")}, "coarse_steps": coarse_steps,
+                        "mw": {k: mw[k] for k in ("fine", "coarse")}, "divb": {k: divb[k] for k in ("fine", "coarse")}}
     return out
 
 
-def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma: float) -> np.ndarray:
-    """One forward pass over the instances `idx`; each gets its correction unless it is
-    non-finite or far outside the training range (then it is marked for fallback).
-    Ghost cells are refreshed afterwards."""
+def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma: float, alpha: float = 1.0,
+                 min_ratio: float = 0.5, rejected: torch.Tensor | None = None) -> np.ndarray:
+    """One forward pass over the instances `idx`; each gets alpha x its correction
+    (cells whose corrected density or pressure would fall below min_ratio of the
+    current value keep their state) unless the correction is non-finite or far
+    outside the training range (then it is marked for fallback).  Ghost cells
+    are refreshed afterwards."""
     N = net.H * net.W
     B = len(idx)
     x = net._buf("eval.x", (10, B * N))
@@ -273,7 +369,8 @@ def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma:
     for b, i in enumerate(idx):
         g = e._grid(i)
         if good[b]:
-            _lib.call("amhd_nn_apply", g, ptr(e.state(i)), ptr(net.out_scale), ptr(y), B * N, int(b), stream_ptr())
+            _lib.call("amhd_nn_apply_guarded", g, ptr(e.state(i)), ptr(net.out_scale), ptr(y), B * N, int(b),
+                      float(alpha), float(min_ratio), ptr(rejected) if rejected is not None else None, stream_ptr())
         _lib.call("amhd_apply_bc", g, ptr(e.state(i)), stream_ptr())
     return good
 
@@ -286,25 +383,33 @@ def main(argv=None) -> int:
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--nyc", type=int, default=64)
-    ap.add_argument("--apply-every", type=int, default=20)
+    ap.add_argument("--delta", type=float, default=DELTA, help="correction interval (simulated time)")
+    ap.add_argument("--alpha", default="1.0", help="comma-separated correction scales to evaluate")
+    ap.add_argument("--min-ratio", type=float, default=0.5)
     ap.add_argument("--save", default=None)
     a = ap.parse_args(argv)
     log = lambda m: print(m, file=sys.stderr, flush=True)
     seeds = list(range(a.train_seeds))
     n_val = max(1, a.train_seeds // 10)
     log(f"generating {a.train_seeds} coarse/fine run pairs ...")
-    X, Y, wall_gen = generate_pairs(seeds, nyc=a.nyc, log=log)
+    X, Y, wall_gen = generate_pairs(seeds, delta=a.delta, nyc=a.nyc, log=log)
     log("training ...")
     net, norm, hist = train(X, Y, range(n_val, a.train_seeds), range(n_val), epochs=a.epochs, batch=a.batch,
                             lr=a.lr, log=log)
     log("evaluating on held-out seeds ...")
     test = list(range(10000, 10000 + a.test_seeds))
-    ev = evaluate(net, norm, test, apply_every=a.apply_every, nyc=a.nyc, log=log)
+    evs, base = [], None
+    for alpha in (float(x) for x in a.alpha.split(",")):
+        log(f"  alpha = {alpha}")
+        ev = evaluate(net, norm, test, delta=a.delta, nyc=a.nyc, alpha=alpha, min_ratio=a.min_ratio, runs_in=base,
+                      log=log)
+        base = ev.pop("_baseline")
+        evs.append(ev)
     if a.save:
         torch.save({"params": net.host_params(), "in_mean": norm.in_mean.cpu(), "in_std": norm.in_std.cpu(),
                     "out_std": norm.out_std.cpu()}, a.save)
     print(json.dumps({"data_generation_wall_s": wall_gen, "pairs": int(X.shape[0] * X.shape[1]),
-                      "training": hist, "evaluation": ev, "params": sum(p["w"].numel() + p["b"].numel()
+                      "training": hist, "evaluation": evs, "params": sum(p["w"].numel() + p["b"].numel()
                                                                         for p in net.p.values())}))
     return 0
 

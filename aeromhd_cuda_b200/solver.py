@@ -75,6 +75,7 @@ class MHDSolver:
         self._ctl = control_tensor(1, self.device)
         self._diag_out = torch.zeros(8, dtype=torch.float64, device=self.device)
         self._diag_rows = torch.zeros(7 * config.nx, dtype=torch.float64, device=self.device)
+        self._diag_colour = torch.zeros(config.nx + config.ny, dtype=torch.float64, device=self.device)
         self._graphs = {}
         self._loop_ready = False
 
@@ -235,22 +236,25 @@ class MHDSolver:
         return dict(zip(DIAG_NAMES, (float(v) for v in vals[:7])))
 
     def compute_diagnostics(self):
-        """solver.py:335-444: the sums, maxima and the integral mixing width come
-        from the GPU; the interface-tracking quantities from the colour field."""
+        """solver.py:335-444.  Every pass over the field runs on the GPU (sums,
+        maxima, integral mixing width, per-row colour variance, per-column
+        interface positions); the host finishes from nx + ny + 7 nx numbers."""
         cfg = self.cfg
         ng = self.ng
         d = self.device_diagnostics()
+        nx_int, ny_int = cfg.nx, cfg.ny
+        col = self._diag_colour
+        _lib.call("amhd_diagnostics_colour", self._grid(), ptr(self._U), float(cfg.x_min), ptr(self._diag_rows),
+                  ptr(col), ptr(col[nx_int:]), stream_ptr())
         rows = self._diag_rows.view(7, cfg.nx).cpu().numpy()
+        colour = col.cpu().numpy()
         x_arr = to_numpy(self.x[ng:-ng])
         y_arr = to_numpy(self.y[ng:-ng])
-        nx_int, ny_int = cfg.nx, cfg.ny
-        C = to_numpy(cons_to_prim(self._U, cfg.gamma)[iCLR, ng:-ng, ng:-ng]).astype(np.float64)
-        C_clamped = np.clip(C, 0.0, 1.0)
         C_bar = rows[0] / ny_int
 
         mixed = np.where((C_bar > 0.01) & (C_bar < 0.99))[0]
         mw_thresh = float(x_arr[mixed[-1]] - x_arr[mixed[0]]) if len(mixed) > 1 else 0.0
-        C_prime_sq = np.mean((C_clamped - C_bar[:, None]) ** 2, axis=1)
+        C_prime_sq = colour[:nx_int] / ny_int
         denom_mix = np.maximum(C_bar * (1.0 - C_bar), 1e-14)
         if len(mixed) > 1:
             num = float(np.trapezoid(C_prime_sq[mixed], x_arr[mixed]))
@@ -260,17 +264,7 @@ class MHDSolver:
             mixedness = 0.0
 
         # interface position per column: gradient-weighted centroid around the peak
-        grad = np.abs(np.gradient(C_clamped, cfg.dx, axis=0))
-        interface_pos = np.full(ny_int, np.nan)
-        peak = np.argmax(grad, axis=0)
-        for j in np.nonzero(grad.max(axis=0) > 1e-6)[0]:
-            ip = int(peak[j])
-            hw = min(10, ip, nx_int - ip - 1)
-            if hw > 0:
-                wgt = grad[ip - hw:ip + hw + 1, j]
-                ws = np.sum(wgt)
-                if ws > 1e-12:
-                    interface_pos[j] = np.sum(x_arr[ip - hw:ip + hw + 1] * wgt) / ws
+        interface_pos = colour[nx_int:]
         valid = ~np.isnan(interface_pos)
         n_valid = int(np.sum(valid))
         if n_valid > ny_int // 2:

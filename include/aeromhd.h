@@ -220,8 +220,21 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
  * dx dy (solver.py:430), [2] max|divB|, [3] sqrt(mean divB^2) (:419-428),
  * [4] integral mixing width (:353-356), [5] peak stagnation pressure (:415-417),
  * [6] global enstrophy mean(rho w^2) (:399-402).
- * rows_dev: scratch of 4*nx doubles.  Asynchronous. */
+ * rows_dev: 7*nx doubles, left holding the per-row sums of clip(C), rho, E,
+ * divB^2, rho w^2 and the per-row maxima of |divB| and the stagnation
+ * pressure (in that order).  Asynchronous. */
 int amhd_diagnostics(const amhd_grid *g, const void *U, double x0, double *out_dev, double *rows_dev, void *stream);
+/* The colour-field part of compute_diagnostics (solver.py:358-383) that needs a
+ * second pass over the field, after amhd_diagnostics filled rows_dev:
+ * cp2_dev[nx] = per-row sum over y of (clip(C) - Cbar)^2 (C_prime_sq x ny,
+ * :360); pos_dev[ny] = per-column interface position, the |dC/dx|-weighted
+ * mean of x within 10 rows of the first maximum of |dC/dx| (numpy.gradient
+ * along x; numpy's pairwise sums), NaN where the reference leaves NaN
+ * (:369-378).  The threshold mixing width, mixedness, perturbation modes and
+ * local enstrophy follow on the host from these nx + ny values and rows_dev.
+ * Asynchronous. */
+int amhd_diagnostics_colour(const amhd_grid *g, const void *U, double x0, const double *rows_dev, double *cp2_dev,
+                            double *pos_dev, void *stream);
 
 /* The same diagnostics for callers that cannot allocate device memory: a
  * caller running inside CUDA stream capture (where an allocation is not a
@@ -330,6 +343,13 @@ int amhd_nn_pack(const amhd_grid *g, const void *U, const float *mean, const flo
  * (ghost cells are left to amhd_apply_bc) */
 int amhd_nn_apply(const amhd_grid *g, void *U, const float *scale, const float *y, int64_t y_vs, int32_t b,
                   void *stream);
+/* the same, per cell and kept admissible: U_cell += alpha * scale[v] * y[v]
+ * only if the corrected cell is finite and keeps >= min_ratio of its density
+ * and of its pressure (float64); rejected cells keep their state and are
+ * counted into *rejected_dev (may be NULL).  Ghost cells are left to
+ * amhd_apply_bc. */
+int amhd_nn_apply_guarded(const amhd_grid *g, void *U, const float *scale, const float *y, int64_t y_vs, int32_t b,
+                          float alpha, float min_ratio, int32_t *rejected_dev, void *stream);
 
 #ifdef __cplusplus
 }
