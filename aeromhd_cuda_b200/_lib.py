@@ -107,7 +107,7 @@ _SIGS = {
     "amhd_nn_restrict": ([_c.POINTER(Grid), _P, _I32, _P, _I64, _I32, _I32, _P], _c.c_int),
     "amhd_nn_pack": ([_c.POINTER(Grid), _P, _P, _P, _P, _I64, _I32, _P], _c.c_int),
     "amhd_nn_apply": ([_c.POINTER(Grid), _P, _P, _P, _I64, _I32, _P], _c.c_int),
-    "amhd_nn_apply_guarded": ([_c.POINTER(Grid), _P, _P, _P, _I64, _I32, _c.c_float, _c.c_float, _P, _P],
+    "amhd_nn_apply_guarded": ([_c.POINTER(Grid), _P, _P, _P, _I64, _I32, _c.c_float, _c.c_float, _I32, _P, _P],
                               _c.c_int),
 }
 

@@ -390,18 +390,21 @@ __global__ void apply_kernel(R *U, int pitch, int64_t vs, int nx, int ny, const 
          k += (int64_t)gridDim.x * blockDim.x) {
         const int j = (int)(k % ny), i = (int)((k / ny) % nx), v = (int)(k / ((int64_t)nx * ny));
         R *u = &U[v * vs + (int64_t)(i + 2) * pitch + j + 2];
-        *u = (R)((float)*u + scale[v] * y[(int64_t)v * y_vs + ((int64_t)b * nx + i) * ny + j]);
+        *u = *u + (R)(scale[v] * y[(int64_t)v * y_vs + ((int64_t)b * nx + i) * ny + j]);  // in the state's precision
     }
 }
 
 // The same, cell by cell and kept admissible: U_cell += alpha scale_v y[v] only
 // when the corrected cell is finite and keeps at least min_ratio of its
 // density and of its pressure p = (gamma-1)(E - |m|^2/2rho - |B|^2/2) (float64);
-// otherwise the cell keeps its state and *rejected counts it.
+// otherwise the cell keeps its state and *rejected counts it.  mode: 0 the
+// correction as is; 1 the passive scalar's correction scaled by 4 C (1 - C) of
+// the cell (none in unmixed fluid); 2 no scalar correction; 3 every variable's
+// correction scaled by 4 C (1 - C) (corrections only in the mixing layer).
 template <typename R>
 __global__ void apply_guarded_kernel(R *U, int pitch, int64_t vs, int nx, int ny, double gamma, const float *scale,
                                      const float *y, int64_t y_vs, int b, float alpha, float min_ratio,
-                                     int *rejected)
+                                     int scalar_mode, int *rejected)
 {
     const int64_t total = (int64_t)nx * ny;
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
@@ -411,10 +414,15 @@ __global__ void apply_guarded_kernel(R *U, int pitch, int64_t vs, int nx, int ny
         const int64_t yc = ((int64_t)b * nx + i) * ny + j;
         double u[10], w[10];
         bool ok = true;
+        const double cc = fmin(fmax((double)U[9 * vs + c] / fmax((double)U[c], 1e-12), 0.0), 1.0);
+        const float mix = float(4.0 * cc * (1.0 - cc));
+        const float sfac = scalar_mode == 0 ? 1.f : (scalar_mode == 2 ? 0.f : mix);
+        const float ofac = scalar_mode == 3 ? mix : 1.f;
 #pragma unroll
         for (int v = 0; v < 10; ++v) {
             u[v] = (double)U[v * vs + c];
-            w[v] = (double)(R)((float)U[v * vs + c] + alpha * scale[v] * y[(int64_t)v * y_vs + yc]);
+            const float a = v == 9 ? alpha * sfac : alpha * ofac;
+            w[v] = (double)(R)(U[v * vs + c] + (R)(a * scale[v] * y[(int64_t)v * y_vs + yc]));
             ok = ok && isfinite(w[v]);
         }
         auto pressure = [&](const double *s) {
@@ -613,19 +621,20 @@ int amhd_nn_apply(const amhd_grid *g, void *U, const float *scale, const float *
 }
 
 int amhd_nn_apply_guarded(const amhd_grid *g, void *U, const float *scale, const float *y, int64_t y_vs, int32_t b,
-                          float alpha, float min_ratio, int32_t *rejected_dev, void *stream)
+                          float alpha, float min_ratio, int32_t scalar_mode, int32_t *rejected_dev, void *stream)
 {
     if (!g || !U || !scale || !y) return nn_fail(AMHD_ERR_ARG, "bad apply arguments");
     if (!(min_ratio >= 0.f && min_ratio <= 1.f)) return nn_fail(AMHD_ERR_ARG, "min_ratio must be in [0, 1]");
+    if (scalar_mode < 0 || scalar_mode > 3) return nn_fail(AMHD_ERR_ARG, "mode must be 0, 1, 2 or 3");
     const int64_t n = (int64_t)g->nx * g->ny;
     if (g->dtype == AMHD_F64)
         apply_guarded_kernel<double><<<blocks_for(n), 256, 0, S(stream)>>>(
             static_cast<double *>(U), g->pitch, g->var_stride, g->nx, g->ny, g->gamma, scale, y, y_vs, b, alpha,
-            min_ratio, rejected_dev);
+            min_ratio, scalar_mode, rejected_dev);
     else
         apply_guarded_kernel<float><<<blocks_for(n), 256, 0, S(stream)>>>(
             static_cast<float *>(U), g->pitch, g->var_stride, g->nx, g->ny, g->gamma, scale, y, y_vs, b, alpha,
-            min_ratio, rejected_dev);
+            min_ratio, scalar_mode, rejected_dev);
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }

@@ -139,17 +139,20 @@ class Normaliser:
 
 
 def train(X: torch.Tensor, Y: torch.Tensor, train_seeds: Sequence[int], val_seeds: Sequence[int], epochs: int = 20,
-          batch: int = 16, lr: float = 1e-3, seed: int = 0, log=print):
-    """X, Y: [snap][seed][10][H][W]; seeds index the second axis.  Returns (net, norm, history)."""
+          batch: int = 16, lr: float = 1e-3, seed: int = 0, net: Corrector | None = None,
+          norm: "Normaliser | None" = None, log=print):
+    """X, Y: [snap][seed][10][H][W]; seeds index the second axis.  Returns (net, norm, history).
+    Given net and norm, continues training that network with its normalisation."""
     H, W = X.shape[-2], X.shape[-1]
     T = Y - X
     tr = X[:, list(train_seeds)].reshape(-1, 10, H, W)
     ttr = T[:, list(train_seeds)].reshape(-1, 10, H, W)
     va = X[:, list(val_seeds)].reshape(-1, 10, H, W)
     tva = T[:, list(val_seeds)].reshape(-1, 10, H, W)
-    norm = Normaliser(tr, ttr)
-    net = Corrector(H, W, seed=seed, device=X.device)
-    net.set_normalisation(norm.in_mean, norm.in_std, norm.out_scale)
+    if net is None:
+        norm = Normaliser(tr, ttr)
+        net = Corrector(H, W, seed=seed, device=X.device)
+        net.set_normalisation(norm.in_mean, norm.in_std, norm.out_scale)
     gen = torch.Generator(device="cpu").manual_seed(seed)
     hist = {"epoch": [], "train_loss": [], "val_loss": [], "wall_s": []}
     n = tr.shape[0]
@@ -178,6 +181,47 @@ def train(X: torch.Tensor, Y: torch.Tensor, train_seeds: Sequence[int], val_seed
     # baseline: the loss of predicting no correction
     hist["val_loss_zero_correction"] = float(norm.targets(tva).pow(2).mean())
     return net, norm, hist
+
+
+def rollout_pairs(net: Corrector, norm: "Normaliser", seeds: Sequence[int], delta: float = DELTA, t_end: float = 3.0,
+                  alpha: float = 1.0, scalar_mode: int = 3, every: int = 3, nyc: int = 64, factor: int = 4,
+                  precision: str = "fp32", log=print):
+    """Pairs from the corrector's own runs (to correct the drift it causes): a
+    corrected coarse run and the fine run of each seed advance together from the
+    same restricted initial state; at every `every`-th correction time the pair
+    (corrected-run state before its correction, fine state restricted) is kept.
+    Returns (X, Y) shaped like generate_pairs'."""
+    coarse, fine = paired_configs(seeds, nyc, factor, precision)
+    ef, ec = Ensemble(fine), Ensemble(coarse)
+    ef.initialize()
+    nxc, nyc_ = coarse[0].nx, coarse[0].ny
+    buf = torch.empty((10, nxc * nyc_), dtype=torch.float32, device=ec.device)
+    _load_restricted(ef, ec, factor, buf)
+    n = len(seeds)
+    m_total = int(round(t_end / delta))
+    keep = [q for q in range(1, m_total + 1) if q % every == 0]
+    X = torch.empty((len(keep), n, 10, nxc, nyc_), dtype=torch.float32, device=ec.device)
+    Y = torch.empty_like(X)
+    ef.start(t_end=delta)
+    ec.start(t_end=delta)
+    idx = np.arange(n)
+    j = 0
+    for q in range(1, m_total + 1):
+        tc = q * delta
+        ef.continue_to(tc)
+        ef.run(chunk=64)
+        ec.continue_to(tc)
+        ec.run(chunk=32)
+        if q % every == 0:
+            for i in range(n):
+                X[j, i].copy_(_interior(ec, i))
+                _lib.call("amhd_nn_restrict", ef._grid(i), ptr(ef.state(i)), factor, ptr(Y[j, i]), nxc * nyc_, 0, 1,
+                          stream_ptr())
+            j += 1
+        _apply_batch(net, norm, ec, idx, 8.0, alpha, 0.5, None, scalar_mode)
+        if log and q % 30 == 0:
+            log(f"  rollout pairs to t={tc:.2f}")
+    return X, Y
 
 
 def _mixing_width(ens: Ensemble, k: int) -> float:
@@ -215,7 +259,7 @@ def _set_limits(e: Ensemble, cap: np.ndarray, stop: np.ndarray) -> None:
 def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: float = DELTA, nyc: int = 64,
              factor: int = 4, t_snaps: Sequence[float] = T_SNAPS, divb_tol: float = 1.0, corr_sigma: float = 8.0,
              step_factor: float = 3.0, dt_drop: float = 0.5, max_wall: float = 900.0, alpha: float = 1.0,
-             min_ratio: float = 0.5, runs_in=None, log=print) -> dict:
+             min_ratio: float = 0.5, scalar_mode: int = 1, runs_in=None, log=print) -> dict:
     """Fine, coarse and corrected runs of the held-out seeds to every snapshot
     time.  The corrected run adds the correction every `delta` of simulated
     time; an instance falls back (stops; its plain fine solve stands in) when
@@ -224,29 +268,42 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: floa
     the instance needs more than step_factor x the plain coarse run's steps
     between two snapshots.  max_wall bounds the corrected run's wall time.
     alpha scales the corrections; cells a correction would leave with less than
-    min_ratio of their density or pressure are not corrected.  runs_in: the
+    min_ratio of their density or pressure are not corrected; scalar_mode: how
+    the passive scalar is corrected (amhd_nn_apply_guarded).  runs_in: the
     fine and coarse results of an earlier call on the same seeds (reused)."""
     coarse, fine = paired_configs(seeds, nyc, factor)
     n = len(seeds)
     runs = {}
     walls = {}
-    mw = {name: np.zeros((len(t_snaps), n)) for name in ("fine", "coarse", "corrected")}
-    divb = {name: np.zeros((len(t_snaps), n)) for name in ("fine", "coarse", "corrected")}
+    names = ("fine", "fine_restricted", "coarse", "corrected")
+    mw = {name: np.zeros((len(t_snaps), n)) for name in names}
+    divb = {name: np.zeros((len(t_snaps), n)) for name in names}
     coarse_steps = np.zeros((len(t_snaps), n), dtype=np.int64)
     fallback = np.zeros(n, dtype=bool)
+    nxc, nycc = coarse[0].nx, coarse[0].ny
+    buf = torch.empty((10, nxc * nycc), dtype=torch.float32, device="cuda")
+    scratch = Ensemble(coarse)   # restricted fine states, for the coarse-grid reference values
     reasons = {"range": 0, "dt_drop": 0, "steps": 0, "wall": 0, "divB": 0}
     n_corr = 0
     rejected = torch.zeros(1, dtype=torch.int32, device="cuda")
     cells_corrected = 0
     if runs_in is not None:
         runs, walls, coarse_steps = dict(runs_in["runs"]), dict(runs_in["walls"]), runs_in["coarse_steps"]
-        for name in ("fine", "coarse"):
+        for name in ("fine", "fine_restricted", "coarse"):
             mw[name], divb[name] = runs_in["mw"][name], runs_in["divb"][name]
+    ic = None
     for name, cfgs in (("fine", fine), ("coarse", coarse), ("corrected", coarse)):
         if name in runs:
             continue
         e = Ensemble(cfgs)
-        e.initialize()
+        if name == "fine":
+            e.initialize()
+        else:
+            # the fine run's initial state restricted: both grids start from the same physical state
+            if ic is None:
+                ic = Ensemble(fine)
+                ic.initialize()
+            _load_restricted(ic, e, factor, buf)
         e.start(t_end=t_snaps[0])
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -290,7 +347,7 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: floa
                     due = np.nonzero(~fallback)[0]
                     if len(due):
                         dt_before = np.array([ctl[i].dt_cfl for i in due])
-                        ok = _apply_batch(net, norm, e, due, corr_sigma, alpha, min_ratio, rejected)
+                        ok = _apply_batch(net, norm, e, due, corr_sigma, alpha, min_ratio, rejected, scalar_mode)
                         n_corr += 1
                         cells_corrected += int(sum(cfgs[i].nx * cfgs[i].ny for i in due[ok]))
                         fallback[due[~ok]] = True
@@ -299,6 +356,10 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: floa
                 t_prev = ts
             for i in range(n):
                 mw[name][k, i], divb[name][k, i] = _mixing_width(e, i)
+            if name == "fine":
+                _load_restricted(e, scratch, factor, buf)
+                for i in range(n):
+                    mw["fine_restricted"][k, i], divb["fine_restricted"][k, i] = _mixing_width(scratch, i)
         torch.cuda.synchronize()
         walls[name] = time.perf_counter() - t0
         runs[name] = e
@@ -311,7 +372,6 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: floa
     fallback |= gate
     # spectral energy at the final time (fine restricted to the coarse grid)
     spec_err = np.zeros((2, n))
-    nxc, nycc = coarse[0].nx, coarse[0].ny
     for i in range(n):
         r = torch.empty((10, nxc, nycc), dtype=torch.float32, device=runs["fine"].device)
         g = runs["fine"]._grid(i)
@@ -320,12 +380,14 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: floa
         for j, name in enumerate(("coarse", "corrected")):
             sp = _ke_spectrum(_interior(runs[name], i))
             spec_err[j, i] = float((sp - ref).abs().sum() / ref.sum().clamp_min(1e-300))
-    peak = np.maximum(np.abs(mw["fine"]).max(0), 1e-12)
+    def mw_err(name, ref):
+        peak = np.maximum(np.abs(mw[ref]).max(0), 1e-12)
+        return np.abs(mw[name] - mw[ref]).max(0) / peak
 
-    def mw_err(name):
-        return np.abs(mw[name] - mw["fine"]).max(0) / peak
-
-    err_c, err_k = mw_err("coarse"), mw_err("corrected")
+    # reference: the fine solution restricted onto the coarse grid (what a coarse
+    # grid can represent); against the fine grid's own values as well
+    err_c, err_k = mw_err("coarse", "fine_restricted"), mw_err("corrected", "fine_restricted")
+    err_cf, err_kf = mw_err("coarse", "fine"), mw_err("corrected", "fine")
     err_final = np.where(fallback, 0.0, err_k)
     out = {
         "seeds": list(map(int, seeds)), "correction_interval": delta, "corrections": n_corr,
@@ -335,9 +397,13 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: floa
         "mixing_width_err_corrected": {"mean": float(err_k.mean()), "median": float(np.median(err_k)),
                                        "max": float(err_k.max())},
         "within_2pct": {"coarse": int((err_c <= 0.02).sum()), "corrected": int((err_k <= 0.02).sum()), "of": n},
+        "within_5pct": {"coarse": int((err_c <= 0.05).sum()), "corrected": int((err_k <= 0.05).sum()), "of": n},
+        "mixing_width_err_vs_fine_grid": {"coarse": float(err_cf.mean()), "corrected": float(err_kf.mean()),
+                                          "fine_restricted": float(mw_err("fine_restricted", "fine").mean())},
         "spectral_energy_err": {"coarse": float(spec_err[0].mean()), "corrected": float(spec_err[1].mean())},
         "divB_L2_final": {k: float(v[-1].mean()) for k, v in divb.items()},
         "fallback_instances": int(fallback.sum()), "fallback_reasons": reasons, "alpha": alpha,
+        "scalar_mode": scalar_mode,
         "min_ratio": min_ratio, "cells_not_corrected_fraction": float(rejected.item()) / max(cells_corrected, 1),
         "speedup_with_fallback_fine_solves": walls["fine"] / max(walls["corrected"] +
                                                                  fallback.mean() * walls["fine"], 1e-12),
@@ -345,12 +411,13 @@ def evaluate(net: Corrector, norm: Normaliser, seeds: Sequence[int], delta: floa
     }
     out["_baseline"] = {"runs": {k: runs[k] for k in ("fine", "coarse")},
                         "walls": {k: walls[k] for k in ("fine", "coarse")}, "coarse_steps": coarse_steps,
-                        "mw": {k: mw[k] for k in ("fine", "coarse")}, "divb": {k: divb[k] for k in ("fine", "coarse")}}
+                        "mw": {k: mw[k] for k in ("fine", "fine_restricted", "coarse")},
+                        "divb": {k: divb[k] for k in ("fine", "fine_restricted", "coarse")}}
     return out
 
 
 def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma: float, alpha: float = 1.0,
-                 min_ratio: float = 0.5, rejected: torch.Tensor | None = None) -> np.ndarray:
+                 min_ratio: float = 0.5, rejected: torch.Tensor | None = None, scalar_mode: int = 1) -> np.ndarray:
     """One forward pass over the instances `idx`; each gets alpha x its correction
     (cells whose corrected density or pressure would fall below min_ratio of the
     current value keep their state) unless the correction is non-finite or far
@@ -370,9 +437,28 @@ def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma:
         g = e._grid(i)
         if good[b]:
             _lib.call("amhd_nn_apply_guarded", g, ptr(e.state(i)), ptr(net.out_scale), ptr(y), B * N, int(b),
-                      float(alpha), float(min_ratio), ptr(rejected) if rejected is not None else None, stream_ptr())
+                      float(alpha), float(min_ratio), int(scalar_mode), ptr(rejected) if rejected is not None else None,
+                      stream_ptr())
         _lib.call("amhd_apply_bc", g, ptr(e.state(i)), stream_ptr())
     return good
+
+
+def save(path: str, net: Corrector, norm: Normaliser) -> None:
+    """Weights and normalisation of a trained corrector (torch.save)."""
+    torch.save({"params": net.host_params(), "H": net.H, "W": net.W,
+                "norm": {k: getattr(norm, k).detach().cpu() for k in ("in_mean", "in_std", "out_std", "active",
+                                                                       "out_max")}}, path)
+
+
+def load(path: str, device="cuda"):
+    """(Corrector, Normaliser) from a file written by save()."""
+    d = torch.load(path, map_location="cpu")
+    norm = Normaliser.__new__(Normaliser)
+    for k, v in d["norm"].items():
+        setattr(norm, k, v.to(device))
+    net = Corrector(int(d["H"]), int(d["W"]), params=d["params"], device=device)
+    net.set_normalisation(norm.in_mean, norm.in_std, norm.out_scale)
+    return net, norm
 
 
 def main(argv=None) -> int:
@@ -386,29 +472,50 @@ def main(argv=None) -> int:
     ap.add_argument("--delta", type=float, default=DELTA, help="correction interval (simulated time)")
     ap.add_argument("--alpha", default="1.0", help="comma-separated correction scales to evaluate")
     ap.add_argument("--min-ratio", type=float, default=0.5)
+    ap.add_argument("--scalar-modes", default="1", help="comma-separated scalar correction modes (0, 1, 2)")
+    ap.add_argument("--load", default=None, help="evaluate a saved corrector instead of generating and training")
+    ap.add_argument("--dagger-rounds", type=int, default=0,
+                    help="rounds of training on pairs from the corrector's own runs")
+    ap.add_argument("--dagger-epochs", type=int, default=20)
+    ap.add_argument("--dagger-mode", type=int, default=3, help="correction mode of those runs")
     ap.add_argument("--save", default=None)
     a = ap.parse_args(argv)
     log = lambda m: print(m, file=sys.stderr, flush=True)
-    seeds = list(range(a.train_seeds))
-    n_val = max(1, a.train_seeds // 10)
-    log(f"generating {a.train_seeds} coarse/fine run pairs ...")
-    X, Y, wall_gen = generate_pairs(seeds, delta=a.delta, nyc=a.nyc, log=log)
-    log("training ...")
-    net, norm, hist = train(X, Y, range(n_val, a.train_seeds), range(n_val), epochs=a.epochs, batch=a.batch,
-                            lr=a.lr, log=log)
+    wall_gen, n_pairs, hist = None, 0, None
+    if a.load:
+        net, norm = load(a.load)
+    else:
+        seeds = list(range(a.train_seeds))
+        n_val = max(1, a.train_seeds // 10)
+        log(f"generating {a.train_seeds} coarse/fine run pairs ...")
+        X, Y, wall_gen = generate_pairs(seeds, delta=a.delta, nyc=a.nyc, log=log)
+        n_pairs = int(X.shape[0] * X.shape[1])
+        log("training ...")
+        net, norm, hist = train(X, Y, range(n_val, a.train_seeds), range(n_val), epochs=a.epochs, batch=a.batch,
+                                lr=a.lr, log=log)
+        for r in range(a.dagger_rounds):
+            log(f"rollout round {r + 1}: pairs from corrected runs ...")
+            X2, Y2 = rollout_pairs(net, norm, seeds, delta=a.delta, scalar_mode=a.dagger_mode, nyc=a.nyc, log=log)
+            X, Y = torch.cat([X, X2]), torch.cat([Y, Y2])
+            del X2, Y2
+            n_pairs = int(X.shape[0] * X.shape[1])
+            net, norm, h2 = train(X, Y, range(n_val, a.train_seeds), range(n_val), epochs=a.dagger_epochs,
+                                  batch=a.batch, lr=a.lr * 0.5, net=net, norm=norm, log=log)
+            hist[f"round{r + 1}"] = h2
+        del X, Y
     log("evaluating on held-out seeds ...")
     test = list(range(10000, 10000 + a.test_seeds))
     evs, base = [], None
-    for alpha in (float(x) for x in a.alpha.split(",")):
-        log(f"  alpha = {alpha}")
-        ev = evaluate(net, norm, test, delta=a.delta, nyc=a.nyc, alpha=alpha, min_ratio=a.min_ratio, runs_in=base,
-                      log=log)
-        base = ev.pop("_baseline")
-        evs.append(ev)
+    for mode in (int(x) for x in a.scalar_modes.split(",")):
+        for alpha in (float(x) for x in a.alpha.split(",")):
+            log(f"  alpha = {alpha}, scalar mode {mode}")
+            ev = evaluate(net, norm, test, delta=a.delta, nyc=a.nyc, alpha=alpha, min_ratio=a.min_ratio,
+                          scalar_mode=mode, runs_in=base, log=log)
+            base = ev.pop("_baseline")
+            evs.append(ev)
     if a.save:
-        torch.save({"params": net.host_params(), "in_mean": norm.in_mean.cpu(), "in_std": norm.in_std.cpu(),
-                    "out_std": norm.out_std.cpu()}, a.save)
-    print(json.dumps({"data_generation_wall_s": wall_gen, "pairs": int(X.shape[0] * X.shape[1]),
+        save(a.save, net, norm)
+    print(json.dumps({"data_generation_wall_s": wall_gen, "pairs": n_pairs,
                       "training": hist, "evaluation": evs, "params": sum(p["w"].numel() + p["b"].numel()
                                                                         for p in net.p.values())}))
     return 0

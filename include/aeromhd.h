@@ -346,10 +346,13 @@ int amhd_nn_apply(const amhd_grid *g, void *U, const float *scale, const float *
 /* the same, per cell and kept admissible: U_cell += alpha * scale[v] * y[v]
  * only if the corrected cell is finite and keeps >= min_ratio of its density
  * and of its pressure (float64); rejected cells keep their state and are
- * counted into *rejected_dev (may be NULL).  Ghost cells are left to
+ * counted into *rejected_dev (may be NULL).  scalar_mode: 0 the correction as
+ * is; 1 the passive scalar's correction scaled by 4 C (1 - C) of the cell;
+ * 2 no scalar correction; 3 every variable's correction scaled by 4 C (1 - C)
+ * (corrections confined to the mixing layer).  Ghost cells are left to
  * amhd_apply_bc. */
 int amhd_nn_apply_guarded(const amhd_grid *g, void *U, const float *scale, const float *y, int64_t y_vs, int32_t b,
-                          float alpha, float min_ratio, int32_t *rejected_dev, void *stream);
+                          float alpha, float min_ratio, int32_t scalar_mode, int32_t *rejected_dev, void *stream);
 
 #ifdef __cplusplus
 }

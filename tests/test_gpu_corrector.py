@@ -160,3 +160,54 @@ def test_training_follows_the_cpu_oracle_trajectory():
     assert ref[-1] < 0.8 * ref[0] and ours[-1] < 0.8 * ours[0]
     for a, r in zip(ours, ref):
         assert abs(a - r) <= 0.10 * r, (a, r)
+
+
+def test_guarded_apply_keeps_cells_admissible():
+    """amhd_nn_apply_guarded: equals amhd_nn_apply (alpha = 1) where every
+    corrected cell stays admissible; a cell whose corrected density or pressure
+    would drop below half keeps its state and is counted."""
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import make_grid, stream_ptr
+    torch.manual_seed(3)
+    U = torch.zeros((10, 12, 20), dtype=torch.float64, device="cuda")
+    U[0] = 1.0 + 0.1 * torch.rand(12, 20, device="cuda", dtype=torch.float64)
+    U[1:4] = 0.1 * torch.randn(3, 12, 20, device="cuda", dtype=torch.float64)
+    U[4:7] = 0.1 * torch.randn(3, 12, 20, device="cuda", dtype=torch.float64)
+    U[7] = 2.0
+    U[9] = U[0] * torch.rand(12, 20, device="cuda", dtype=torch.float64)
+    g = make_grid(U, 1.4)
+    y = 0.01 * torch.randn((10, 128), device="cuda")
+    scale = torch.ones(10, device="cuda")
+    a, b = U.clone(), U.clone()
+    rej = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("amhd_nn_apply", g, a.data_ptr(), scale.data_ptr(), y.data_ptr(), 128, 0, stream_ptr())
+    _lib.call("amhd_nn_apply_guarded", g, b.data_ptr(), scale.data_ptr(), y.data_ptr(), 128, 0, 1.0, 0.5,
+              0, rej.data_ptr(), stream_ptr())
+    assert int(rej.item()) == 0
+    assert torch.allclose(a, b, rtol=0, atol=1e-6)       # float32 arithmetic of the correction in both
+    # cell (3, 5) of the interior: density would fall to 30 %; cell (7, 1): pressure negative
+    y2 = y.clone().view(10, 8, 16)
+    y2[0, 3, 5] = -0.7 * float(U[0, 5, 7])
+    y2[7, 7, 1] = -5.0
+    c = U.clone()
+    rej.zero_()
+    _lib.call("amhd_nn_apply_guarded", g, c.data_ptr(), scale.data_ptr(), y2.data_ptr(), 128, 0, 1.0, 0.5,
+              0, rej.data_ptr(), stream_ptr())
+    assert int(rej.item()) == 2
+    assert torch.equal(c[:, 5, 7], U[:, 5, 7]) and torch.equal(c[:, 9, 3], U[:, 9, 3])
+    half = U.clone()
+    _lib.call("amhd_nn_apply_guarded", g, half.data_ptr(), scale.data_ptr(), y.data_ptr(), 128, 0, 0.5, 0.5,
+              0, None, stream_ptr())
+    assert torch.allclose(half[:, 2:-2, 2:-2] - U[:, 2:-2, 2:-2], 0.5 * (a - U)[:, 2:-2, 2:-2], atol=1e-6)
+
+    # scalar modes: 2 leaves rho C alone, 1 scales its correction by 4 C (1 - C)
+    for mode in (1, 2):
+        d = U.clone()
+        _lib.call("amhd_nn_apply_guarded", g, d.data_ptr(), scale.data_ptr(), y.data_ptr(), 128, 0, 1.0, 0.5,
+                  mode, None, stream_ptr())
+        assert torch.allclose(d[:9], a[:9], rtol=0, atol=1e-6)
+        if mode == 2:
+            assert torch.equal(d[9], U[9])
+        else:
+            C = (U[9] / U[0]).clamp(0, 1)
+            assert torch.allclose(d[9] - U[9], (a[9] - U[9]) * 4 * C * (1 - C), atol=1e-6)
