@@ -571,6 +571,53 @@ int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *
     return AMHD_OK;
 }
 
+int amhd_control_init_split(const amhd_grid *g, void *U, amhd_control *ctl, double t, double t_end, int64_t step,
+                            int64_t max_steps, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !ctl) return fail(AMHD_ERR_ARG, "NULL argument");
+    cudaStream_t s = S(stream);
+    if (int e = control_upload(ctl, t, t_end, step, max_steps, s)) return e;
+    CK(run_dt_reduce(g, U, 0, ctl, s));
+    CK(run_bc_fill(g, U, s));
+    return AMHD_OK;
+}
+
+int amhd_advance_stage(const amhd_grid *g, int32_t stage, void *U, void *U1, void *U2, amhd_control *ctl,
+                       void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (stage < 1 || stage > 3) return fail(AMHD_ERR_ARG, "stage must be 1, 2 or 3");
+    const void *ptrs[3] = {U, U1, U2};
+    if (int e = check_padded(g, ptrs, 3)) return e;
+    if (!ctl) return fail(AMHD_ERR_ARG, "NULL control");
+    const int tx = g_tile_x;
+    const amhd_instance one = single_instance(g, tx);
+    StageParams p;
+    memset(&p, 0, sizeof p);
+    void *in[3] = {U, U1, U2};
+    void *out[3] = {U1, U2, U};
+    set_input(p, in[stage - 1], g, tx);
+    p.u0 = U;
+    p.uout = out[stage - 1];
+    p.one = one;
+    p.n_tiles = one.tiles_x * one.tiles_y;
+    p.ctl = ctl;
+    p.use_ctl = 1;
+    p.fuse_dt = stage == 3;
+    CK(run_stage(g->dtype, stage, tx, p, stage_grid(g->dtype, tx, p.n_tiles, g_ctas_per_sm), S(stream)));
+    return AMHD_OK;
+}
+
+int amhd_advance_finish(const amhd_grid *g, void *U, amhd_control *ctl, int32_t advance, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    if (!U || !ctl) return fail(AMHD_ERR_ARG, "NULL argument");
+    const amhd_instance one = single_instance(g, g_tile_x);
+    CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, advance ? 1 : 0, 0, S(stream)));
+    return AMHD_OK;
+}
+
 int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps,
                          double *ms_out, void *stream)
 {

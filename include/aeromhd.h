@@ -199,6 +199,25 @@ int amhd_control_resume(amhd_control *ctl, int32_t n, double snap_t, void *strea
  * in a CUDA graph. */
 int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps,
                  void *stream);
+/* The run loop taken apart, for drivers that act between its pieces (a grid
+ * split over GPUs by x rows exchanges ghost rows after every stage and
+ * max-reduces the CFL maxima ctl->red[4] across GPUs before the dt):
+ *   amhd_control_init_split -- as amhd_control_init, but stops after
+ *     accumulating the state's CFL maxima into ctl->red (no dt yet) and
+ *     filling U's ghost cells;
+ *   amhd_advance_stage -- stage 1 (U -> U1), 2 (U1 -> U2, base U) or 3
+ *     (U2 -> U, base U, CFL maxima of the new state into ctl->red) with dt,
+ *     ch and the psi damping from ctl, ghost cells of the output filled;
+ *   amhd_advance_finish -- advance = 1: t += dt, step += 1 (as at the end of
+ *     an amhd_advance iteration), then in both cases dt / ch / damping / the
+ *     stop flags from ctl->red, which is cleared.
+ * amhd_advance(n) == n x (stage 1, 2, 3, finish(1)).  Asynchronous.  No
+ * counterpart in the reference. */
+int amhd_control_init_split(const amhd_grid *g, void *U, amhd_control *ctl, double t, double t_end, int64_t step,
+                            int64_t max_steps, void *stream);
+int amhd_advance_stage(const amhd_grid *g, int32_t stage, void *U, void *U1, void *U2, amhd_control *ctl,
+                       void *stream);
+int amhd_advance_finish(const amhd_grid *g, void *U, amhd_control *ctl, int32_t advance, void *stream);
 /* amhd_advance with a CUDA event recorded after every launch: ms_out[0..3]
  * receive the summed device time of the stage-1, stage-2, stage-3 and
  * finalize launches, ms_out[4] the whole interval.  Synchronises.  For

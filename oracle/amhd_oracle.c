@@ -29,7 +29,7 @@ enum { IVX = 1, IVY = 2, IVZ = 3, IPR = 7, ICLR = 9 };
 #define FLOOR_PR 1e-12
 
 /* boundary kinds (Config.get_bc_x, config.py:86-89; apply_bc, solver.py:158-197) */
-enum { ORC_BC_PERIODIC = 0, ORC_BC_EXTRAP = 1, ORC_BC_CHARACTERISTIC = 2 };
+enum { ORC_BC_PERIODIC = 0, ORC_BC_EXTRAP = 1, ORC_BC_CHARACTERISTIC = 2, ORC_BC_NONE = 3 };
 
 /* numpy.maximum / numpy.clip semantics: a NaN operand propagates */
 static inline double np_max(double a, double b) { return (isnan(a) || a >= b) ? a : b; }
@@ -371,8 +371,10 @@ void orc_apply_bc(double *U, int nxt, int nyt, int bc_x, int bc_y)
     long n = (long)nxt * nyt;
     for (int v = 0; v < NV; ++v) {
         double *u = U + (long)v * n;
-        /* x direction, solver.py:164-172, :188-194 */
-        if (bc_x == ORC_BC_PERIODIC) {
+        /* x direction, solver.py:164-172, :188-194 (ORC_BC_NONE: x ghost rows are
+         * left as they are -- a test driver of a row-split grid fills them) */
+        if (bc_x == ORC_BC_NONE) {
+        } else if (bc_x == ORC_BC_PERIODIC) {
             for (int i = 0; i < NG; ++i)
                 memcpy(u + (long)i * nyt, u + (long)(nxt - 2 * NG + i) * nyt, sizeof(double) * nyt);
             for (int i = 0; i < NG; ++i)
