@@ -712,10 +712,11 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
     __syncwarp();  // the next item reuses the shared rows
 }
 
-// resident CTAs of kMarchThreads per SM the register budget is shaped for
-// (float32: stage 3 carries the CFL maxima and keeps a larger budget)
+// resident CTAs of kMarchThreads per SM the register budget is shaped for:
+// float32 4 (128 registers, no spills; 5 CTAs at 96 registers spilled and ran
+// 5 % slower), float64 2
 template <typename R, int STAGE>
-constexpr int kMarchMinBlocks = kFast<R> ? (STAGE == 3 ? 4 : 5) : 2;
+constexpr int kMarchMinBlocks = kFast<R> ? 4 : 2;
 
 template <typename R, int STAGE>
 __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) march_stage_kernel(
