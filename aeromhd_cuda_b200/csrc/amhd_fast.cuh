@@ -51,6 +51,21 @@ __device__ __forceinline__ float slope(float wm, float w0, float wp, int limiter
     return (ab > 0.f) ? 2.f * ab * rcp(dm + dp + 1e-30f) : 0.f;
 }
 
+// the same for two independent values at once, on the packed float32x2 path of
+// sm_100 (one FFMA2/FADD2/FMUL2 per pair; per component the scalar arithmetic)
+__device__ __forceinline__ float2 slope2(float2 wm, float2 w0, float2 wp, int limiter)
+{
+    const float2 m1 = make_float2(-1.f, -1.f);
+    const float2 dm = __ffma2_rn(wm, m1, w0), dp = __ffma2_rn(w0, m1, wp);
+    const float2 ab = __fmul2_rn(dm, dp);
+    if (limiter == AMHD_LIMITER_MINMOD)
+        return make_float2((ab.x > 0.f) ? (fabsf(dm.x) < fabsf(dp.x) ? dm.x : dp.x) : 0.f,
+                           (ab.y > 0.f) ? (fabsf(dm.y) < fabsf(dp.y) ? dm.y : dp.y) : 0.f);
+    const float2 den = __fadd2_rn(__fadd2_rn(dm, dp), make_float2(1e-30f, 1e-30f));
+    const float2 q = __fmul2_rn(__fmul2_rn(make_float2(2.f, 2.f), ab), make_float2(rcp(den.x), rcp(den.y)));
+    return make_float2(ab.x > 0.f ? q.x : 0.f, ab.y > 0.f ? q.y : 0.f);
+}
+
 // conserved -> primitive with the pressure recovered in float64
 __device__ __forceinline__ void cons_to_prim(const float u[NV], double gamma, float w[NV])
 {

@@ -131,8 +131,14 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
     const R dx = R(g.dx), dy = R(g.dy);
     if constexpr (kFast<R>) {
         const float idx = float(1.0 / g.dx), idy = float(1.0 / g.dy);
+        const float2 nix = make_float2(-idx, -idx), niy = make_float2(-idy, -idy);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) rhs[v] = -dfx[v] * idx - dfy[v] * idy;
+        for (int v = 0; v < NV; v += 2) {
+            const float2 r = __ffma2_rn(make_float2(dfy[v], dfy[v + 1]), niy,
+                                        __fmul2_rn(make_float2(dfx[v], dfx[v + 1]), nix));
+            rhs[v] = r.x;
+            rhs[v + 1] = r.y;
+        }
     } else {
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
@@ -165,6 +171,28 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
         for (int v = 0; v < NV; ++v) out[v] = rhs[v];
     } else {
         const R dtr = R(dt);
+        if constexpr (kFast<R>) {
+            // pairs of variables on the packed float32x2 path; stages 2, 3 in the
+            // increment form U0 + w ((U* - U0) + dt R): in float32 the weights 1/3
+            // and 2/3 round to a sum of 1 + 3e-8, which as a weighted average would
+            // scale the state every step (a mass drift); U* - U0 is exact
+            const float w = STAGE == 2 ? 0.25f : float(2.0 / 3.0);
+            const float2 dt2 = make_float2(dtr, dtr), w2 = make_float2(w, w), m1 = make_float2(-1.f, -1.f);
+#pragma unroll
+            for (int v = 0; v < NV; v += 2) {
+                const float2 b0 = make_float2(base_at(v), base_at(v + 1));
+                const float2 r = make_float2(rhs[v], rhs[v + 1]);
+                float2 o;
+                if (STAGE == 1) {
+                    o = __ffma2_rn(dt2, r, b0);
+                } else {
+                    const float2 us = make_float2(in_at(v), in_at(v + 1));
+                    o = __ffma2_rn(w2, __ffma2_rn(dt2, r, __ffma2_rn(b0, m1, us)), b0);
+                }
+                out[v] = o.x;
+                out[v + 1] = o.y;
+            }
+        } else
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
             R b0 = base_at(v);
@@ -641,17 +669,44 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
             // the flux through the face on the cell's left (rotated slot order of
             // physics.py:376-379); the right face is the next lane's left face
             R wl[NV], wr[NV], f[NV];
+            if constexpr (kFast<R>) {
 #pragma unroll
-            for (int k = 0; k < NV; ++k) {
-                const int v = rot[k];
-                const R wm = __shfl_up_sync(0xffffffffu, w0[v], 1);
-                const R wp = __shfl_down_sync(0xffffffffu, w0[v], 1);
-                const R sy = cell_slope(wm, w0[v], wp, lim);
-                wr[k] = w0[v] - R(0.5) * sy;
-                wl[k] = __shfl_up_sync(0xffffffffu, w0[v] + R(0.5) * sy, 1);
-                if (v == BY) {
-                    bym = wm;
-                    byp = wp;
+                for (int k = 0; k < NV; k += 2) {
+                    const int v0 = rot[k], v1 = rot[k + 1];
+                    const float2 c = make_float2(w0[v0], w0[v1]);
+                    const float2 m = make_float2(__shfl_up_sync(0xffffffffu, c.x, 1),
+                                                 __shfl_up_sync(0xffffffffu, c.y, 1));
+                    const float2 q = make_float2(__shfl_down_sync(0xffffffffu, c.x, 1),
+                                                 __shfl_down_sync(0xffffffffu, c.y, 1));
+                    const float2 sy = fast::slope2(m, c, q, lim);
+                    const float2 r = __ffma2_rn(make_float2(-0.5f, -0.5f), sy, c);
+                    const float2 l = __ffma2_rn(make_float2(0.5f, 0.5f), sy, c);
+                    wr[k] = r.x;
+                    wr[k + 1] = r.y;
+                    wl[k] = __shfl_up_sync(0xffffffffu, l.x, 1);
+                    wl[k + 1] = __shfl_up_sync(0xffffffffu, l.y, 1);
+                    if (v0 == BY) {
+                        bym = m.x;
+                        byp = q.x;
+                    }
+                    if (v1 == BY) {
+                        bym = m.y;
+                        byp = q.y;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < NV; ++k) {
+                    const int v = rot[k];
+                    const R wm = __shfl_up_sync(0xffffffffu, w0[v], 1);
+                    const R wp = __shfl_down_sync(0xffffffffu, w0[v], 1);
+                    const R sy = cell_slope(wm, w0[v], wp, lim);
+                    wr[k] = w0[v] - R(0.5) * sy;
+                    wl[k] = __shfl_up_sync(0xffffffffu, w0[v] + R(0.5) * sy, 1);
+                    if (v == BY) {
+                        bym = wm;
+                        byp = wp;
+                    }
                 }
             }
             face_flux(wl, wr, gam, igm1, chr, half_ich, f);
@@ -667,12 +722,30 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
 #pragma unroll
             for (int v = 0; v < NV; ++v) u[v] = ms.raw[s2][v][lane];
             to_prim(u, g.gamma, w2);
+            if constexpr (kFast<R>) {
+                // pairs of variables on the packed float32x2 path
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                const R s1 = cell_slope(w0[v], w1[v], w2[v], lim);
-                wl[v] = w0[v] + R(0.5) * ms.sx[v][lane];
-                wr[v] = w1[v] - R(0.5) * s1;
-                ms.sx[v][lane] = s1;
+                for (int v = 0; v < NV; v += 2) {
+                    const float2 a = make_float2(w0[v], w0[v + 1]), b = make_float2(w1[v], w1[v + 1]);
+                    const float2 s1 = fast::slope2(a, b, make_float2(w2[v], w2[v + 1]), lim);
+                    const float2 l = __ffma2_rn(make_float2(0.5f, 0.5f),
+                                                make_float2(ms.sx[v][lane], ms.sx[v + 1][lane]), a);
+                    const float2 r = __ffma2_rn(make_float2(-0.5f, -0.5f), s1, b);
+                    wl[v] = l.x;
+                    wl[v + 1] = l.y;
+                    wr[v] = r.x;
+                    wr[v + 1] = r.y;
+                    ms.sx[v][lane] = s1.x;
+                    ms.sx[v + 1][lane] = s1.y;
+                }
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    const R s1 = cell_slope(w0[v], w1[v], w2[v], lim);
+                    wl[v] = w0[v] + R(0.5) * ms.sx[v][lane];
+                    wr[v] = w1[v] - R(0.5) * s1;
+                    ms.sx[v][lane] = s1;
+                }
             }
             face_flux(wl, wr, gam, igm1, chr, half_ich, f);
 #pragma unroll
