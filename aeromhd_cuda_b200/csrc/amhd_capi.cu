@@ -162,6 +162,7 @@ int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instan
     memset(&p, 0, sizeof p);
     p.inst = insts;
     p.n_inst = n_inst;
+    p.pull_ghosts = 1;  // the run loop: U1 and U2 are internal, their ghost cells are never stored
     p.one = one;
     p.tile_inst = tile_inst;
     p.tile_order = tile_order;
@@ -640,6 +641,7 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
     p.n_tiles = n_tiles;
     p.ctl = ctl;
     p.use_ctl = 1;
+    p.pull_ghosts = 1;
     cudaError_t ce = cudaEventRecord(ev[0], s);
     for (int k = 0; k < n_steps && ce == cudaSuccess; ++k) {
         for (int st = 1; st <= 3 && ce == cudaSuccess; ++st) {

@@ -612,7 +612,16 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
     const int local = item - in.first_tile;
     const int strip = local % in.tiles_y, chunk = local / in.tiles_y;
     const int j = kMarchCols * strip + lane;  // storage column of this lane (first interior column - 2 + lane)
-    const int jl = min(j, g.pitch - 1);       // lanes past the padded row load a cell they do not use
+    // ghost cells of the input: as stored, or (pull) taken from the interior cells
+    // they copy (apply_bc, solver.py:158-197; psi zero in non-periodic x ghosts)
+    const bool pull = p.pull_ghosts != 0;
+    const int jl = pull ? ghost_source(min(j, NG + g.ny + 1), g.ny, g.bc_y)
+                        : min(j, g.pitch - 1);  // lanes past the padded row load a cell they do not use
+    const bool zero_psi = pull && g.bc_x != AMHD_BC_PERIODIC;
+    auto src_row = [&](int r) { return pull ? ghost_source(r, g.nx, g.bc_x) : r; };
+    auto ghost_psi = [&](int r, R u[NV]) {
+        if (zero_psi && (r < NG || r >= NG + g.nx)) u[PSI] = R(0);
+    };
     const int ib = NG + chunk * p.march_rows;
     const int ie = min(ib + p.march_rows, NG + g.nx);
     const int64_t vs = g.var_stride;
@@ -637,8 +646,8 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
     // slots they replace, and waits for them just before the x faces.
     int s0 = (ib - 2) % 3;  // slot of row i (ib-2 here)
     const int s1i = s0 == 2 ? 0 : s0 + 1, s2i = s1i == 2 ? 0 : s1i + 1;
-    fetch_row(ms.raw[s0], uin, vs, (int64_t)(ib - 2) * pitch + jl, lane);
-    fetch_row(ms.raw[s1i], uin, vs, (int64_t)(ib - 1) * pitch + jl, lane);
+    fetch_row(ms.raw[s0], uin, vs, (int64_t)src_row(ib - 2) * pitch + jl, lane);
+    fetch_row(ms.raw[s1i], uin, vs, (int64_t)src_row(ib - 1) * pitch + jl, lane);
     fetch_row(ms.raw[s2i], uin, vs, (int64_t)ib * pitch + jl, lane);
     fetch_wait();
     R w0[NV], w1[NV], bxm = R(0);
@@ -646,10 +655,12 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
         R u[NV], wa[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) u[v] = ms.raw[s0][v][lane];
+        ghost_psi(ib - 2, u);
         to_prim(u, g.gamma, wa);
-        fetch_row(ms.raw[s0], uin, vs, (int64_t)(ib + 1) * pitch + jl, lane);  // row ib-2 is converted
+        fetch_row(ms.raw[s0], uin, vs, (int64_t)src_row(ib + 1) * pitch + jl, lane);  // row ib-2 is converted
 #pragma unroll
         for (int v = 0; v < NV; ++v) u[v] = ms.raw[s1i][v][lane];
+        ghost_psi(ib - 1, u);
         to_prim(u, g.gamma, w0);
 #pragma unroll
         for (int v = 0; v < NV; ++v) u[v] = ms.raw[s2i][v][lane];
@@ -721,6 +732,7 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
             R u[NV], wl[NV], wr[NV], f[NV];
 #pragma unroll
             for (int v = 0; v < NV; ++v) u[v] = ms.raw[s2][v][lane];
+            ghost_psi(i + 2, u);
             to_prim(u, g.gamma, w2);
             if constexpr (kFast<R>) {
                 // pairs of variables on the packed float32x2 path
@@ -771,7 +783,7 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
         }
         // rows done with: input row i (slot s0) -> row i+3; U0 of row i -> row i+1
         if (i + 1 < ie) {
-            fetch_row(ms.raw[s0], uin, vs, (int64_t)(i + 3) * pitch + jl, lane);
+            fetch_row(ms.raw[s0], uin, vs, (int64_t)src_row(i + 3) * pitch + jl, lane);
             if (own_base) fetch_row(ms.base, u0, vs, (int64_t)(i + 1) * pitch + jl, lane);
         }
         s0 = s0 == 2 ? 0 : s0 + 1;

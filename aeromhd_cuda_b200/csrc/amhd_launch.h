@@ -31,6 +31,8 @@ struct StageParams {
     int32_t fuse_dt;               // stage 3: accumulate the CFL reduction
     int32_t march_rows;            // warp-marching kernel: rows of one work item
     int32_t n_inst;                // instances in inst (ghost fill after a marching stage)
+    int32_t pull_ghosts;           // marching kernel: read ghost cells from their interior sources,
+                                   // so stages 1 and 2 need no ghost fill of their output
 };
 
 // Work geometry of the stage kernels, passed around as one int "tile_x":

@@ -122,6 +122,8 @@ cudaError_t Launch<R>::stage(int stage, int tile_x, const StageParams &p, int gr
         }
         if (e != cudaSuccess) return e;
         // the marching kernel leaves the ghost cells of its output to this pass
+        // (not needed after stages 1 and 2 when the next stage pulls them)
+        if (p.pull_ghosts && stage < 3) return cudaSuccess;
         const int n_inst = p.inst ? p.n_inst : 1;
         if (n_inst <= 0) return cudaErrorInvalidValue;
         const int per = p.inst ? 8 : elem_blocks(4LL * (p.one.grid.ny + 2 * NG) + 4LL * p.one.grid.nx);
