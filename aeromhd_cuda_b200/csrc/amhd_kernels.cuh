@@ -2,15 +2,17 @@
 // type.  Included by amhd_f64.cu (Real = double, -fmad=false) and amhd_f32.cu
 // (Real = float).  Host-side launchers are declared in amhd_launch.h.
 //
-// The fused RK stage (rk_stage_kernel) does, per 8..16 x 32 tile of interior
-// cells: stage the tile plus its 2-cell halo of the stage's input state into
-// shared memory as primitives (float64 pressure recovery), MUSCL + HLLD on
-// every x and y face of the tile (interface states and fluxes never leave
-// shared memory / registers), flux divergence + Powell source, the SSP-RK3
-// combination with the step's base state, the passive-scalar clamp, psi
-// damping (last stage), the boundary conditions (boundary cells push their
-// values into the ghost cells that copy them), and on the last stage the CFL
-// reduction of the new state for the next dt.
+// One RK stage is one fused kernel: stage input -> primitives (float64
+// pressure recovery), MUSCL + HLLD on every x and y face, flux divergence +
+// Powell source, the SSP-RK3 combination with the step's base state, the
+// passive-scalar clamp, psi damping (last stage) and on the last stage the CFL
+// reduction of the new state for the next dt.  Two kernels implement it with
+// the same per-cell functions (update_cell_d, face_flux / hlld):
+//   march_stage_kernel (default) -- one warp walks a 28-column strip row by
+//     row, rows staged with cp.async, x-slopes and x-face fluxes carried from
+//     row to row, y neighbours by warp shuffles, no CTA barriers;
+//   rk_stage_kernel -- one CTA per 8..16 x 32 tile staged (TMA) with its halo
+//     in shared memory, boundary cells pushing their values into the ghosts.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
