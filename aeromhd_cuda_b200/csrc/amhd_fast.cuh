@@ -132,18 +132,19 @@ __device__ __forceinline__ float fast_speed(const FSide &s, float gamma, float b
     return sqrt_(fmaxf(0.5f * (tmp + sqrt_(disc)), 0.f));
 }
 
-__device__ __forceinline__ void side_flux(const FSide &s, float bxf, float bx2, float psif, float ch, float f[NV])
+__device__ __forceinline__ void side_flux(const FSide &s, float bxf, float bx2, float psif, float ch, bool glm,
+                                          float f[NV])
 {
     const float mx = s.rho * s.vx;
     f[0] = mx;
     f[1] = mx * s.vx + s.pt - bx2;
     f[2] = mx * s.vy - bxf * s.by;
     f[3] = mx * s.vz - bxf * s.bz;
-    f[4] = (ch > 0.f) ? psif : 0.f;
+    f[4] = glm ? psif : 0.f;
     f[5] = s.by * s.vx - bxf * s.vy;
     f[6] = s.bz * s.vx - bxf * s.vz;
     f[7] = (s.e + s.pt) * s.vx - bxf * s.vb;
-    f[8] = (ch > 0.f) ? bxf * ch * ch : 0.f;
+    f[8] = glm ? bxf * ch * ch : 0.f;
     f[9] = mx * s.c;
 }
 
@@ -181,12 +182,14 @@ __device__ __forceinline__ void star_energy(FSide &s, float S, float SM, float p
     s.es = ((S - s.vx) * s.e - s.pt * s.vx + ptS * SM + bxf * (s.vb - s.vbs)) * s.idsm;
 }
 
-// HLLD flux through an x-normal face (physics.py:43-276), float32
+// HLLD flux through an x-normal face (physics.py:43-276), float32.  glm: ch > 0
+// (a caller that knows it passes the constant, which removes the ch = 0 code
+// and the supersonic branch: with GLM the outer speeds bracket -ch .. ch)
 __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], float gamma, float igm1, float ch,
-                                     float half_ich, float f[NV])
+                                     float half_ich, float f[NV], bool glm)
 {
     float bxf, psif;
-    if (ch > 0.f) {
+    if (glm) {
         bxf = 0.5f * (wl[4] + wr[4]) - half_ich * (wr[8] - wl[8]);
         psif = 0.5f * (wl[8] + wr[8]) - 0.5f * ch * (wr[4] - wl[4]);
     } else {
@@ -200,7 +203,7 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
     const float cfL = fast_speed(L, gamma, bx2), cfR = fast_speed(R, gamma, bx2);
     float SL = fminf(L.vx - cfL, R.vx - cfR);
     float SR = fmaxf(L.vx + cfL, R.vx + cfR);
-    if (ch > 0.f) {
+    if (glm) {
         SL = fminf(SL, -ch);
         SR = fmaxf(SR, ch);
     }
@@ -214,10 +217,10 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
     if (SM > SR - 1e-14f) SM = SR - 1e-14f;
     const float ptS = L.pt + rdl * (SM - L.vx);
 
-    if (SL >= 0.f || SR <= 0.f) {  // supersonic: the upwind side's flux (only without GLM)
+    if (!glm && (SL >= 0.f || SR <= 0.f)) {  // supersonic: the upwind side's flux (only without GLM)
         FSide &U = SL >= 0.f ? L : R;
         side_energy(U, bxf, igm1);
-        side_flux(U, bxf, bx2, psif, ch, f);
+        side_flux(U, bxf, bx2, psif, ch, glm, f);
         return;
     }
     const float eps_rel = 1e-8f * fmaxf(fabsf(ptS), 1.f);
@@ -235,7 +238,7 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
     const float S = left ? SL : SR;
     side_energy(K, bxf, igm1);
     star_energy(K, S, SM, ptS, bxf);
-    side_flux(K, bxf, bx2, psif, ch, f);
+    side_flux(K, bxf, bx2, psif, ch, glm, f);
     // + S (U* - U)
     f[0] += S * (K.rs - K.rho);
     f[1] += S * (K.rs * SM - K.rho * K.vx);
@@ -264,7 +267,7 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
         f[6] += SA * (bzds - K.bzs);
         f[7] += SA * (eds - K.es);
     }
-    if (ch > 0.f) {
+    if (glm) {
         f[4] = psif;
         f[8] = ch * ch * bxf;
     }

@@ -219,7 +219,11 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
         }
         // enforce_scalar_bounds, solver.py:199-204
         R rho = np_max(out[RHO], R(FLOOR_RHO));
-        R cc = np_min(np_max(out[RHOC] / rho, R(0)), R(1));
+        R cc;
+        if constexpr (kFast<R>)
+            cc = np_min(np_max(out[RHOC] * fast::rcp(rho), R(0)), R(1));
+        else
+            cc = np_min(np_max(out[RHOC] / rho, R(0)), R(1));
         out[RHOC] = rho * cc;
         if (STAGE == 3) {
             if (ch > 0.0) out[PSI] *= R(decay);  // solver.py:331-333
@@ -232,8 +236,16 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
 #pragma unroll
                 for (int k = 0; k < 4; ++k) q[k] = umax64(q[k], ord_bits(qd[k]));
             }
+            if constexpr (kFast<R>) {
+                // x * 0 is NaN exactly when x is not finite: one test for the cell
+                float2 z = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) bad |= !isfinite((double)out[v]);
+                for (int v = 0; v < NV; v += 2) z = __ffma2_rn(make_float2(out[v], out[v + 1]), make_float2(0.f, 0.f), z);
+                bad |= !(z.x == 0.f && z.y == 0.f);
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) bad |= !isfinite((double)out[v]);
+            }
         }
     }
     // write the cell, then every ghost that copies it (apply_bc, solver.py:158-197)
@@ -416,7 +428,7 @@ __device__ __forceinline__ bool rk_stage_tile(const StageParams &p, TileSmem<R, 
                     wr[v] = sm.w[rot[v]][a + NG][c + 2] - 0.5f * sm.sy[rot[v]][a][c + 1];
                 }
             }
-            fast::hlld(wl, wr, gam, igm1, chr, half_ich, fl);
+            fast::hlld(wl, wr, gam, igm1, chr, half_ich, fl, chr > 0.f);
         } else {
             if (xf) {
 #pragma unroll
@@ -552,12 +564,14 @@ __device__ __forceinline__ R cell_slope(R wm, R w0, R wp, int limiter)
         return limited_slope(wm, w0, wp, limiter);
 }
 
-// HLLD flux of one face from its reconstructed states (slot order of an x face)
+// HLLD flux of one face from its reconstructed states (slot order of an x face);
+// glm: chr > 0 (see fast::hlld)
 template <typename R>
-__device__ __forceinline__ void face_flux(R wl[NV], R wr[NV], R gam, float igm1, R chr, float half_ich, R f[NV])
+__device__ __forceinline__ void face_flux(R wl[NV], R wr[NV], R gam, float igm1, R chr, float half_ich, R f[NV],
+                                          bool glm)
 {
     if constexpr (kFast<R>) {
-        fast::hlld(wl, wr, gam, igm1, chr, half_ich, f);
+        fast::hlld(wl, wr, gam, igm1, chr, half_ich, f, glm);
     } else {
         // floors of physics.py:331-334 (slot 7 is p in both orders)
         wl[RHO] = np_max(wl[RHO], R(FLOOR_RHO));
@@ -568,24 +582,78 @@ __device__ __forceinline__ void face_flux(R wl[NV], R wr[NV], R gam, float igm1,
     }
 }
 
-// per-warp shared memory of the marching kernel, [var][lane] (conflict-free);
-// every entry but fy is private to its lane
+// per-warp shared memory of the marching kernel.  A row holds the 10 planes of
+// 32 lanes as [pair][lane][2]: variables 2k and 2k+1 of one lane side by side,
+// so that a lane moves a pair with one 8-byte (float) or 16-byte (double)
+// access and a warp's access covers 256 / 512 contiguous bytes (conflict-free).
+// Every row but fy is private to its lane.
+template <typename R>
+using MarchRow = R[NV / 2][32][2];
+
 template <typename R>
 struct MarchSmem {
-    R raw[3][NV][32];  // conserved stage-input rows i .. i+2 (cp.async), row r in slot r % 3
-    R base[NV][32];    // U0 of row i when U0 is not the stage input
-    R sx[NV][32];      // limited x-slope of the current row
-    R fx[NV][32];      // flux through the x face below the current row
-    R fy[NV][32];      // flux through each lane's left y face of the current row (read by the lane on the left)
+    MarchRow<R> raw[3];  // conserved stage-input rows i .. i+2 (cp.async), row r in slot r % 3
+    MarchRow<R> base;    // U0 of row i when U0 is not the stage input
+    MarchRow<R> sx;      // limited x-slope of the current row
+    MarchRow<R> fx;      // flux through the x face below the current row
+    MarchRow<R> fy;      // flux through each lane's left y face of the current row (read by the lane on the left)
 };
+
+template <typename R>
+struct Pair;
+template <>
+struct Pair<float> {
+    using T = float2;
+};
+template <>
+struct Pair<double> {
+    using T = double2;
+};
+
+// the 10 values of one lane's column of a row, pairwise
+template <typename R>
+__device__ __forceinline__ void row_load(const MarchRow<R> &r, int lane, R u[NV])
+{
+#pragma unroll
+    for (int k = 0; k < NV / 2; ++k) {
+        const typename Pair<R>::T t = *reinterpret_cast<const typename Pair<R>::T *>(&r[k][lane][0]);
+        u[2 * k] = t.x;
+        u[2 * k + 1] = t.y;
+    }
+}
+template <typename R>
+__device__ __forceinline__ void row_store(MarchRow<R> &r, int lane, const R u[NV])
+{
+#pragma unroll
+    for (int k = 0; k < NV / 2; ++k) {
+        typename Pair<R>::T t;
+        t.x = u[2 * k];
+        t.y = u[2 * k + 1];
+        *reinterpret_cast<typename Pair<R>::T *>(&r[k][lane][0]) = t;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ typename Pair<R>::T pair_load(const MarchRow<R> &r, int k, int lane)
+{
+    return *reinterpret_cast<const typename Pair<R>::T *>(&r[k][lane][0]);
+}
+template <typename R>
+__device__ __forceinline__ void pair_store(MarchRow<R> &r, int k, int lane, R a, R b)
+{
+    typename Pair<R>::T t;
+    t.x = a;
+    t.y = b;
+    *reinterpret_cast<typename Pair<R>::T *>(&r[k][lane][0]) = t;
+}
 
 // asynchronous copy of one row of the state (this lane's column) into shared memory
 template <typename R>
-__device__ __forceinline__ void fetch_row(R (*dst)[32], const R *u, int64_t vs, int64_t gi, int lane)
+__device__ __forceinline__ void fetch_row(MarchRow<R> &dst, const R *u, int64_t vs, int64_t gi, int lane)
 {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
-        const uint32_t d = (uint32_t)__cvta_generic_to_shared(&dst[v][lane]);
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(&dst[v >> 1][lane][v & 1]);
         if constexpr (sizeof(R) == 4)
             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(u + v * vs + gi) : "memory");
         else
@@ -595,22 +663,14 @@ __device__ __forceinline__ void fetch_row(R (*dst)[32], const R *u, int64_t vs, 
 }
 __device__ __forceinline__ void fetch_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-template <typename R, int STAGE>
-__device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &ms, int item, int lane,
-                                           unsigned long long q[4], bool &bad, amhd_control *&ctl_out)
+// One work item: rows [ib, ie) of a 28-column strip.  SPEC: the item runs the
+// van Leer limiter with GLM on (ch > 0), known at compile time -- the walk the
+// solver's loop takes; otherwise both are read at run time.
+template <typename R, int STAGE, bool SPEC>
+__device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &ms, const amhd_instance &in,
+                                           const amhd_grid &g, int item, int lane, double dt, double ch, double decay,
+                                           unsigned long long q[4], bool &bad)
 {
-    int ii;
-    const amhd_instance &in = inst_of(p, item, ii);
-    const amhd_grid g = in.grid;
-    amhd_control *ctl = p.ctl ? p.ctl + ii : nullptr;
-    ctl_out = ctl;
-    double dt = p.dt, ch = p.ch, decay = p.decay;
-    if (p.use_ctl) {
-        if (!ctl->active) return;
-        dt = ctl->dt;
-        ch = ctl->ch;
-        decay = ctl->decay;
-    }
     const int local = item - in.first_tile;
     const int strip = local % in.tiles_y, chunk = local / in.tiles_y;
     const int j = kMarchCols * strip + lane;  // storage column of this lane (first interior column - 2 + lane)
@@ -636,7 +696,8 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
     const bool own_base = STAGE >= 1 && p.u0 != p.uin;
 
     const R gam = R(g.gamma), chr = R(ch);
-    const int lim = g.limiter;
+    const int lim = SPEC ? AMHD_LIMITER_VANLEER : g.limiter;
+    const bool glm = SPEC || chr > R(0);
     const float igm1 = 1.0f / float(g.gamma - 1.0), half_ich = ch > 0.0 ? float(0.5 / ch) : 0.f;
     constexpr int rot[NV] = {0, 2, 1, 3, 5, 4, 6, 7, 8, 9};
 
@@ -655,20 +716,18 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
     R w0[NV], w1[NV], bxm = R(0);
     {
         R u[NV], wa[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) u[v] = ms.raw[s0][v][lane];
+        row_load(ms.raw[s0], lane, u);
         ghost_psi(ib - 2, u);
         to_prim(u, g.gamma, wa);
         fetch_row(ms.raw[s0], uin, vs, (int64_t)src_row(ib + 1) * pitch + jl, lane);  // row ib-2 is converted
-#pragma unroll
-        for (int v = 0; v < NV; ++v) u[v] = ms.raw[s1i][v][lane];
+        row_load(ms.raw[s1i], lane, u);
         ghost_psi(ib - 1, u);
         to_prim(u, g.gamma, w0);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) u[v] = ms.raw[s2i][v][lane];
+        row_load(ms.raw[s2i], lane, u);
         to_prim(u, g.gamma, w1);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) ms.sx[v][lane] = cell_slope(wa[v], w0[v], w1[v], lim);  // row ib-1
+        for (int v = 0; v < NV; ++v) wa[v] = cell_slope(wa[v], w0[v], w1[v], lim);
+        row_store(ms.sx, lane, wa);  // slope of row ib-1
     }
     s0 = s1i;  // slot of row ib-1
 
@@ -722,9 +781,10 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
                     }
                 }
             }
-            face_flux(wl, wr, gam, igm1, chr, half_ich, f);
+            face_flux(wl, wr, gam, igm1, chr, half_ich, f, glm);
 #pragma unroll
-            for (int k = 0; k < NV; ++k) ms.fy[rot[k]][lane] = f[k];
+            for (int k = 0; k < NV; ++k) wl[rot[k]] = f[k];  // back to the unrotated slot order
+            row_store(ms.fy, lane, wl);
         }
         // x: primitives of row i+2, slope of row i+1, flux through face i+1/2 and
         // the x-flux difference of row i
@@ -732,8 +792,7 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
         R w2[NV], dfx[NV];
         {
             R u[NV], wl[NV], wr[NV], f[NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) u[v] = ms.raw[s2][v][lane];
+            row_load(ms.raw[s2], lane, u);
             ghost_psi(i + 2, u);
             to_prim(u, g.gamma, w2);
             if constexpr (kFast<R>) {
@@ -742,30 +801,33 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
                 for (int v = 0; v < NV; v += 2) {
                     const float2 a = make_float2(w0[v], w0[v + 1]), b = make_float2(w1[v], w1[v + 1]);
                     const float2 s1 = fast::slope2(a, b, make_float2(w2[v], w2[v + 1]), lim);
-                    const float2 l = __ffma2_rn(make_float2(0.5f, 0.5f),
-                                                make_float2(ms.sx[v][lane], ms.sx[v + 1][lane]), a);
+                    const float2 l = __ffma2_rn(make_float2(0.5f, 0.5f), pair_load(ms.sx, v >> 1, lane), a);
                     const float2 r = __ffma2_rn(make_float2(-0.5f, -0.5f), s1, b);
                     wl[v] = l.x;
                     wl[v + 1] = l.y;
                     wr[v] = r.x;
                     wr[v + 1] = r.y;
-                    ms.sx[v][lane] = s1.x;
-                    ms.sx[v + 1][lane] = s1.y;
+                    pair_store(ms.sx, v >> 1, lane, s1.x, s1.y);
                 }
             } else {
+                R sx[NV];
+                row_load(ms.sx, lane, sx);
 #pragma unroll
                 for (int v = 0; v < NV; ++v) {
                     const R s1 = cell_slope(w0[v], w1[v], w2[v], lim);
-                    wl[v] = w0[v] + R(0.5) * ms.sx[v][lane];
+                    wl[v] = w0[v] + R(0.5) * sx[v];
                     wr[v] = w1[v] - R(0.5) * s1;
-                    ms.sx[v][lane] = s1;
+                    sx[v] = s1;
                 }
+                row_store(ms.sx, lane, sx);
             }
-            face_flux(wl, wr, gam, igm1, chr, half_ich, f);
+            face_flux(wl, wr, gam, igm1, chr, half_ich, f, glm);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) {
-                dfx[v] = f[v] - ms.fx[v][lane];
-                ms.fx[v][lane] = f[v];
+            for (int k = 0; k < NV / 2; ++k) {
+                const typename Pair<R>::T o = pair_load(ms.fx, k, lane);
+                dfx[2 * k] = f[2 * k] - o.x;
+                dfx[2 * k + 1] = f[2 * k + 1] - o.y;
+                pair_store(ms.fx, k, lane, f[2 * k], f[2 * k + 1]);
             }
         }
         if (full) {
@@ -773,13 +835,19 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
             if (out_lane) {
                 R dfy[NV];
 #pragma unroll
-                for (int v = 0; v < NV; ++v) dfy[v] = ms.fy[v][lane + 1] - ms.fy[v][lane];  // output lanes stop at 29
+                for (int k = 0; k < NV / 2; ++k) {  // output lanes stop at 29
+                    const typename Pair<R>::T a = pair_load(ms.fy, k, lane + 1), b = pair_load(ms.fy, k, lane);
+                    dfy[2 * k] = a.x - b.x;
+                    dfy[2 * k + 1] = a.y - b.y;
+                }
                 auto pw = [&]() {
                     return PowellIn<R>{w0[BX], bxm, w1[BX], w0[BY], bym, byp, w0[IVX], w0[IVY], w0[IVZ], w0[BZ]};
                 };
-                const int slot = s0;
-                auto in_at = [&](int v) { return ms.raw[slot][v][lane]; };
-                auto base_at = [&](int v) { return own_base ? ms.base[v][lane] : ms.raw[slot][v][lane]; };
+                R us[NV], ub[NV];
+                row_load(ms.raw[s0], lane, us);
+                row_load(own_base ? ms.base : ms.raw[s0], lane, ub);
+                auto in_at = [&](int v) { return us[v]; };
+                auto base_at = [&](int v) { return ub[v]; };
                 update_cell_d<R, STAGE, false>(p, g, uout, i, j, dfx, dfy, pw, base_at, in_at, dt, ch, decay, q, bad);
             }
         }
@@ -797,6 +865,28 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
         }
     }
     __syncwarp();  // the next item reuses the shared rows
+}
+
+template <typename R, int STAGE>
+__device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &ms, int item, int lane,
+                                           unsigned long long q[4], bool &bad, amhd_control *&ctl_out)
+{
+    int ii;
+    const amhd_instance &in = inst_of(p, item, ii);
+    const amhd_grid g = in.grid;
+    amhd_control *ctl = p.ctl ? p.ctl + ii : nullptr;
+    ctl_out = ctl;
+    double dt = p.dt, ch = p.ch, decay = p.decay;
+    if (p.use_ctl) {
+        if (!ctl->active) return;
+        dt = ctl->dt;
+        ch = ctl->ch;
+        decay = ctl->decay;
+    }
+    if (g.limiter == AMHD_LIMITER_VANLEER && R(ch) > R(0))
+        march_walk<R, STAGE, true>(p, ms, in, g, item, lane, dt, ch, decay, q, bad);
+    else
+        march_walk<R, STAGE, false>(p, ms, in, g, item, lane, dt, ch, decay, q, bad);
 }
 
 // resident CTAs of kMarchThreads per SM the register budget is shaped for:
