@@ -21,8 +21,15 @@ AMHD_ERR_UNSUPPORTED = -5
 AMHD_F64 = 0
 AMHD_F32 = 1
 LIMITER_CODES = {"vanleer": 0, "minmod": 1}
-# stage-kernel geometry the library starts with (amhd_set_tiling): warp-marching, 16 rows per item
-DEFAULT_TILE_X = -16
+# stage-kernel geometry the library starts with (amhd_set_tiling): 0 = per precision,
+# the warp-marching kernel with default_tile_x(precision) rows per item
+DEFAULT_TILE_X = 0
+
+
+def default_tile_x(precision: str) -> int:
+    """Rows per marching item of the library default: 24 in float32, 16 in float64
+    (float64 runs 2 CTAs per SM, where 16-row items fill whole waves at 2048^2)."""
+    return -24 if precision == "fp32" else -16
 
 AMHD_FLAG_NONFINITE = 1
 AMHD_FLAG_DT_TINY = 2

@@ -21,7 +21,7 @@ import os
 from dataclasses import asdict, dataclass
 from typing import Callable, Dict, Iterable, List, Optional, Sequence
 
-TILE_XS = (4, 8, 16, -16, -32, -64)
+TILE_XS = (4, 8, 16, -16, -24, -32, -64)
 ORDERS = ("instance", "interleave", "largest_first")
 GRIDS = (-1, 0)  # -1: one CTA per tile; 0: persistent (resident CTAs per SM x SMs)
 

@@ -39,11 +39,17 @@ int fail(int code, const char *fmt, ...)
 constexpr int kNG = 2;
 constexpr int kTY = 32;
 
-int g_tile_x = -16;  // warp-marching kernel, 16 rows per work item
+int g_tile_x = 0;  // 0: per precision (tile_of)
 int g_ctas_per_sm = 0;
 int g_use_tma = 1;
 
 inline size_t elem_size(int dtype) { return dtype == AMHD_F32 ? 4 : 8; }
+
+// stage-kernel geometry of a grid: the one set by amhd_set_tiling, else the
+// marching kernel with 24 rows per item in float32 and 16 in float64 (the
+// fastest measured at 2048 x 2048: float64 runs 2 CTAs per SM, where 16-row
+// items fill whole waves)
+inline int tile_of(const amhd_grid *g) { return g_tile_x ? g_tile_x : (g->dtype == AMHD_F32 ? -24 : -16); }
 
 int check_grid(const amhd_grid *g)
 {
@@ -276,7 +282,8 @@ int amhd_padded_layout(int32_t nx, int32_t ny, int32_t dtype, int32_t *pitch, in
 
 int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm)
 {
-    if (!valid_geometry(tile_x)) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8, 16 or -1024..-4 (marching rows)");
+    if (tile_x != 0 && !valid_geometry(tile_x))
+        return fail(AMHD_ERR_ARG, "tile_x must be 0 (default), 4, 8, 16 or -1024..-4 (marching rows)");
     if (ctas_per_sm < 0 || ctas_per_sm > 32) return fail(AMHD_ERR_ARG, "ctas_per_sm out of range");
     g_tile_x = tile_x;
     g_ctas_per_sm = ctas_per_sm;
@@ -471,7 +478,7 @@ int amhd_compute_rhs(const amhd_grid *g, void *U, void *R, double ch, void *stre
     cudaStream_t s = S(stream);
     CK(run_bc_fill(g, U, s));
     CK(cudaMemsetAsync(R, 0, (size_t)g->var_stride * 10 * elem_size(g->dtype), s));
-    const int tx = g_tile_x;
+    const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
     StageParams p;
     memset(&p, 0, sizeof p);
@@ -500,7 +507,7 @@ int amhd_step_ssprk3(const amhd_grid *g, void *U, void *U1, void *U2, double dt,
             CK(Launch<float>::bflux_accum(*g, static_cast<const float *>(U), ctl, dt, s));
     }
     CK(run_bc_fill(g, U, s));  // compute_rhs(U0) fills U0's ghosts first (solver.py:276)
-    const int tx = g_tile_x;
+    const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
     const int n_tiles = one.tiles_x * one.tiles_y;
     return three_stages(g, one, nullptr, nullptr, n_tiles, tx, stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm), U,
@@ -514,7 +521,7 @@ int amhd_rk_stage(const amhd_grid *g, int32_t stage, const void *Uin, const void
     if (stage < 1 || stage > 3) return fail(AMHD_ERR_ARG, "stage must be 1, 2 or 3");
     const void *ptrs[3] = {Uin, U0, Uout};
     if (int e = check_padded(g, ptrs, 3)) return e;
-    const int tx = g_tile_x;
+    const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
     StageParams p;
     memset(&p, 0, sizeof p);
@@ -560,7 +567,7 @@ int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *
     if (!ctl) return fail(AMHD_ERR_ARG, "NULL control");
     if (n_steps < 0) return fail(AMHD_ERR_ARG, "n_steps < 0");
     cudaStream_t s = S(stream);
-    const int tx = g_tile_x;
+    const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
     const int n_tiles = one.tiles_x * one.tiles_y;
     const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
@@ -592,7 +599,7 @@ int amhd_advance_stage(const amhd_grid *g, int32_t stage, void *U, void *U1, voi
     const void *ptrs[3] = {U, U1, U2};
     if (int e = check_padded(g, ptrs, 3)) return e;
     if (!ctl) return fail(AMHD_ERR_ARG, "NULL control");
-    const int tx = g_tile_x;
+    const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
     StageParams p;
     memset(&p, 0, sizeof p);
@@ -614,7 +621,7 @@ int amhd_advance_finish(const amhd_grid *g, void *U, amhd_control *ctl, int32_t 
 {
     if (int e = check_grid(g)) return e;
     if (!U || !ctl) return fail(AMHD_ERR_ARG, "NULL argument");
-    const amhd_instance one = single_instance(g, g_tile_x);
+    const amhd_instance one = single_instance(g, tile_of(g));
     CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, advance ? 1 : 0, 0, S(stream)));
     return AMHD_OK;
 }
@@ -628,7 +635,7 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
     if (!ctl || !ms_out) return fail(AMHD_ERR_ARG, "NULL argument");
     if (n_steps <= 0) return fail(AMHD_ERR_ARG, "n_steps must be positive");
     cudaStream_t s = S(stream);
-    const int tx = g_tile_x;
+    const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
     const int n_tiles = one.tiles_x * one.tiles_y;
     const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
@@ -692,7 +699,7 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
     // dt of this step from the uploaded state, ghosts as given (solver.py:476-479)
     if (int e = control_upload(ctl, t, t_end, 0, 1, s)) return e;
     CK(run_dt_reduce(g, dev_U, 0, ctl, s));
-    const int tx = g_tile_x;
+    const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
     CK(run_finalize(g->dtype, nullptr, 1, one, dev_U, ctl, 0, 0, s));
     CK(run_bc_fill(g, dev_U, s));

@@ -218,7 +218,7 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
     const float ptS = L.pt + rdl * (SM - L.vx);
 
     if (!glm && (SL >= 0.f || SR <= 0.f)) {  // supersonic: the upwind side's flux (only without GLM)
-        FSide &U = SL >= 0.f ? L : R;
+        FSide U = SL >= 0.f ? L : R;  // a copy: writing through a runtime-chosen reference would put L and R in local memory
         side_energy(U, bxf, igm1);
         side_flux(U, bxf, bx2, psif, ch, glm, f);
         return;
@@ -234,7 +234,7 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
 
     const bool left = (SAL >= 0.f) || (SM >= 0.f);
     const bool dstar = left ? !(SAL >= 0.f) : (SAR >= 0.f);
-    FSide &K = left ? L : R;
+    FSide K = left ? L : R;  // a copy (see above)
     const float S = left ? SL : SR;
     side_energy(K, bxf, igm1);
     star_energy(K, S, SM, ptS, bxf);

@@ -145,7 +145,7 @@ class _GridView:
 
 
 class Ensemble:
-    def __init__(self, configs: Sequence[Config], tile_x: int = -16, order: str = "instance", ctas: int = 0,
+    def __init__(self, configs: Sequence[Config], tile_x: int = 0, order: str = "instance", ctas: int = 0,
                  device=None, use_tma: bool = True):
         if not configs:
             raise ValueError("empty ensemble")
@@ -161,7 +161,8 @@ class Ensemble:
         self.code = _lib.AMHD_F64 if self.dtype == torch.float64 else _lib.AMHD_F32
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.n = len(self.configs)
-        self.tile_x = int(tile_x)
+        tile_x = int(tile_x) or _lib.default_tile_x(self.precision)  # 0: the library default
+        self.tile_x = tile_x
         self.ctas = int(ctas)
         self.use_tma = bool(use_tma)
         self.layouts, off = pack_layout(self.configs, self.code)

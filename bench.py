@@ -53,8 +53,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--tma", type=int, default=1, help="stage tiles with TMA (1) or 128-bit loads (0)")
-    ap.add_argument("--tile-x", type=int, default=-16,
-                    help="stage kernel geometry: 4, 8, 16 (tiled kernel rows) or negative (warp-marching rows)")
+    ap.add_argument("--tile-x", type=int, default=0,
+                    help="stage kernel geometry: 4, 8, 16 (tiled kernel rows), negative (warp-marching rows) "
+                         "or 0 (the library default: marching, 24 rows in fp32, 16 in fp64)")
     ap.add_argument("--decomp", action="store_true",
                     help="one n x n grid split over the ranks by x rows (strong scaling) instead of replicas")
     ap.add_argument("--ensemble", type=int, default=0,
@@ -253,6 +254,7 @@ def run_ours(a, world, rank, local):
     _lib.call("amhd_init")
     _lib.call("amhd_set_tma", int(a.tma))
     _lib.call("amhd_set_tiling", int(a.tile_x), 0)
+    tx = int(a.tile_x) or _lib.default_tile_x(a.precision)  # the geometry the fp32 / fp64 run uses
     cfg = ot_config(n, a.precision)
     s = MHDSolver(cfg)
     s.set_primitive(ic.orszag_tang(s))
@@ -289,7 +291,7 @@ def run_ours(a, world, rank, local):
     stage_ms = prof[0] + prof[1] + prof[2]
     alg_bytes_step = 80 * es * cells
     achieved = alg_bytes_step * a.steps / (stage_ms / 1e3) / 1e9
-    tr = profile_traffic(a.tile_x)
+    tr = profile_traffic(tx)
     traffic = None
     if tr.get("precision") == a.precision and tr.get("n"):
         try:
@@ -298,7 +300,7 @@ def run_ours(a, world, rank, local):
             traffic = None
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": hbm_kind,
-                "kernel": stage_kernel_name(a.tile_x) + " (3 launches/step)",
+                "kernel": stage_kernel_name(tx) + " (3 launches/step)",
                 "algorithmic_bytes_per_step": alg_bytes_step,
                 "ms_per_step": {"stage1": prof[0] / a.steps, "stage2": prof[1] / a.steps,
                                 "stage3_fused_dt": prof[2] / a.steps, "finalize": prof[3] / a.steps}}
@@ -368,10 +370,10 @@ def run_ours(a, world, rank, local):
         "config": {"workload": f"orszag_tang_{n}x{n}_{a.precision}", "nx": n, "ny": n, "precision": a.precision,
                    "pressure_recovery": "f64", "dt_reduction": "f64",
                    "l2": "inputs larger than L2 (3 state buffers of %.0f MB)" % (10 * (n + 4) * (n + 4) * es / 1e6),
-                   "parallelism": f"replicas x{world}", "stage_kernel": stage_geometry(a.tile_x),
-                   "staging": ("cp.async rows" if a.tile_x < 0 else
+                   "parallelism": f"replicas x{world}", "stage_kernel": stage_geometry(tx),
+                   "staging": ("cp.async rows" if tx < 0 else
                                "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads")},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step(a.tile_x) * a.steps,
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step(tx) * a.steps,
         "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
     }
     return line
@@ -386,6 +388,7 @@ def run_decomp(a, world, rank):
     from aeromhd_cuda_b200.solver import MHDSolver
     _lib.call("amhd_init")
     _lib.call("amhd_set_tiling", int(a.tile_x), 0)
+    tx = int(a.tile_x) or _lib.default_tile_x(a.precision)
     cfg = ot_config(a.n, a.precision)
     full = MHDSolver(ot_config(a.n, a.precision))   # whole-grid initial state on every rank
     full.set_primitive(ic.orszag_tang(full))
@@ -412,9 +415,9 @@ def run_decomp(a, world, rank):
         "data": "synthetic (analytic Orszag-Tang initial data)",
         "config": {"workload": f"orszag_tang_{a.n}x{a.n}_{a.precision}", "nx": a.n, "ny": a.n,
                    "precision": a.precision, "parallelism": f"x-row split over {world} ranks",
-                   "rows_per_rank": d.r1 - d.r0, "stage_kernel": stage_geometry(a.tile_x),
+                   "rows_per_rank": d.r1 - d.r0, "stage_kernel": stage_geometry(tx),
                    "l2": "inputs larger than L2 (3 state buffers per rank)"},
-        "gpu_launches": launches_per_step(a.tile_x) * a.steps,
+        "gpu_launches": launches_per_step(tx) * a.steps,
         "clocks": clk.summary(),
     }
 
@@ -444,7 +447,7 @@ def run_ensemble(a, world):
         raise SystemExit("non-finite state in the ensemble benchmark")
     return {"value": world * cells * k / (ms / 1e3), "unit": "zone-updates/s", "instances": a.ensemble,
             "cells": cells, "steps": k, "ms_per_step": ms / k,
-            "schedule": {"tile_x": a.tile_x, "order": "instance", "grid": "persistent"}}
+            "schedule": {"tile_x": ens.tile_x, "order": "instance", "grid": "persistent"}}
 
 
 def run_reference(a, world, rank):

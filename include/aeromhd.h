@@ -117,8 +117,9 @@ size_t amhd_control_size(void);
  * fluxes carried from row to row (no CTA barriers).  ctas_per_sm: 0 = one CTA
  * per tile (tiled) / per 4 items (marching), otherwise a persistent grid of
  * ctas_per_sm x SM-count CTAs.  Both kernels compute the same arithmetic
- * (identical float64 results).  Default -16.  Process-wide; chosen by the autotuner.  The
- * same tile_x values are accepted by amhd_stage_info and
+ * (identical float64 results).  0 restores the default: -24 for float32 grids, -16
+ * for float64 grids.  Process-wide; chosen by the autotuner.  The
+ * same nonzero tile_x values are accepted by amhd_stage_info and
  * amhd_ensemble_advance.  No counterpart in the reference. */
 int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm);
 /* Stage the tile + halo with TMA (cp.async.bulk.tensor) when on (default) or

@@ -63,7 +63,8 @@ def test_argument_errors_are_codes_not_crashes(L):
     assert L.amhd_set_tiling(-2000, 0) == _lib.AMHD_ERR_ARG
     assert L.amhd_set_tiling(8, 0) == _lib.AMHD_OK
     assert L.amhd_set_tiling(-16, 0) == _lib.AMHD_OK
-    assert L.amhd_set_tiling(_lib.DEFAULT_TILE_X, 0) == _lib.AMHD_OK
+    assert L.amhd_set_tiling(_lib.DEFAULT_TILE_X, 0) == _lib.AMHD_OK  # 0: per-precision default
+    assert (_lib.default_tile_x("fp32"), _lib.default_tile_x("fp64")) == (-24, -16)
     g = _lib.Grid(nx=8, ny=8, pitch=4, dtype=0, var_stride=1000, dx=0.1, dy=0.1, gamma=1.4, cfl=0.3,
                   glm_alpha=1.5)
     # pitch < ny+4 is refused before any device call

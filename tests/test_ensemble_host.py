@@ -66,7 +66,7 @@ def test_shard_balances_cells_and_covers_everything():
 
 def test_candidates_and_choice():
     ens = candidates(True, "fp32")
-    assert Candidate(8, "interleave", 0) in ens and len(ens) == 6 * 3 * 2
+    assert Candidate(8, "interleave", 0) in ens and len(ens) == 7 * 3 * 2
     assert Candidate(-32, "instance", 0) in ens  # warp-marching kernel, 32 rows per item
     assert all(c.tile_x != 16 for c in candidates(True, "fp64"))
     assert all(c.order == "instance" for c in candidates(False, "fp32"))

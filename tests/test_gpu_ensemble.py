@@ -13,7 +13,7 @@ def small_configs(precision, n=6, seed=11):
     return draw_configs(n, seed=seed, t_end=3.0, precision=precision, ny_choices=(32, 64))
 
 
-@pytest.mark.parametrize("tile_x", [8, -16])
+@pytest.mark.parametrize("tile_x", [8, -16, -24])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_instances_equal_single_grid_runs(precision, tile_x):
     from aeromhd_cuda_b200 import _lib

@@ -89,7 +89,7 @@ def step_cfg(bcx, bcy, By, **kw):
 
 
 # 4, 8, 16: tiled kernel; negative: warp-marching kernel with that many rows per work item
-@pytest.mark.parametrize("tile_x", [8, 4, 16, -4, -6, -64])
+@pytest.mark.parametrize("tile_x", [8, 4, 16, -4, -6, -24, -64])
 @pytest.mark.parametrize("k", range(len(STEP_CASES)))
 def test_three_steps_bit_exact(amhd, k, tile_x):
     g = golden("steps.npz")
