@@ -353,7 +353,8 @@ def test_tma_staging_matches_plain_loads_single_grid(amhd, precision):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
-@pytest.mark.parametrize("shape,rows", [((80, 80), -8), ((75, 61), -5), ((64, 130), -32), ((33, 29), -4)])
+@pytest.mark.parametrize("shape,rows", [((80, 80), -8), ((75, 61), -5), ((64, 130), -32), ((33, 29), -4),
+                                        ((40, 200), -24)])
 def test_marching_kernel_matches_tiled(amhd, precision, shape, rows):
     """Warp-marching stage kernel vs the tiled one on odd shapes (strips of 28
     columns and chunks of rows that do not divide the grid): identical bits in
@@ -383,16 +384,17 @@ def test_marching_kernel_matches_tiled(amhd, precision, shape, rows):
         assert rel_l1(np_(b), np_(a)) < 1e-6
 
 
-@pytest.mark.parametrize("bcx", ["extrapolation", "characteristic"])
-def test_marching_kernel_rmi_device_loop_bit_exact(amhd, bcx):
+@pytest.mark.parametrize("bcx,ny", [("extrapolation", 40), ("characteristic", 40), ("extrapolation", 124),
+                                    ("characteristic", 124)])
+def test_marching_kernel_rmi_device_loop_bit_exact(amhd, bcx, ny):
     """Shocked-interface problem (outflow / characteristic x boundaries, Powell
     source on) on the marching kernel against the tiled kernel, 25 device-loop
-    steps in float64."""
+    steps in float64 (ny = 124: several strips of 28 columns)."""
     res = []
     try:
         for tx in (8, -16):
             amhd.lib.call("amhd_set_tiling", tx, 0)
-            cfg = C(nx=96, ny=40, B_transverse=0.3, glm_ch=0.0, bc_x_type=bcx, t_end=1.0)
+            cfg = C(nx=96, ny=ny, B_transverse=0.3, glm_ch=0.0, bc_x_type=bcx, t_end=1.0)
             s = amhd.solver.MHDSolver(cfg)
             s.initialize()
             s.advance(max_steps=25, chunk=25, graph=False)
