@@ -159,16 +159,20 @@ cudaError_t run_dt_reduce(const amhd_grid *g, const void *A, int from_prim, amhd
 }
 
 // three fused stages of one step; dt/ch/decay from the host or from ctl
+// One run-loop step.  defer_fill (marching kernel): U's ghost cells are not
+// filled after stage 3 either -- the next step pulls them like those of U1 and
+// U2 -- and the caller fills them after its last step (fill_after_loop).
 int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instance *insts, const int32_t *tile_inst,
                  int n_tiles, int tile_x, int grid, void *U, void *U1, void *U2, amhd_control *ctl, int use_ctl,
                  double dt, double ch, double decay, int fuse_dt, cudaStream_t s, const int32_t *tile_order = nullptr,
-                 const CUtensorMap *tmaps = nullptr, int n_inst = 1)
+                 const CUtensorMap *tmaps = nullptr, int n_inst = 1, int defer_fill = 0)
 {
     StageParams p;
     memset(&p, 0, sizeof p);
     p.inst = insts;
     p.n_inst = n_inst;
     p.pull_ghosts = 1;  // the run loop: U1 and U2 are internal, their ghost cells are never stored
+    p.defer_fill = defer_fill;
     p.one = one;
     p.tile_inst = tile_inst;
     p.tile_order = tile_order;
@@ -195,6 +199,20 @@ int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instan
         p.fuse_dt = st == 3 ? fuse_dt : 0;
         CK(run_stage(dtype, st, tile_x, p, grid, s));
     }
+    return AMHD_OK;
+}
+
+// the ghost cells of U after a run loop whose steps deferred them (every instance)
+int fill_after_loop(int dtype, const amhd_instance &one, const amhd_instance *insts, int n_inst, void *U,
+                    cudaStream_t s)
+{
+    StageParams p;
+    memset(&p, 0, sizeof p);
+    p.inst = insts;
+    p.n_inst = n_inst;
+    p.one = one;
+    p.uout = U;
+    CK(dtype == AMHD_F64 ? Launch<double>::march_fill(p, s) : Launch<float>::march_fill(p, s));
     return AMHD_OK;
 }
 
@@ -571,11 +589,15 @@ int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *
     const amhd_instance one = single_instance(g, tx);
     const int n_tiles = one.tiles_x * one.tiles_y;
     const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
+    const int defer = is_march(tx);
     for (int k = 0; k < n_steps; ++k) {
-        if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, grid, U, U1, U2, ctl, 1, 0, 0, 1, 1, s))
+        if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, grid, U, U1, U2, ctl, 1, 0, 0, 1, 1, s,
+                                 nullptr, nullptr, 1, defer))
             return e;
         CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, 1, 0, s));
     }
+    if (defer && n_steps > 0)
+        if (int e = fill_after_loop(g->dtype, one, nullptr, 1, U, s)) return e;
     return AMHD_OK;
 }
 
@@ -649,6 +671,7 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
     p.ctl = ctl;
     p.use_ctl = 1;
     p.pull_ghosts = 1;
+    p.defer_fill = is_march(tx);  // as amhd_advance: U's ghost cells once, after the last step (timed)
     cudaError_t ce = cudaEventRecord(ev[0], s);
     for (int k = 0; k < n_steps && ce == cudaSuccess; ++k) {
         for (int st = 1; st <= 3 && ce == cudaSuccess; ++st) {
@@ -660,6 +683,8 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
             if (ce == cudaSuccess) ce = cudaEventRecord(ev[4 * k + st], s);
         }
         if (ce == cudaSuccess) ce = run_finalize(g->dtype, nullptr, 1, one, U, ctl, 1, 0, s);
+        if (ce == cudaSuccess && p.defer_fill && k == n_steps - 1)
+            ce = g->dtype == AMHD_F64 ? Launch<double>::march_fill(p, s) : Launch<float>::march_fill(p, s);
         if (ce == cudaSuccess) ce = cudaEventRecord(ev[4 * k + 4], s);
     }
     if (ce == cudaSuccess) ce = cudaEventSynchronize(ev.back());
@@ -825,12 +850,15 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
     gdt.dtype = dtype;
     amhd_instance dummy;
     memset(&dummy, 0, sizeof dummy);
+    const int defer = is_march(tile_x);
     for (int k = 0; k < n_steps; ++k) {
         if (int e = three_stages(&gdt, dummy, inst_dev, tile_inst_dev, n_tiles, tile_x, grid, U, U1, U2, ctl_dev, 1, 0,
-                                 0, 1, 1, s, tile_order_dev, static_cast<const CUtensorMap *>(tmaps_dev), n_inst))
+                                 0, 1, 1, s, tile_order_dev, static_cast<const CUtensorMap *>(tmaps_dev), n_inst, defer))
             return e;
         CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 1, 0, s));
     }
+    if (defer && n_steps > 0)
+        if (int e = fill_after_loop(dtype, dummy, inst_dev, n_inst, U, s)) return e;
     return AMHD_OK;
 }
 

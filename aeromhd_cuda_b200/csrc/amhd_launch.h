@@ -33,6 +33,8 @@ struct StageParams {
     int32_t n_inst;                // instances in inst (ghost fill after a marching stage)
     int32_t pull_ghosts;           // marching kernel: read ghost cells from their interior sources,
                                    // so stages 1 and 2 need no ghost fill of their output
+    int32_t defer_fill;            // with pull_ghosts: stage 3 leaves U's ghost cells too (the run
+                                   // loop fills them once after its last step, Launch::march_fill)
 };
 
 // Work geometry of the stage kernels, passed around as one int "tile_x":
@@ -54,6 +56,8 @@ struct Layout {
 template <typename R>
 struct Launch {
     static cudaError_t stage(int stage, int tile_x, const StageParams &p, int grid, cudaStream_t s);
+    // ghost cells of p.uout for every instance of p, active or not (idempotent)
+    static cudaError_t march_fill(const StageParams &p, cudaStream_t s);
     static size_t stage_smem(int tile_x);
     static cudaError_t configure();
     static int stage_ctas_per_sm(int tile_x);

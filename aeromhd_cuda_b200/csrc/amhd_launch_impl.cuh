@@ -122,8 +122,9 @@ cudaError_t Launch<R>::stage(int stage, int tile_x, const StageParams &p, int gr
         }
         if (e != cudaSuccess) return e;
         // the marching kernel leaves the ghost cells of its output to this pass
-        // (not needed after stages 1 and 2 when the next stage pulls them)
-        if (p.pull_ghosts && stage < 3) return cudaSuccess;
+        // (not needed after stages 1 and 2 when the next stage pulls them, nor
+        // after stage 3 when the loop fills U once after its last step)
+        if (p.pull_ghosts && (stage < 3 || p.defer_fill)) return cudaSuccess;
         const int n_inst = p.inst ? p.n_inst : 1;
         if (n_inst <= 0) return cudaErrorInvalidValue;
         const int per = p.inst ? 8 : elem_blocks(4LL * (p.one.grid.ny + 2 * NG) + 4LL * p.one.grid.nx);
@@ -168,6 +169,18 @@ int Launch<R>::stage_ctas_per_sm(int tile_x)
     case 16: return ctas_per_sm_t<R, 16>();
     default: return 1;
     }
+}
+
+template <typename R>
+cudaError_t Launch<R>::march_fill(const StageParams &p, cudaStream_t s)
+{
+    const int n_inst = p.inst ? p.n_inst : 1;
+    if (n_inst <= 0) return cudaErrorInvalidValue;
+    StageParams q = p;
+    q.use_ctl = 0;  // every instance: one that stopped during the loop still has its last state to fill
+    const int per = p.inst ? 8 : elem_blocks(4LL * (p.one.grid.ny + 2 * NG) + 4LL * p.one.grid.nx);
+    march_bc_fill_kernel<R><<<dim3(per, n_inst), 256, 0, s>>>(q);
+    return cudaGetLastError();
 }
 
 template <typename R>

@@ -80,10 +80,17 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def launches_per_step(tile_x):
-    """Kernels of one run-loop step: 3 stages (+ the ghost fill of stage 3's output with the
-    marching kernel; stages 2 and 3 read their inputs' ghost cells from the interior) + finalize."""
-    return 3 + (1 if tile_x < 0 else 0) + 1
+def loop_launches(tile_x, steps):
+    """Kernels of a run loop of `steps` steps: 3 stages + finalize per step; with the marching
+    kernel every stage reads its input's ghost cells from the interior, and U's ghost cells
+    are filled once after the last step."""
+    return 4 * steps + (1 if tile_x < 0 else 0)
+
+
+def split_launches(tile_x, steps):
+    """Kernels of the row-split loop: each stage fills its output's ghost cells (marching
+    kernel: a separate pass), then finalize."""
+    return (3 * (2 if tile_x < 0 else 1) + 1) * steps
 
 
 def stage_kernel_name(tile_x):
@@ -373,7 +380,7 @@ def run_ours(a, world, rank, local):
                    "parallelism": f"replicas x{world}", "stage_kernel": stage_geometry(tx),
                    "staging": ("cp.async rows" if tx < 0 else
                                "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads")},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step(tx) * a.steps,
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": loop_launches(tx, a.steps),
         "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
     }
     return line
@@ -417,7 +424,7 @@ def run_decomp(a, world, rank):
                    "precision": a.precision, "parallelism": f"x-row split over {world} ranks",
                    "rows_per_rank": d.r1 - d.r0, "stage_kernel": stage_geometry(tx),
                    "l2": "inputs larger than L2 (3 state buffers per rank)"},
-        "gpu_launches": launches_per_step(tx) * a.steps,
+        "gpu_launches": split_launches(tx, a.steps),
         "clocks": clk.summary(),
     }
 
@@ -428,10 +435,16 @@ def run_ensemble(a, world):
     import torch
     from aeromhd_cuda_b200.ensemble import Ensemble, draw_configs
     from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200.autotune import Cache, tune_ensemble
     cfgs = draw_configs(a.ensemble, seed=0, t_end=3.0, precision=a.precision)
     ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=0, use_tma=bool(a.tma))
     ens.initialize()
     ens.start()
+    tuned = None
+    if a.tile_x == 0:
+        # work shape, order and grid chosen by the autotuner (untimed; fresh cache)
+        best, timings = tune_ensemble(ens, steps=5, cache=Cache())
+        tuned = {"candidates": len(timings), "best_ms_per_step": round(min(timings.values()) / 5 * 1e3, 4)}
     k = max(3, a.steps // 2)
     ens.advance(k)  # warm-up + graph capture
     torch.cuda.synchronize()
@@ -447,7 +460,8 @@ def run_ensemble(a, world):
         raise SystemExit("non-finite state in the ensemble benchmark")
     return {"value": world * cells * k / (ms / 1e3), "unit": "zone-updates/s", "instances": a.ensemble,
             "cells": cells, "steps": k, "ms_per_step": ms / k,
-            "schedule": {"tile_x": ens.tile_x, "order": "instance", "grid": "persistent"}}
+            "schedule": {"tile_x": ens.tile_x, "order": ens.order,
+                         "grid": "persistent" if ens.ctas >= 0 else "one CTA per work group", "autotuned": tuned}}
 
 
 def run_reference(a, world, rank):
