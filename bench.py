@@ -305,9 +305,15 @@ def run_ours(a, world, rank, local):
             traffic = float(tr["dram_bytes_per_step"]) * (cells / float(tr["n"]) ** 2)
         except (KeyError, ValueError):
             traffic = None
+    limiter = None
+    if tr.get("precision") == a.precision and "issue_active_pct" in tr:
+        # the committed ncu capture's view of what bounds the kernel (stage 2)
+        limiter = {k: float(tr[k]) for k in ("issue_active_pct", "fma_pipe_pct", "alu_pipe_pct", "xu_pipe_pct",
+                                             "lsu_pipe_pct", "dram_throughput_pct") if k in tr}
+        limiter["source"] = "profiles/" + stage_kernel_name(tx) + "_traffic.txt (ncu, stage 2)"
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
                 "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": hbm_kind,
-                "kernel": stage_kernel_name(tx) + " (3 launches/step)",
+                "kernel": stage_kernel_name(tx) + " (3 launches/step)", "sm_utilisation": limiter,
                 "algorithmic_bytes_per_step": alg_bytes_step,
                 "ms_per_step": {"stage1": prof[0] / a.steps, "stage2": prof[1] / a.steps,
                                 "stage3_fused_dt": prof[2] / a.steps, "finalize": prof[3] / a.steps}}
