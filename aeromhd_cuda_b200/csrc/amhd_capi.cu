@@ -143,11 +143,11 @@ cudaError_t run_bc_fill(const amhd_grid *g, void *U, cudaStream_t s)
 }
 
 cudaError_t run_finalize(int dtype, const amhd_instance *insts, int n, const amhd_instance &one, const void *U,
-                         amhd_control *ctl, int advance, int set_only, cudaStream_t s)
+                         amhd_control *ctl, int advance, int set_only, cudaStream_t s, int pdl = 0)
 {
     return dtype == AMHD_F64
-               ? Launch<double>::finalize(insts, n, one, static_cast<const double *>(U), ctl, advance, set_only, s)
-               : Launch<float>::finalize(insts, n, one, static_cast<const float *>(U), ctl, advance, set_only, s);
+               ? Launch<double>::finalize(insts, n, one, static_cast<const double *>(U), ctl, advance, set_only, s, pdl)
+               : Launch<float>::finalize(insts, n, one, static_cast<const float *>(U), ctl, advance, set_only, s, pdl);
 }
 
 cudaError_t run_dt_reduce(const amhd_grid *g, const void *A, int from_prim, amhd_control *ctl, cudaStream_t s)
@@ -173,6 +173,7 @@ int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instan
     p.n_inst = n_inst;
     p.pull_ghosts = 1;  // the run loop: U1 and U2 are internal, their ghost cells are never stored
     p.defer_fill = defer_fill;
+    p.pdl = defer_fill;  // the marching run loop: each launch overlaps the previous one's tail
     p.one = one;
     p.tile_inst = tile_inst;
     p.tile_order = tile_order;
@@ -594,7 +595,7 @@ int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *
         if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, grid, U, U1, U2, ctl, 1, 0, 0, 1, 1, s,
                                  nullptr, nullptr, 1, defer))
             return e;
-        CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, 1, 0, s));
+        CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, 1, 0, s, defer));
     }
     if (defer && n_steps > 0)
         if (int e = fill_after_loop(g->dtype, one, nullptr, 1, U, s)) return e;
@@ -855,7 +856,7 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
         if (int e = three_stages(&gdt, dummy, inst_dev, tile_inst_dev, n_tiles, tile_x, grid, U, U1, U2, ctl_dev, 1, 0,
                                  0, 1, 1, s, tile_order_dev, static_cast<const CUtensorMap *>(tmaps_dev), n_inst, defer))
             return e;
-        CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 1, 0, s));
+        CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 1, 0, s, defer));
     }
     if (defer && n_steps > 0)
         if (int e = fill_after_loop(dtype, dummy, inst_dev, n_inst, U, s)) return e;

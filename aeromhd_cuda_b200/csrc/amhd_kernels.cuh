@@ -61,6 +61,14 @@ struct TileSmem {
     int tma_ok;
 };
 
+// Programmatic dependent launch (sm_90 and later): pdl_trigger lets the next
+// kernel of the stream be scheduled onto SMs this grid frees, pdl_wait blocks
+// until the previous kernel has completed and its writes are visible.  For a
+// kernel launched without the programmatic-serialization attribute both have
+// nothing to do (stream order already holds).
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ const amhd_instance &inst_of(const StageParams &p, int tile, int &inst_idx)
 {
     if (p.inst != nullptr) {
@@ -900,6 +908,10 @@ __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) ma
     const __grid_constant__ StageParams p)
 {
     extern __shared__ __align__(16) unsigned char march_smem[];
+    // run loop: the next launch may take SM slots as this grid drains; nothing
+    // of the previous launch (stage input, controls) is read before it is done
+    pdl_trigger();
+    pdl_wait();
     MarchSmem<R> &ms = reinterpret_cast<MarchSmem<R> *>(march_smem)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
@@ -1231,6 +1243,8 @@ template <typename R>
 __global__ void finalize_kernel(const amhd_instance *insts, const amhd_instance one, const R *Ubase,
                                 amhd_control *ctls, int advance, int set_only)
 {
+    pdl_trigger();
+    pdl_wait();  // the reduced maxima of the stage before
     const amhd_instance &in = insts ? insts[blockIdx.x] : one;
     const amhd_grid &g = in.grid;
     amhd_control *ctl = ctls + blockIdx.x;

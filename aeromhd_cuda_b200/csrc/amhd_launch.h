@@ -35,6 +35,8 @@ struct StageParams {
                                    // so stages 1 and 2 need no ghost fill of their output
     int32_t defer_fill;            // with pull_ghosts: stage 3 leaves U's ghost cells too (the run
                                    // loop fills them once after its last step, Launch::march_fill)
+    int32_t pdl;                   // marching kernel: launch as a programmatic dependent of the
+                                   // previous kernel in the stream (run loop)
 };
 
 // Work geometry of the stage kernels, passed around as one int "tile_x":
@@ -73,8 +75,9 @@ struct Launch {
     static cudaError_t powell(const Layout &l, const R *W, R *S, double dx, double dy, cudaStream_t s);
     static cudaError_t dt_reduce(const Layout &l, const R *A, int from_prim, double gamma, amhd_control *ctl,
                                  cudaStream_t s);
+    // pdl: launch as a programmatic dependent of the previous kernel (run loop)
     static cudaError_t finalize(const amhd_instance *insts, int n_inst, const amhd_instance &one, const R *U,
-                                amhd_control *ctl, int advance, int set_only, cudaStream_t s);
+                                amhd_control *ctl, int advance, int set_only, cudaStream_t s, int pdl = 0);
     static cudaError_t diag_rows(const amhd_grid &g, const R *U, double *rows, cudaStream_t s);
     static cudaError_t diag_colour(const amhd_grid &g, const R *U, double x0, const double *csum, double *cp2,
                                    double *pos, cudaStream_t s);

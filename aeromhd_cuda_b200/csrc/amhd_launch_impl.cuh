@@ -1,6 +1,9 @@
 // amhd_launch_impl.cuh -- definitions of Launch<R>; included once per
 // precision translation unit, which then instantiates Launch<R>.
 #pragma once
+#include <cstring>
+#include <utility>
+
 #include "amhd_kernels.cuh"
 
 namespace amhd {
@@ -87,6 +90,27 @@ static cudaError_t launch_stage_tx(int stage, const StageParams &p, int grid, cu
     }
 }
 
+// a launch that may start while the previous kernel of the stream drains
+// (programmatic dependent launch; the kernel waits in pdl_wait before it reads
+// anything the previous one wrote)
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                    Args &&...args)
+{
+    cudaLaunchConfig_t cfg;
+    memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <typename R, int ST>
 static cudaError_t launch_march_t(const StageParams &p, int grid, cudaStream_t s)
 {
@@ -97,6 +121,7 @@ static cudaError_t launch_march_t(const StageParams &p, int grid, cudaStream_t s
         if (e != cudaSuccess) return e;
         configured = true;
     }
+    if (p.pdl) return launch_dependent(march_stage_kernel<R, ST>, dim3(grid), dim3(kMarchThreads), kMarchSmem<R>, s, p);
     march_stage_kernel<R, ST><<<grid, kMarchThreads, kMarchSmem<R>, s>>>(p);
     return cudaGetLastError();
 }
@@ -247,8 +272,9 @@ cudaError_t Launch<R>::dt_reduce(const Layout &l, const R *A, int from_prim, dou
 
 template <typename R>
 cudaError_t Launch<R>::finalize(const amhd_instance *insts, int n_inst, const amhd_instance &one, const R *U,
-                                amhd_control *ctl, int advance, int set_only, cudaStream_t s)
+                                amhd_control *ctl, int advance, int set_only, cudaStream_t s, int pdl)
 {
+    if (pdl) return launch_dependent(finalize_kernel<R>, dim3(n_inst), dim3(256), 0, s, insts, one, U, ctl, advance, set_only);
     finalize_kernel<R><<<n_inst, 256, 0, s>>>(insts, one, U, ctl, advance, set_only);
     return cudaGetLastError();
 }

@@ -44,7 +44,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
@@ -274,20 +274,36 @@ def run_ours(a, world, rank, local):
     ms = (ctypes.c_double * 5)()
 
     def advance_profiled(k):
+        """k steps with an event after every launch: the per-stage kernel times"""
         _lib.call("amhd_advance_profile", g, _tensors.ptr(s._U), _tensors.ptr(s._U1), _tensors.ptr(s._U2),
                   _tensors.ptr(s._ctl), int(k), ms, stream)
         return [ms[i] for i in range(5)]
 
+    def advance(k):
+        """k steps of the run loop the solver runs (amhd_advance: each launch a programmatic
+        dependent of the one before), timed with events on the launching stream"""
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.call("amhd_advance", g, _tensors.ptr(s._U), _tensors.ptr(s._U1), _tensors.ptr(s._U2),
+                  _tensors.ptr(s._ctl), int(k), stream)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
     if a.warmup > 0:
-        advance_profiled(a.warmup)
+        advance(a.warmup)
+        advance_profiled(min(a.warmup, 3))
     torch.cuda.synchronize()
     barrier(world)
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clk:
-        prof = advance_profiled(a.steps)
-        torch.cuda.synchronize()
+        loop_ms = advance(a.steps)
     barrier(world)
-    total_ms = max_over_ranks(prof[4], world)
+    total_ms = max_over_ranks(loop_ms, world)
+    # up to 200 more steps with an event after every launch, for the stage times
+    prof_steps = max(1, min(a.steps, 200))
+    prof = advance_profiled(prof_steps)
+    torch.cuda.synchronize()
     c = _tensors.read_controls(s._ctl)[0]
     if c.flags & _lib.AMHD_FLAG_NONFINITE:
         raise SystemExit("non-finite state during the benchmark")
@@ -297,7 +313,7 @@ def run_ours(a, world, rank, local):
     hbm, hbm_kind = peaks()
     stage_ms = prof[0] + prof[1] + prof[2]
     alg_bytes_step = 80 * es * cells
-    achieved = alg_bytes_step * a.steps / (stage_ms / 1e3) / 1e9
+    achieved = alg_bytes_step * prof_steps / (stage_ms / 1e3) / 1e9
     tr = profile_traffic(tx)
     traffic = None
     if tr.get("precision") == a.precision and tr.get("n"):
@@ -315,8 +331,9 @@ def run_ours(a, world, rank, local):
                 "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": hbm_kind,
                 "kernel": stage_kernel_name(tx) + " (3 launches/step)", "sm_utilisation": limiter,
                 "algorithmic_bytes_per_step": alg_bytes_step,
-                "ms_per_step": {"stage1": prof[0] / a.steps, "stage2": prof[1] / a.steps,
-                                "stage3_fused_dt": prof[2] / a.steps, "finalize": prof[3] / a.steps}}
+                "ms_per_step": {"stage1": prof[0] / prof_steps, "stage2": prof[1] / prof_steps,
+                                "stage3_fused_dt": prof[2] / prof_steps, "finalize": prof[3] / prof_steps},
+                "stage_times": f"{prof_steps} steps with an event after every launch (no launch overlap)"}
 
     # ---- end to end: host state in pinned memory, one C-ABI call per step
     e2e = None
@@ -357,13 +374,19 @@ def run_ours(a, world, rank, local):
         s64._loop_init(1e30, 1 << 60)
         g64 = s64._grid()
         k64 = max(3, a.steps // 2)
-        _lib.call("amhd_advance_profile", g64, _tensors.ptr(s64._U), _tensors.ptr(s64._U1), _tensors.ptr(s64._U2),
-                  _tensors.ptr(s64._ctl), 2, ms, stream)
-        _lib.call("amhd_advance_profile", g64, _tensors.ptr(s64._U), _tensors.ptr(s64._U1), _tensors.ptr(s64._U2),
-                  _tensors.ptr(s64._ctl), k64, ms, stream)
-        t64 = max_over_ranks(ms[4], world)
+        p64 = (g64, _tensors.ptr(s64._U), _tensors.ptr(s64._U1), _tensors.ptr(s64._U2), _tensors.ptr(s64._ctl))
+        _lib.call("amhd_advance", *p64, 2, stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.call("amhd_advance", *p64, k64, stream)
+        e1.record()
+        torch.cuda.synchronize()
+        t64 = max_over_ranks(e0.elapsed_time(e1), world)
+        k64p = max(3, min(k64, 50))
+        _lib.call("amhd_advance_profile", *p64, k64p, ms, stream)
         fp64 = {"value": world * cells * k64 / (t64 / 1e3), "steps": k64,
-                "stage_hbm_frac": round(80 * 8 * cells * k64 / ((ms[0] + ms[1] + ms[2]) / 1e3) / 1e9 / hbm, 4)}
+                "stage_hbm_frac": round(80 * 8 * cells * k64p / ((ms[0] + ms[1] + ms[2]) / 1e3) / 1e9 / hbm, 4)}
         del s64
 
     ens_line = None
