@@ -138,13 +138,26 @@ class Normaliser:
         return t.transpose(0, 1).reshape(10, -1).contiguous()
 
 
+def project_rows(T: torch.Tensor) -> torch.Tensor:
+    """The mean over y (the last axis) of every x-row, broadcast back: the part of
+    a correction that moves the row averages -- the mixing width and the other
+    integral diagnostics are functions of those -- without the small-scale part
+    in which the coarse and fine runs of a chaotic layer decorrelate."""
+    return T.mean(dim=-1, keepdim=True).expand_as(T)
+
+
 def train(X: torch.Tensor, Y: torch.Tensor, train_seeds: Sequence[int], val_seeds: Sequence[int], epochs: int = 20,
           batch: int = 16, lr: float = 1e-3, seed: int = 0, net: Corrector | None = None,
-          norm: "Normaliser | None" = None, log=print):
+          norm: "Normaliser | None" = None, project_y: bool = False, log=print):
     """X, Y: [snap][seed][10][H][W]; seeds index the second axis.  Returns (net, norm, history).
-    Given net and norm, continues training that network with its normalisation."""
+    Given net and norm, continues training that network with its normalisation.
+    project_y: the targets are the row averages of the corrections (project_rows),
+    and so are the corrections the network applies (net.project_y)."""
     H, W = X.shape[-2], X.shape[-1]
+    project_y = project_y or bool(getattr(net, "project_y", False))
     T = Y - X
+    if project_y:
+        T = project_rows(T)
     tr = X[:, list(train_seeds)].reshape(-1, 10, H, W)
     ttr = T[:, list(train_seeds)].reshape(-1, 10, H, W)
     va = X[:, list(val_seeds)].reshape(-1, 10, H, W)
@@ -153,6 +166,7 @@ def train(X: torch.Tensor, Y: torch.Tensor, train_seeds: Sequence[int], val_seed
         norm = Normaliser(tr, ttr)
         net = Corrector(H, W, seed=seed, device=X.device)
         net.set_normalisation(norm.in_mean, norm.in_std, norm.out_scale)
+        net.project_y = bool(project_y)
     gen = torch.Generator(device="cpu").manual_seed(seed)
     hist = {"epoch": [], "train_loss": [], "val_loss": [], "wall_s": []}
     n = tr.shape[0]
@@ -430,6 +444,8 @@ def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma:
         _lib.call("amhd_nn_pack", e._grid(i), ptr(e.state(i)), ptr(net.in_mean), ptr(net.in_istd), ptr(x), B * N,
                   int(b), stream_ptr())
     y = net.forward(x, B)
+    if getattr(net, "project_y", False):
+        y = project_rows(y.view(10, B, net.H, net.W)).reshape(10, B * N).contiguous()
     lim = (norm.out_max * corr_sigma).view(10, 1, 1)
     yb = y.view(10, B, N)
     good = (torch.isfinite(yb).all(dim=2).all(dim=0) & (yb.abs() <= lim).all(dim=2).all(dim=0)).cpu().numpy()
@@ -445,7 +461,7 @@ def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma:
 
 def save(path: str, net: Corrector, norm: Normaliser) -> None:
     """Weights and normalisation of a trained corrector (torch.save)."""
-    torch.save({"params": net.host_params(), "H": net.H, "W": net.W,
+    torch.save({"params": net.host_params(), "H": net.H, "W": net.W, "project_y": bool(getattr(net, "project_y", 0)),
                 "norm": {k: getattr(norm, k).detach().cpu() for k in ("in_mean", "in_std", "out_std", "active",
                                                                        "out_max")}}, path)
 
@@ -458,6 +474,7 @@ def load(path: str, device="cuda"):
         setattr(norm, k, v.to(device))
     net = Corrector(int(d["H"]), int(d["W"]), params=d["params"], device=device)
     net.set_normalisation(norm.in_mean, norm.in_std, norm.out_scale)
+    net.project_y = bool(d.get("project_y", False))
     return net, norm
 
 
@@ -478,6 +495,8 @@ def main(argv=None) -> int:
                     help="rounds of training on pairs from the corrector's own runs")
     ap.add_argument("--dagger-epochs", type=int, default=20)
     ap.add_argument("--dagger-mode", type=int, default=3, help="correction mode of those runs")
+    ap.add_argument("--project-y", action="store_true",
+                    help="train on and apply the row averages of the corrections (project_rows)")
     ap.add_argument("--save", default=None)
     a = ap.parse_args(argv)
     log = lambda m: print(m, file=sys.stderr, flush=True)
@@ -492,7 +511,7 @@ def main(argv=None) -> int:
         n_pairs = int(X.shape[0] * X.shape[1])
         log("training ...")
         net, norm, hist = train(X, Y, range(n_val, a.train_seeds), range(n_val), epochs=a.epochs, batch=a.batch,
-                                lr=a.lr, log=log)
+                                lr=a.lr, project_y=a.project_y, log=log)
         for r in range(a.dagger_rounds):
             log(f"rollout round {r + 1}: pairs from corrected runs ...")
             X2, Y2 = rollout_pairs(net, norm, seeds, delta=a.delta, scalar_mode=a.dagger_mode, nyc=a.nyc, log=log)
