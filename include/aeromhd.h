@@ -197,7 +197,11 @@ int amhd_control_resume(amhd_control *ctl, int32_t n, double snap_t, void *strea
  * last stage, then t += dt, step += 1, boundary-energy bookkeeping and the
  * next dt.  Iterations after the stop condition (t >= t_end, step >=
  * max_steps, dt <= 1e-16) do nothing.  No host synchronisation; capturable
- * in a CUDA graph. */
+ * in a CUDA graph.  With the marching kernel every stage reads the ghost
+ * cells of its input from the interior cells they copy, and U's ghost cells
+ * are filled once, after the last iteration (every stream-ordered reader of
+ * U sees a complete state); the launches of the loop are programmatic
+ * dependents of one another (each waits for the one before on the device). */
 int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps,
                  void *stream);
 /* The run loop taken apart, for drivers that act between its pieces (a grid
