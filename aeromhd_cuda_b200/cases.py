@@ -4,6 +4,8 @@
     python -m aeromhd_cuda_b200.cases cp_alfven --sizes 32 64 128 256 512 1024
     python -m aeromhd_cuda_b200.cases shock_interface --nx 2048 --ny 512 --t-end 3
     python -m aeromhd_cuda_b200.cases brio_wu
+    python -m aeromhd_cuda_b200.cases reference_rmi        # main.py:446-474
+    python -m aeromhd_cuda_b200.cases rmi_convergence      # main.py:294-396, :476-492
 
 Each prints one JSON object (wall time, steps, zone-updates/s and the case's
 accuracy figures).  Errors of the float32 path are measured against a float64
@@ -167,9 +169,89 @@ def brio_wu(nx: int = 800, precision: str = "fp64", cfl: float = 0.3, limiter: s
             "passed": all(checks.values())}
 
 
+# The reference drivers' shocked-interface set-up (main.py:446-458): Mach 10,
+# density ratio 3, mode-4 perturbation, characteristic x boundaries, Powell on.
+REFERENCE_RMI = dict(nx=400, ny=200, x_min=0.0, x_max=6.0, y_min=0.0, y_max=2.0, t_end=0.25, cfl=0.30, mach=10.0,
+                     interface_x=1.5, perturbation_amp=0.15, perturbation_mode=4, density_ratio=3.0,
+                     interface_width=2.0, powell_source=True, use_char_bc=True, bc_x_type="characteristic",
+                     bc_y_type="periodic", enable_smoothing=False, diag_interval=20,
+                     snapshot_times=[0.0, 0.05, 0.10, 0.15, 0.20, 0.25])
+REFERENCE_RMI_CASES = {"Hydro (B=0)": 0.0, "MHD (By=0.5)": 0.5, "MHD (By=1.5)": 1.5}   # main.py:460-464
+
+
+def _peak_after(s: MHDSolver, values, t_skip: float = 0.03) -> float:
+    """Peak of a diagnostic history after t_skip (main.py:329-336)."""
+    t = np.asarray(s.diag_times)
+    v = np.asarray(values)[t > t_skip]
+    return float(v.max()) if len(v) else 0.0
+
+
+def reference_rmi_cases(precision: str = "fp64", t_end: float = 0.25) -> dict:
+    """The three shocked-interface runs of the reference drivers (main.py:466-474)
+    with their diagnostic summary (main.py:500-520: peaks after t = 0.03)."""
+    out = {"case": "reference_rmi", "precision": precision, "runs": {}}
+    for label, by in REFERENCE_RMI_CASES.items():
+        cfg = Config(**{**REFERENCE_RMI, "t_end": t_end, "B_transverse": by, "precision": precision})
+        s = MHDSolver(cfg)
+        s.initialize()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.run()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        out["runs"][label] = {"steps": s.step, "t": s.t, "wall_s": wall,
+                              "mw_integral_peak": _peak_after(s, s.diag_mixing_width_integral),
+                              "mw_thresh_peak": _peak_after(s, s.diag_mixing_width_thresh),
+                              "mixedness_peak": _peak_after(s, s.diag_mixedness),
+                              "enstrophy_local_peak": _peak_after(s, s.diag_enstrophy_local),
+                              "divB_L2_final": float(s.diag_divB_L2[-1])}
+    return out
+
+
+def convergence_config(nx: int, ny: int, by: float, precision: str = "fp64") -> Config:
+    """One resolution of the reference's grid-convergence study (main.py:476-492,
+    :306-312): the driver set-up to t = 0.15, diagnostics every max(10, 4000 / nx) steps."""
+    return Config(**{**REFERENCE_RMI, "t_end": 0.15, "snapshot_times": [0.0, 0.15], "nx": nx, "ny": ny,
+                     "B_transverse": by, "diag_interval": max(10, 20 * 200 // nx), "precision": precision})
+
+
+def rmi_convergence(by: float, resolutions=((100, 50), (200, 100), (400, 200)), precision: str = "fp64") -> dict:
+    """run_convergence_study, main.py:294-396: peak integral / threshold mixing
+    width and local enstrophy per resolution, and the convergence order of the
+    integral mixing width from three successive resolutions (main.py:346-356)."""
+    rows, dxs, mwi = [], [], []
+    for nx, ny in resolutions:
+        cfg = convergence_config(nx, ny, by, precision)
+        s = MHDSolver(cfg)
+        s.initialize()
+        wall = _timed_advance_run(s)
+        rows.append({"nx": nx, "ny": ny, "dx": cfg.dx, "steps": s.step, "wall_s": wall,
+                     "mw_integral_peak": _peak_after(s, s.diag_mixing_width_integral),
+                     "mw_thresh_peak": _peak_after(s, s.diag_mixing_width_thresh),
+                     "enstrophy_local_peak": _peak_after(s, s.diag_enstrophy_local)})
+        dxs.append(cfg.dx)
+        mwi.append(rows[-1]["mw_integral_peak"])
+    orders = []
+    for i in range(2, len(mwi)):
+        d, dp = abs(mwi[i] - mwi[i - 1]), abs(mwi[i - 1] - mwi[i - 2])
+        if mwi[i] > 0 and mwi[i - 1] > 0 and d > 1e-14 and dp > 1e-14:
+            orders.append(float(np.log(dp / d) / np.log(dxs[i - 1] / dxs[i])))
+    return {"case": "rmi_convergence", "By": by, "precision": precision, "resolutions": rows,
+            "mw_integral_order": orders}
+
+
+def _timed_advance_run(s: MHDSolver) -> float:
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.run()
+    torch.cuda.synchronize()
+    return time.perf_counter() - t0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["orszag_tang", "cp_alfven", "shock_interface", "brio_wu"])
+    ap.add_argument("case", choices=["orszag_tang", "cp_alfven", "shock_interface", "brio_wu", "reference_rmi",
+                                     "rmi_convergence"])
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--ny", type=int, default=512)
@@ -186,6 +268,10 @@ def main(argv=None) -> int:
         r = {p: cp_alfven(tuple(a.sizes), p) for p in precs}
     elif a.case == "shock_interface":
         r = shock_interface(a.nx, a.ny, a.t_end or 3.0, precs)
+    elif a.case == "reference_rmi":
+        r = {p: reference_rmi_cases(p, a.t_end or 0.25) for p in precs}
+    elif a.case == "rmi_convergence":
+        r = {p: [rmi_convergence(by, precision=p) for by in (0.0, 1.5)] for p in precs}
     else:
         r = {p: brio_wu(precision=p, cfl=a.cfl or 0.3, limiter=a.limiter) for p in precs}
     print(json.dumps(r))
