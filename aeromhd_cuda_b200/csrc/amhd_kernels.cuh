@@ -750,10 +750,12 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
             // physics.py:376-379); the right face is the next lane's left face
             R wl[NV], wr[NV], f[NV];
             if constexpr (kFast<R>) {
+                R ll[NV];  // states on each variable's left face, from the lane on the left
 #pragma unroll
-                for (int k = 0; k < NV; k += 2) {
-                    const int v0 = rot[k], v1 = rot[k + 1];
-                    const float2 c = make_float2(w0[v0], w0[v1]);
+                for (int v = 0; v < NV; v += 2) {
+                    // pairs in the stored slot order (as the x-slopes pair them);
+                    // the rotation to the y-face order is a renaming below
+                    const float2 c = make_float2(w0[v], w0[v + 1]);
                     const float2 m = make_float2(__shfl_up_sync(0xffffffffu, c.x, 1),
                                                  __shfl_up_sync(0xffffffffu, c.y, 1));
                     const float2 q = make_float2(__shfl_down_sync(0xffffffffu, c.x, 1),
@@ -761,18 +763,19 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
                     const float2 sy = fast::slope2(m, c, q, lim);
                     const float2 r = __ffma2_rn(make_float2(-0.5f, -0.5f), sy, c);
                     const float2 l = __ffma2_rn(make_float2(0.5f, 0.5f), sy, c);
-                    wr[k] = r.x;
-                    wr[k + 1] = r.y;
-                    wl[k] = __shfl_up_sync(0xffffffffu, l.x, 1);
-                    wl[k + 1] = __shfl_up_sync(0xffffffffu, l.y, 1);
-                    if (v0 == BY) {
-                        bym = m.x;
-                        byp = q.x;
-                    }
-                    if (v1 == BY) {
+                    f[v] = r.x;
+                    f[v + 1] = r.y;
+                    ll[v] = __shfl_up_sync(0xffffffffu, l.x, 1);
+                    ll[v + 1] = __shfl_up_sync(0xffffffffu, l.y, 1);
+                    if (v + 1 == BY) {
                         bym = m.y;
                         byp = q.y;
                     }
+                }
+#pragma unroll
+                for (int k = 0; k < NV; ++k) {
+                    wr[k] = f[rot[k]];
+                    wl[k] = ll[rot[k]];
                 }
             } else {
 #pragma unroll
