@@ -836,8 +836,14 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
 #pragma unroll
             for (int k = 0; k < NV / 2; ++k) {
                 const typename Pair<R>::T o = pair_load(ms.fx, k, lane);
-                dfx[2 * k] = f[2 * k] - o.x;
-                dfx[2 * k + 1] = f[2 * k + 1] - o.y;
+                if constexpr (kFast<R>) {
+                    const float2 d = __ffma2_rn(o, make_float2(-1.f, -1.f), make_float2(f[2 * k], f[2 * k + 1]));
+                    dfx[2 * k] = d.x;
+                    dfx[2 * k + 1] = d.y;
+                } else {
+                    dfx[2 * k] = f[2 * k] - o.x;
+                    dfx[2 * k + 1] = f[2 * k + 1] - o.y;
+                }
                 pair_store(ms.fx, k, lane, f[2 * k], f[2 * k + 1]);
             }
         }
@@ -848,8 +854,14 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
 #pragma unroll
                 for (int k = 0; k < NV / 2; ++k) {  // output lanes stop at 29
                     const typename Pair<R>::T a = pair_load(ms.fy, k, lane + 1), b = pair_load(ms.fy, k, lane);
-                    dfy[2 * k] = a.x - b.x;
-                    dfy[2 * k + 1] = a.y - b.y;
+                    if constexpr (kFast<R>) {
+                        const float2 d = __ffma2_rn(b, make_float2(-1.f, -1.f), a);  // a - b, one rounding
+                        dfy[2 * k] = d.x;
+                        dfy[2 * k + 1] = d.y;
+                    } else {
+                        dfy[2 * k] = a.x - b.x;
+                        dfy[2 * k + 1] = a.y - b.y;
+                    }
                 }
                 auto pw = [&]() {
                     return PowellIn<R>{w0[BX], bxm, w1[BX], w0[BY], bym, byp, w0[IVX], w0[IVY], w0[IVZ], w0[BZ]};
