@@ -48,7 +48,8 @@ __device__ __forceinline__ float slope(float wm, float w0, float wp, int limiter
     const float dm = w0 - wm, dp = wp - w0;
     const float ab = dm * dp;
     if (limiter == AMHD_LIMITER_MINMOD) return (ab > 0.f) ? (fabsf(dm) < fabsf(dp) ? dm : dp) : 0.f;
-    return (ab > 0.f) ? 2.f * ab * rcp(dm + dp + 1e-30f) : 0.f;
+    // 2ab / den as ab / (den / 2): halving is exact, so is the factor 2 it saves
+    return (ab > 0.f) ? ab * rcp(fmaf(0.5f, dm + dp, 0.5e-30f)) : 0.f;
 }
 
 // the same for two independent values at once, on the packed float32x2 path of
@@ -61,8 +62,9 @@ __device__ __forceinline__ float2 slope2(float2 wm, float2 w0, float2 wp, int li
     if (limiter == AMHD_LIMITER_MINMOD)
         return make_float2((ab.x > 0.f) ? (fabsf(dm.x) < fabsf(dp.x) ? dm.x : dp.x) : 0.f,
                            (ab.y > 0.f) ? (fabsf(dm.y) < fabsf(dp.y) ? dm.y : dp.y) : 0.f);
-    const float2 den = __fadd2_rn(__fadd2_rn(dm, dp), make_float2(1e-30f, 1e-30f));
-    const float2 q = __fmul2_rn(__fmul2_rn(make_float2(2.f, 2.f), ab), make_float2(rcp(den.x), rcp(den.y)));
+    // 2ab / den as ab / (den / 2): halving is exact, so is the factor 2 it saves
+    const float2 hden = __ffma2_rn(make_float2(0.5f, 0.5f), __fadd2_rn(dm, dp), make_float2(0.5e-30f, 0.5e-30f));
+    const float2 q = __fmul2_rn(ab, make_float2(rcp(hden.x), rcp(hden.y)));
     return make_float2(ab.x > 0.f ? q.x : 0.f, ab.y > 0.f ? q.y : 0.f);
 }
 
@@ -124,11 +126,12 @@ __device__ __forceinline__ void load_side(FSide &s, const float w[NV], float bxf
     s.pt = s.p + 0.5f * s.bm2;
 }
 
-__device__ __forceinline__ float fast_speed(const FSide &s, float gamma, float bx2)
+// bx2_4 = 4 Bx^2 of the face, shared by both sides
+__device__ __forceinline__ float fast_speed(const FSide &s, float gamma, float bx2_4)
 {
     const float a2 = gamma * s.p * s.ir;
     const float tmp = a2 + s.bm2 * s.ir;
-    const float disc = fmaxf(tmp * tmp - 4.f * a2 * bx2 * s.ir, 0.f);
+    const float disc = fmaxf(tmp * tmp - a2 * bx2_4 * s.ir, 0.f);
     return sqrt_(fmaxf(0.5f * (tmp + sqrt_(disc)), 0.f));
 }
 
@@ -200,7 +203,8 @@ __device__ __forceinline__ void hlld(const float wl[NV], const float wr[NV], flo
     FSide L, R;
     load_side(L, wl, bx2);
     load_side(R, wr, bx2);
-    const float cfL = fast_speed(L, gamma, bx2), cfR = fast_speed(R, gamma, bx2);
+    const float bx2_4 = 4.f * bx2;
+    const float cfL = fast_speed(L, gamma, bx2_4), cfR = fast_speed(R, gamma, bx2_4);
     float SL = fminf(L.vx - cfL, R.vx - cfR);
     float SR = fmaxf(L.vx + cfL, R.vx + cfR);
     if (glm) {
