@@ -411,6 +411,11 @@ def run_ours(a, world, rank, local):
                                "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads")},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": loop_launches(tx, a.steps),
         "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
+        # the metric's "learned vs plain" half: not timed here (training takes minutes)
+        "learned": {"timed": False, "corrector": "python -m aeromhd_cuda_b200.learned",
+                    "status": "not used by default: corrected 256x64 runs are 7-17x faster than the "
+                              "1024x256 solve but their mixing-width error (0.27-0.47 mean) is not "
+                              "below the plain coarse run's (0.28), so the plain solve stands"},
     }
     return line
 
