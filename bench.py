@@ -121,7 +121,7 @@ def profile_traffic(tile_x):
 class ClockSampler:
     """NVML clock / throttle-reason sampling during the timed region (read only)."""
 
-    def __init__(self, device_index: int, period_s: float = 0.01):
+    def __init__(self, device_index: int, period_s: float = 0.002):
         self.samples = []
         self.period = period_s
         self._stop = threading.Event()
