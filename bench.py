@@ -471,7 +471,7 @@ def run_ensemble(a, world):
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200.autotune import Cache, tune_ensemble
     cfgs = draw_configs(a.ensemble, seed=0, t_end=3.0, precision=a.precision)
-    ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=0, use_tma=bool(a.tma))
+    ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=-1, use_tma=bool(a.tma))
     ens.initialize()
     ens.start()
     tuned = None
