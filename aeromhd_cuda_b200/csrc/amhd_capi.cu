@@ -719,9 +719,15 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
     const int nxt = g->nx + 2 * kNG, nyt = g->ny + 2 * kNG;
     char *h = static_cast<char *>(U_host);
     char *d = static_cast<char *>(dev_U);
-    for (int v = 0; v < 10; ++v)
-        CK(cudaMemcpy2DAsync(d + (size_t)v * g->var_stride * es, (size_t)g->pitch * es, h + (size_t)v * nxt * nyt * es,
-                             (size_t)nyt * es, (size_t)nyt * es, nxt, cudaMemcpyHostToDevice, s));
+    // the device planes are the host array itself when no row or plane is padded
+    const bool contiguous = g->pitch == nyt && g->var_stride == (int64_t)nxt * nyt;
+    if (contiguous)
+        CK(cudaMemcpyAsync(d, h, (size_t)10 * nxt * nyt * es, cudaMemcpyHostToDevice, s));
+    else
+        for (int v = 0; v < 10; ++v)
+            CK(cudaMemcpy2DAsync(d + (size_t)v * g->var_stride * es, (size_t)g->pitch * es,
+                                 h + (size_t)v * nxt * nyt * es, (size_t)nyt * es, (size_t)nyt * es, nxt,
+                                 cudaMemcpyHostToDevice, s));
     // dt of this step from the uploaded state, ghosts as given (solver.py:476-479)
     if (int e = control_upload(ctl, t, t_end, 0, 1, s)) return e;
     CK(run_dt_reduce(g, dev_U, 0, ctl, s));
@@ -734,9 +740,12 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
                              dev_U, dev_U1, dev_U2, ctl, 1, 0, 0, 1, 0, s))
         return e;
     CK(run_finalize(g->dtype, nullptr, 1, one, dev_U, ctl, 1, 0, s));
-    for (int v = 0; v < 10; ++v)
-        CK(cudaMemcpy2DAsync(h + (size_t)v * nxt * nyt * es, (size_t)nyt * es, d + (size_t)v * g->var_stride * es,
-                             (size_t)g->pitch * es, (size_t)nyt * es, nxt, cudaMemcpyDeviceToHost, s));
+    if (contiguous)
+        CK(cudaMemcpyAsync(h, d, (size_t)10 * nxt * nyt * es, cudaMemcpyDeviceToHost, s));
+    else
+        for (int v = 0; v < 10; ++v)
+            CK(cudaMemcpy2DAsync(h + (size_t)v * nxt * nyt * es, (size_t)nyt * es, d + (size_t)v * g->var_stride * es,
+                                 (size_t)g->pitch * es, (size_t)nyt * es, nxt, cudaMemcpyDeviceToHost, s));
     amhd_control r;
     CK(cudaMemcpyAsync(&r, ctl, sizeof r, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

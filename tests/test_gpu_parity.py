@@ -296,12 +296,13 @@ def test_fp32_vs_fp64_oracle(amhd):
     assert max(errs.values()) < 1e-5, errs
 
 
-def test_step_host_entry_point_matches_device_loop(amhd):
+@pytest.mark.parametrize("n", [64, 60])  # 64: unpadded planes, one copy each way; 60: padded rows, per-plane copies
+def test_step_host_entry_point_matches_device_loop(amhd, n):
     from aeromhd_cuda_b200 import _tensors, initial_conditions as ic
-    s = amhd.solver.MHDSolver(ot_cfg(64))
+    s = amhd.solver.MHDSolver(ot_cfg(n))
     s.set_primitive(ic.orszag_tang(s))
     host = np.ascontiguousarray(np_(s.U))
-    ref = amhd.solver.MHDSolver(ot_cfg(64))
+    ref = amhd.solver.MHDSolver(ot_cfg(n))
     ref.U = s.U.clone()
     ref.advance(max_steps=1)
     out = (ctypes.c_double * 4)()
