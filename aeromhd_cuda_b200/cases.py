@@ -6,6 +6,7 @@
     python -m aeromhd_cuda_b200.cases brio_wu
     python -m aeromhd_cuda_b200.cases reference_rmi        # main.py:446-474
     python -m aeromhd_cuda_b200.cases rmi_convergence      # main.py:294-396, :476-492
+    python -m aeromhd_cuda_b200.cases function_by_function --n 2048   # solver.py:268-333, pass by pass
 
 Each prints one JSON object (wall time, steps, zone-updates/s and the case's
 accuracy figures).  Errors of the float32 path are measured against a float64
@@ -248,10 +249,59 @@ def _timed_advance_run(s: MHDSolver) -> float:
     return time.perf_counter() - t0
 
 
+def function_by_function(n: int = 2048, precision: str = "fp64", steps: int = 5) -> dict:
+    """The reference's step structure (compute_rhs / step_ssprk3, solver.py:268-333)
+    executed function by function on the GPU: ghost fill, cons->prim, MUSCL and
+    HLLD in x and y as separate passes over the grid (this library's
+    per-function kernels), the flux differences, the right-hand side and the RK
+    combinations as torch array operations -- the shape of the reference's
+    CuPy path, with one pass per function where CuPy takes several.  Timed on
+    the Orszag-Tang n x n grid; the fused run loop does the same step in one
+    pass per stage."""
+    from . import physics as P
+    s = MHDSolver(orszag_tang_config(n, precision, t_end=1e30))
+    s.set_primitive(ic.orszag_tang(s))
+    cfg, ng, nx, ny = s.cfg, 2, n, n
+
+    def rhs(U, ch):
+        s.apply_bc(U)
+        W = P.cons_to_prim(U, cfg.gamma)
+        WLx, WRx = P.muscl_x(W)
+        Fx, _ = P.hlld_flux_x(WLx, WRx, cfg.gamma, ch, return_smax_array=True)
+        WLy, WRy = P.muscl_y(W)
+        Fy, _ = P.hlld_flux_y(WLy, WRy, cfg.gamma, ch, return_smax_array=True)
+        R = torch.zeros_like(U)
+        R[:, ng:ng + nx, ng:ng + ny] -= (Fx[:, 1:1 + nx, :] - Fx[:, 0:nx, :])[:, :, ng:ng + ny] / cfg.dx
+        R[:, ng:ng + nx, ng:ng + ny] -= (Fy[:, :, 1:1 + ny] - Fy[:, :, 0:ny])[:, ng:ng + nx, :] / cfg.dy
+        return R
+
+    def step(U, dt, ch):
+        U0 = U.clone()
+        U1 = s.enforce_scalar_bounds(U0 + dt * rhs(U0, ch))
+        U2 = s.enforce_scalar_bounds(0.75 * U0 + 0.25 * (U1 + dt * rhs(U1, ch)))
+        return s.enforce_scalar_bounds((1.0 / 3.0) * U0 + (2.0 / 3.0) * (U2 + dt * rhs(U2, ch)))
+
+    U = s.U.clone()
+    dt = s.compute_dt(P.cons_to_prim(U, cfg.gamma))
+    ch = cfg.glm_ch
+    for _ in range(2):
+        U = step(U, dt, ch)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        U = step(U, dt, ch)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"case": "function_by_function", "n": n, "precision": precision, "ms_per_step": ms,
+            "zone_updates_per_s": n * n / (ms / 1e3)}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("case", choices=["orszag_tang", "cp_alfven", "shock_interface", "brio_wu", "reference_rmi",
-                                     "rmi_convergence"])
+                                     "rmi_convergence", "function_by_function"])
     ap.add_argument("--n", type=int, default=512)
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--ny", type=int, default=512)
@@ -270,6 +320,8 @@ def main(argv=None) -> int:
         r = shock_interface(a.nx, a.ny, a.t_end or 3.0, precs)
     elif a.case == "reference_rmi":
         r = {p: reference_rmi_cases(p, a.t_end or 0.25) for p in precs}
+    elif a.case == "function_by_function":
+        r = {p: function_by_function(a.n, p) for p in precs}
     elif a.case == "rmi_convergence":
         r = {p: [rmi_convergence(by, precision=p) for by in (0.0, 1.5)] for p in precs}
     else:
