@@ -161,6 +161,186 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(int transA, int transB, 
             }
 }
 
+// ---------------------------------------------------------------------------
+// The same GEMM on the 5th-generation tensor cores: tcgen05.mma (kind::f16,
+// BF16 operands, FP32 accumulation in tensor memory).  One 128 x 128 output
+// tile per CTA of 4 warps, K in steps of 64: the warps stage the A and B tiles
+// in shared memory, both K-major in the canonical layout without swizzle (core
+// matrices of 8 rows x 8 values, 128 contiguous bytes; 128 B between core
+// matrices along M / N, 2 KB between the 8-value groups along K), one thread
+// issues four MMAs of K = 16 and commits them to an mbarrier, and every thread
+// waits for it (bounded: after kTcWaitIters polls the CTA records an error and
+// stops issuing) before the tiles are restaged.  The accumulator, 128 TMEM
+// lanes x 128 columns, is read back with tcgen05.ld (each warp its 32 rows).
+// The TMEM columns are freed on every path.  The CTA asks for enough shared
+// memory that at most 4 are resident on an SM (4 x 128 of the 512 columns).
+// ---------------------------------------------------------------------------
+constexpr int TM = 128, TN = 128, TK = 64;
+__device__ int g_tc_err;  // set when an MMA wait gave up (amhd_nn_gemm_status reads and clears it)
+constexpr uint32_t kTcWaitIters = 1u << 24;
+constexpr int kTcSmemBytes = 52 * 1024;  // > 228 KB / 5: at most 4 CTAs per SM
+
+struct TcSmem {
+    bf16 a[TK / 8][TM / 8][8][8];  // element (m, k) at [k / 8][m / 8][m % 8][k % 8]
+    bf16 b[TK / 8][TN / 8][8][8];  // element (n, k) likewise
+    uint64_t mbar;
+    uint32_t tmem;
+    int err;
+};
+
+__device__ __forceinline__ uint32_t tc_smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: no swizzle, K-major (version 1, base offset 0)
+__device__ __forceinline__ uint64_t tc_desc(const void *start, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+    const uint64_t a = (tc_smem_addr(start) >> 4) & 0x3FFFu;
+    return a | ((uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16) | ((uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32) |
+           (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: F32 accumulator, BF16 A and B, both K-major, M = TM, N = TN
+constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                              ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity)
+{
+    const uint32_t a = tc_smem_addr(bar);
+    for (uint32_t it = 0; it < kTcWaitIters; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, int M, int N, int K, const bf16 *A,
+                                                      int lda, const bf16 *B, int ldb, float *C, int ldc,
+                                                      float alpha, float beta, int k_per_split, int *err_flag)
+{
+    extern __shared__ __align__(1024) unsigned char tc_raw[];
+    TcSmem &sm = *reinterpret_cast<TcSmem *>(tc_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int kbeg = blockIdx.z * k_per_split;
+    const int kend = min(K, kbeg + k_per_split);
+    const bf16 zero = __float2bfloat16(0.f);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_addr(&sm.tmem)),
+                     "r"(TN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        sm.err = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem;
+
+    uint32_t phase = 0;
+    bool first = true;
+    for (int k0 = kbeg; k0 < kend && !sm.err; k0 += TK) {
+        for (int e = tid; e < TM * TK; e += 128) {
+            int mm, kk;
+            if (!transA) {
+                mm = e / TK;
+                kk = e % TK;
+            } else {
+                kk = e / TM;
+                mm = e % TM;
+            }
+            const int gm = m0 + mm, gk = k0 + kk;
+            bf16 v = zero;
+            if (gm < M && gk < kend) v = transA ? A[(int64_t)gk * lda + gm] : A[(int64_t)gm * lda + gk];
+            sm.a[kk >> 3][mm >> 3][mm & 7][kk & 7] = v;
+        }
+        for (int e = tid; e < TN * TK; e += 128) {
+            int nn, kk;
+            if (!transB) {
+                kk = e / TN;
+                nn = e % TN;
+            } else {
+                nn = e / TK;
+                kk = e % TK;
+            }
+            const int gn = n0 + nn, gk = k0 + kk;
+            bf16 v = zero;
+            if (gn < N && gk < kend) v = transB ? B[(int64_t)gn * ldb + gk] : B[(int64_t)gk * ldb + gn];
+            sm.b[kk >> 3][nn >> 3][nn & 7][kk & 7] = v;
+        }
+        // the tensor cores read the tiles through the async proxy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < TK / 16; ++j) {
+                const uint64_t da = tc_desc(&sm.a[2 * j][0][0][0], 2048u, 128u);
+                const uint64_t db = tc_desc(&sm.b[2 * j][0][0][0], 2048u, 128u);
+                const uint32_t acc = (first && j == 0) ? 0u : 1u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             tc_smem_addr(&sm.mbar))
+                         : "memory");
+        }
+        first = false;
+        if (!tc_wait(&sm.mbar, phase)) sm.err = 1;  // every thread gave up: no more MMAs, nothing read back
+        phase ^= 1u;
+        __syncthreads();
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!first && !sm.err) {
+        const int row = m0 + warp * 32 + lane;
+        const bool split = gridDim.z > 1;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TN; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int col = n0 + c0 + i;
+                    if (col < N) {
+                        float *p = &C[(int64_t)row * ldc + col];
+                        const float v = alpha * __uint_as_float(r[i]);
+                        if (split)
+                            atomicAdd(p, v);
+                        else
+                            *p = (beta != 0.f) ? v + beta * (*p) : v;
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN) : "memory");
+    }
+    if (tid == 0 && sm.err) atomicOr(err_flag, 1);
+}
+
 __global__ void scale_kernel(float *C, int M, int N, int ldc, float beta)
 {
     const int64_t n = (int64_t)M * N;
@@ -447,6 +627,48 @@ __global__ void apply_guarded_kernel(R *U, int pitch, int64_t vs, int nx, int ny
 extern "C" {
 
 const char *amhd_nn_last_error(void) { return g_nn_err.c_str(); }
+
+int amhd_nn_gemm_tc(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K, const void *A, int32_t lda,
+                    const void *B, int32_t ldb, float *C, int32_t ldc, float alpha, float beta, int32_t splits,
+                    void *stream)
+{
+    if (M < 0 || N < 0 || K < 0 || !A || !B || !C) return nn_fail(AMHD_ERR_ARG, "bad gemm arguments");
+    if (M == 0 || N == 0) return AMHD_OK;
+    static bool configured = false;
+    if (!configured) {
+        NNCK(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes));
+        configured = true;
+    }
+    int *err = nullptr;
+    NNCK(cudaGetSymbolAddress(reinterpret_cast<void **>(&err), g_tc_err));
+    if (splits < 1) splits = 1;
+    int kps = (K + splits - 1) / splits;
+    kps = (kps + TK - 1) / TK * TK;
+    if (kps < TK) kps = TK;
+    splits = K > 0 ? (K + kps - 1) / kps : 1;
+    cudaStream_t s = S(stream);
+    if (splits > 1 || K == 0) {
+        scale_kernel<<<blocks_for((int64_t)M * N), 256, 0, s>>>(C, M, N, ldc, beta);
+        NNCK(cudaGetLastError());
+        if (K == 0) return AMHD_OK;
+    }
+    dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM, splits);
+    gemm_tc_kernel<<<grid, 128, kTcSmemBytes, s>>>(transA, transB, M, N, K, static_cast<const bf16 *>(A), lda,
+                                                   static_cast<const bf16 *>(B), ldb, C, ldc, alpha,
+                                                   splits > 1 ? 0.f : beta, kps, err);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_gemm_status(int32_t *flag)
+{
+    if (!flag) return nn_fail(AMHD_ERR_ARG, "NULL flag");
+    int v = 0, z = 0;
+    NNCK(cudaMemcpyFromSymbol(&v, g_tc_err, sizeof v));
+    NNCK(cudaMemcpyToSymbol(g_tc_err, &z, sizeof z));
+    *flag = v;
+    return AMHD_OK;
+}
 
 int amhd_nn_gemm(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K, const void *A, int32_t lda,
                  const void *B, int32_t ldb, float *C, int32_t ldc, float alpha, float beta, int32_t splits,

@@ -330,6 +330,14 @@ const char *amhd_nn_last_error(void);
  * m16n8k16, FP32 accumulate).  op(A) = A ([M][K], lda) or, transA, A^T (A
  * stored [K][M]); op(B) = B ([K][N]) or, transB, B^T (B stored [N][K]).
  * splits > 1 divides K over CTAs and accumulates atomically. */
+/* The same contract on the 5th-generation tensor cores (tcgen05.mma, FP32
+ * accumulator in tensor memory, 128 x 128 tiles).  amhd_nn_gemm_status
+ * returns (and clears) 1 if an MMA completion wait gave up since the last
+ * call, else 0. */
+int amhd_nn_gemm_tc(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K, const void *A, int32_t lda,
+                    const void *B, int32_t ldb, float *C, int32_t ldc, float alpha, float beta, int32_t splits,
+                    void *stream);
+int amhd_nn_gemm_status(int32_t *flag);
 int amhd_nn_gemm(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K, const void *A, int32_t lda,
                  const void *B, int32_t ldb, float *C, int32_t ldc, float alpha, float beta, int32_t splits,
                  void *stream);

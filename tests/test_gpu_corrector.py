@@ -33,6 +33,34 @@ def test_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
     assert err < 2e-6, err
 
 
+@pytest.mark.parametrize("transA,transB", [(0, 0), (0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("M,N,K,splits", [(128, 128, 64, 1), (37, 91, 53, 1), (256, 300, 700, 4), (10, 4096, 288, 1),
+                                          (64, 64, 5000, 7)])
+def test_tcgen05_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
+    """amhd_nn_gemm_tc (tcgen05.mma, FP32 accumulator in tensor memory) against a
+    float64 matmul of the same BF16 operands, every transpose and split-K case,
+    partial tiles included; its completion waits never gave up."""
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import stream_ptr
+    import ctypes
+    g = torch.Generator(device="cuda").manual_seed(M * N + K + 7)
+    A = bf(torch.randn((K, M) if transA else (M, K), device="cuda", generator=g))
+    B = bf(torch.randn((N, K) if transB else (K, N), device="cuda", generator=g))
+    C = torch.randn((M, N), device="cuda", generator=g)
+    C0 = C.clone()
+    _lib.call("amhd_nn_gemm_tc", transA, transB, M, N, K, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1],
+              C.data_ptr(), N, 0.5, 2.0, splits, stream_ptr())
+    torch.cuda.synchronize()
+    flag = ctypes.c_int32(-1)
+    _lib.call("amhd_nn_gemm_status", ctypes.byref(flag))
+    assert flag.value == 0
+    opA = A.float().t() if transA else A.float()
+    opB = B.float().t() if transB else B.float()
+    ref = 0.5 * (opA.double() @ opB.double()) + 2.0 * C0.double()
+    err = float((C.double() - ref).abs().max() / ref.abs().max())
+    assert err < 2e-6, err
+
+
 def _net_and_oracle(H=32, W=16, B=2, seed=5):
     import nn_oracle
     from aeromhd_cuda_b200.corrector import Corrector, architecture, init_params
