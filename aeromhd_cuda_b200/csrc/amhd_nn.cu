@@ -180,13 +180,53 @@ __device__ int g_tc_err;  // set when an MMA wait gave up (amhd_nn_gemm_status r
 constexpr uint32_t kTcWaitIters = 1u << 24;
 constexpr int kTcSmemBytes = 52 * 1024;  // > 228 KB / 5: at most 4 CTAs per SM
 
+// Each operand tile is stored in the layout of its source: K-major, element
+// (m, k) at [k / 8][m / 8][m % 8][k % 8], when the source is contiguous along K
+// (A not transposed, B transposed), MN-major, element (m, k) at
+// [k / 8][m / 8][k % 8][m % 8], when it is contiguous along M / N; either way
+// 8 consecutive source values are one 16-byte row of a core matrix.
 struct TcSmem {
-    bf16 a[TK / 8][TM / 8][8][8];  // element (m, k) at [k / 8][m / 8][m % 8][k % 8]
-    bf16 b[TK / 8][TN / 8][8][8];  // element (n, k) likewise
+    bf16 a[TK / 8][TM / 8][8][8];
+    bf16 b[TK / 8][TN / 8][8][8];
     uint64_t mbar;
     uint32_t tmem;
     int err;
 };
+
+// Stage rows x TK values of one operand: src is contiguous along K (kmajor) or
+// along the rows; 8-value pieces move as 16-byte copies when aligned and in
+// range, the rest value by value with zero fill.
+__device__ __forceinline__ void tc_stage(bf16 (*dst)[TM / 8][8][8], const bf16 *src, int ld, bool kmajor, int r0,
+                                         int rows_total, int k0, int kend, int tid)
+{
+    const bf16 zero = __float2bfloat16(0.f);
+    constexpr int kPieces = TM * TK / 8;
+#pragma unroll 2
+    for (int e = tid; e < kPieces; e += 128) {
+        int r, k;  // first value of the piece: tile row r, tile column k
+        if (kmajor) {
+            r = e / (TK / 8);
+            k = (e % (TK / 8)) * 8;
+        } else {
+            k = e / (TM / 8);
+            r = (e % (TM / 8)) * 8;
+        }
+        const int gr = r0 + r, gk = k0 + k;
+        bf16 *d = kmajor ? &dst[k >> 3][r >> 3][r & 7][0] : &dst[k >> 3][r >> 3][k & 7][0];
+        const bf16 *s = kmajor ? src + (int64_t)gr * ld + gk : src + (int64_t)gk * ld + gr;
+        const bool full = kmajor ? (gr < rows_total && gk + 8 <= kend) : (gk < kend && gr + 8 <= rows_total);
+        if (full && (reinterpret_cast<uintptr_t>(s) & 15) == 0) {
+            *reinterpret_cast<uint4 *>(d) = *reinterpret_cast<const uint4 *>(s);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int rr = kmajor ? gr : gr + i, kk = kmajor ? gk + i : gk;
+                d[i] = (rr < rows_total && kk < kend) ? (kmajor ? src[(int64_t)rr * ld + kk] : src[(int64_t)kk * ld + rr])
+                                                      : zero;
+            }
+        }
+    }
+}
 
 __device__ __forceinline__ uint32_t tc_smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -198,7 +238,8 @@ __device__ __forceinline__ uint64_t tc_desc(const void *start, uint32_t lbo_byte
            (1ull << 46);
 }
 
-// instruction descriptor of kind::f16: F32 accumulator, BF16 A and B, both K-major, M = TM, N = TN
+// instruction descriptor of kind::f16: F32 accumulator, BF16 A and B, M = TM,
+// N = TN; bit 15 / 16: A / B MN-major
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
                               ((uint32_t)(TM >> 4) << 24);
 
@@ -247,35 +288,11 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, in
 
     uint32_t phase = 0;
     bool first = true;
+    const bool a_kmajor = !transA, b_kmajor = transB != 0;
+    const uint32_t idesc = kTcIdesc | (a_kmajor ? 0u : 1u << 15) | (b_kmajor ? 0u : 1u << 16);
     for (int k0 = kbeg; k0 < kend && !sm.err; k0 += TK) {
-        for (int e = tid; e < TM * TK; e += 128) {
-            int mm, kk;
-            if (!transA) {
-                mm = e / TK;
-                kk = e % TK;
-            } else {
-                kk = e / TM;
-                mm = e % TM;
-            }
-            const int gm = m0 + mm, gk = k0 + kk;
-            bf16 v = zero;
-            if (gm < M && gk < kend) v = transA ? A[(int64_t)gk * lda + gm] : A[(int64_t)gm * lda + gk];
-            sm.a[kk >> 3][mm >> 3][mm & 7][kk & 7] = v;
-        }
-        for (int e = tid; e < TN * TK; e += 128) {
-            int nn, kk;
-            if (!transB) {
-                kk = e / TN;
-                nn = e % TN;
-            } else {
-                nn = e / TK;
-                kk = e % TK;
-            }
-            const int gn = n0 + nn, gk = k0 + kk;
-            bf16 v = zero;
-            if (gn < N && gk < kend) v = transB ? B[(int64_t)gn * ldb + gk] : B[(int64_t)gk * ldb + gn];
-            sm.b[kk >> 3][nn >> 3][nn & 7][kk & 7] = v;
-        }
+        tc_stage(sm.a, A, lda, a_kmajor, m0, M, k0, kend, tid);
+        tc_stage(sm.b, B, ldb, b_kmajor, n0, N, k0, kend, tid);
         // the tensor cores read the tiles through the async proxy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -289,7 +306,7 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, in
                 asm volatile(
                     "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                    "l"(da), "l"(db), "r"(kTcIdesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
                     : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
