@@ -173,12 +173,14 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(int transA, int transB, 
 // stops issuing) before the tiles are restaged.  The accumulator, 128 TMEM
 // lanes x 128 columns, is read back with tcgen05.ld (each warp its 32 rows).
 // The TMEM columns are freed on every path.  The CTA asks for enough shared
-// memory that at most 4 are resident on an SM (4 x 128 of the 512 columns).
+// memory that at most 3 are resident on an SM (3 x 128 of the 512 columns).
+// Two shared-memory stages: while the MMAs of one K step run, the warps stage
+// the next.
 // ---------------------------------------------------------------------------
 constexpr int TM = 128, TN = 128, TK = 64;
 __device__ int g_tc_err;  // set when an MMA wait gave up (amhd_nn_gemm_status reads and clears it)
 constexpr uint32_t kTcWaitIters = 1u << 24;
-constexpr int kTcSmemBytes = 52 * 1024;  // > 228 KB / 5: at most 4 CTAs per SM
+constexpr int kTcSmemBytes = 66 * 1024;  // > 228 KB / 4: at most 3 CTAs per SM (3 x 128 TMEM columns)
 
 // Each operand tile is stored in the layout of its source: K-major, element
 // (m, k) at [k / 8][m / 8][m % 8][k % 8], when the source is contiguous along K
@@ -186,9 +188,9 @@ constexpr int kTcSmemBytes = 52 * 1024;  // > 228 KB / 5: at most 4 CTAs per SM
 // [k / 8][m / 8][k % 8][m % 8], when it is contiguous along M / N; either way
 // 8 consecutive source values are one 16-byte row of a core matrix.
 struct TcSmem {
-    bf16 a[TK / 8][TM / 8][8][8];
-    bf16 b[TK / 8][TN / 8][8][8];
-    uint64_t mbar;
+    bf16 a[2][TK / 8][TM / 8][8][8];  // two stages: the next tile is staged while the MMAs read this one
+    bf16 b[2][TK / 8][TN / 8][8][8];
+    uint64_t mbar[2];  // completion of the MMAs that read stage 0 / 1
     uint32_t tmem;
     int err;
 };
@@ -278,7 +280,8 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, in
     }
     if (tid == 0) {
         sm.err = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.mbar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.mbar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.mbar[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -286,23 +289,40 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, in
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = sm.tmem;
 
-    uint32_t phase = 0;
-    bool first = true;
     const bool a_kmajor = !transA, b_kmajor = transB != 0;
     const uint32_t idesc = kTcIdesc | (a_kmajor ? 0u : 1u << 15) | (b_kmajor ? 0u : 1u << 16);
-    for (int k0 = kbeg; k0 < kend && !sm.err; k0 += TK) {
-        tc_stage(sm.a, A, lda, a_kmajor, m0, M, k0, kend, tid);
-        tc_stage(sm.b, B, ldb, b_kmajor, n0, N, k0, kend, tid);
+    const int nk = kend > kbeg ? (kend - kbeg + TK - 1) / TK : 0;
+    // commit i arrives on mbar[i & 1]; `done` commits have been waited for, in
+    // order, so each barrier has at most one phase outstanding.  A timeout marks
+    // the CTA (read by every thread only after the next barrier, so all decide
+    // alike); the waits stay bounded either way.
+    uint32_t ph = 0u;  // bit b: the parity awaited next on mbar[b]
+    int done = 0;
+    auto wait_until = [&](int n) {
+        for (; done < n; ++done) {
+            const int b = done & 1;
+            if (!tc_wait(&sm.mbar[b], (ph >> b) & 1u)) sm.err = 1;
+            ph ^= 1u << b;
+        }
+    };
+    if (nk > 0) {
+        tc_stage(sm.a[0], A, lda, a_kmajor, m0, M, kbeg, kend, tid);
+        tc_stage(sm.b[0], B, ldb, b_kmajor, n0, N, kbeg, kend, tid);
+    }
+    int issued = 0;
+    for (int it = 0; it < nk; ++it) {
+        const int buf = it & 1;
         // the tensor cores read the tiles through the async proxy
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
+        if (sm.err) break;
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
             for (int j = 0; j < TK / 16; ++j) {
-                const uint64_t da = tc_desc(&sm.a[2 * j][0][0][0], 2048u, 128u);
-                const uint64_t db = tc_desc(&sm.b[2 * j][0][0][0], 2048u, 128u);
-                const uint32_t acc = (first && j == 0) ? 0u : 1u;
+                const uint64_t da = tc_desc(&sm.a[buf][2 * j][0][0][0], 2048u, 128u);
+                const uint64_t db = tc_desc(&sm.b[buf][2 * j][0][0][0], 2048u, 128u);
+                const uint32_t acc = (it == 0 && j == 0) ? 0u : 1u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
@@ -310,15 +330,22 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, in
                     : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             tc_smem_addr(&sm.mbar))
+                             tc_smem_addr(&sm.mbar[buf]))
                          : "memory");
         }
-        first = false;
-        if (!tc_wait(&sm.mbar, phase)) sm.err = 1;  // every thread gave up: no more MMAs, nothing read back
-        phase ^= 1u;
-        __syncthreads();
+        issued = it + 1;
+        if (it + 1 < nk) {
+            // stage it+1 goes where the MMAs of step it-1 read: wait for them first
+            wait_until(it);
+            const int k1 = kbeg + (it + 1) * TK;
+            tc_stage(sm.a[buf ^ 1], A, lda, a_kmajor, m0, M, k1, kend, tid);
+            tc_stage(sm.b[buf ^ 1], B, ldb, b_kmajor, n0, N, k1, kend, tid);
+        }
     }
+    wait_until(issued);  // the MMAs still in flight (the last one or two steps)
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool first = issued == 0;
     if (!first && !sm.err) {
         const int row = m0 + warp * 32 + lane;
         const bool split = gridDim.z > 1;
