@@ -6,10 +6,12 @@
 // Activations are FP32 in [C][B*H*W] layout (channel-major: the output of a
 // GEMM W[Cout][K] x col[K][N] is the next layer's input as is); GEMM operands
 // are BF16, weights keep an FP32 master copy for Adam.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <string>
@@ -385,6 +387,197 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, in
     if (tid == 0 && sm.err) atomicOr(err_flag, 1);
 }
 
+// ---------------------------------------------------------------------------
+// tcgen05 GEMM with TMA operand loads: 128 x 64 tiles (M x N), K steps of 64
+// through a ring of kTmaStages shared-memory stages.  Thread 0 issues the
+// loads (one TMA per operand and step, completion counted in bytes on
+// full[s]); thread 32 waits for a stage, issues its four 128 x 64 x 16 MMAs
+// and commits them to empty[s], which frees the stage for the next load; a
+// last commit on `done` releases the epilogue (all 4 warps, one TMEM lane
+// quadrant each).  Tensor maps (one per operand, built on the host):
+//   K-major (rows contiguous along K):  dims {8, rows, K / 8}, strides
+//     {ld, 8} elements, box {8, tile rows, 8} -> element (r, k) of the tile
+//     at [k / 8][r][k % 8]
+//   MN-major (contiguous along the rows): dims {8, 8, rows / 8, K / 8},
+//     strides {ld, 8, 8 ld}, box {8, 8, tile rows / 8, 8} -> element (r, k)
+//     at [k / 8][r / 8][k % 8][r % 8]
+// which are the canonical no-swizzle layouts of the thread-staged kernel
+// (8 x 16-byte core matrices; K-direction stride tile rows x 16 bytes,
+// row-direction stride 128 bytes).  Out-of-range rows and K groups read as
+// zero.  Every wait is bounded; a timeout marks the CTA, which still waits
+// (bounded) for its loads and MMAs in flight and frees its TMEM columns.
+// ---------------------------------------------------------------------------
+constexpr int kTmaStages = 4, TN2 = 64;
+constexpr int kTmaABytes = TM * TK * 2, kTmaBBytes = TN2 * TK * 2;
+
+struct TmaSmem {
+    alignas(1024) unsigned char a[kTmaStages][kTmaABytes];
+    alignas(1024) unsigned char b[kTmaStages][kTmaBBytes];
+    uint64_t full[kTmaStages], empty[kTmaStages], done;
+    uint32_t tmem;
+    int err;
+};
+constexpr int kTmaSmemBytes = (int)sizeof(TmaSmem) + 1024;  // + alignment slack of the dynamic window
+
+constexpr uint32_t kTmaIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN2 >> 3) << 17) |
+                               ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, bool four_d, int c1, int c2, int c3,
+                                         uint64_t *bar)
+{
+    if (four_d)
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+            "%5}], [%6];" ::"r"(tc_smem_addr(dst)),
+            "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(c2), "r"(c3), "r"(tc_smem_addr(bar))
+            : "memory");
+    else
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+            "%4}], [%5];" ::"r"(tc_smem_addr(dst)),
+            "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(c1), "r"(c3), "r"(tc_smem_addr(bar))
+            : "memory");
+}
+
+__global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ CUtensorMap mapA,
+                                                       const __grid_constant__ CUtensorMap mapB, int a_kmajor,
+                                                       int b_kmajor, int M, int N, int K, float *C, int ldc,
+                                                       float alpha, float beta, int k_per_split, int *err_flag)
+{
+    extern __shared__ unsigned char tma_raw[];
+    TmaSmem &sm = *reinterpret_cast<TmaSmem *>((reinterpret_cast<uintptr_t>(tma_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN2;
+    const int kbeg = blockIdx.z * k_per_split;
+    const int kend = min(K, kbeg + k_per_split);
+    const int nk = kend > kbeg ? (kend - kbeg + TK - 1) / TK : 0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_addr(&sm.tmem)),
+                     "r"(TN2)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        sm.err = 0;
+        for (int s = 0; s < kTmaStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.full[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.empty[s])) : "memory");
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.done)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem;
+
+    if (tid == 0) {
+        // producer: stage s = kt % kTmaStages takes load kt once the MMAs of load kt - kTmaStages are done
+        int issued = 0;
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % kTmaStages;
+            if (kt >= kTmaStages && !tc_wait(&sm.empty[s], (uint32_t)((kt / kTmaStages) - 1) & 1u)) {
+                sm.err = 1;
+                break;
+            }
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem_addr(&sm.full[s])),
+                         "r"(kTmaABytes + kTmaBBytes)
+                         : "memory");
+            const int kg = (kbeg + kt * TK) >> 3;
+            tma_load(sm.a[s], &mapA, !a_kmajor, m0, m0 >> 3, kg, &sm.full[s]);
+            tma_load(sm.b[s], &mapB, !b_kmajor, n0, n0 >> 3, kg, &sm.full[s]);
+            issued = kt + 1;
+        }
+        // the loads still in flight land before the CTA can leave: the last one of each stage
+        for (int s = 0; s < kTmaStages && s < issued; ++s) {
+            const int uses = (issued - 1 - s) / kTmaStages + 1;
+            if (!tc_wait(&sm.full[s], (uint32_t)(uses - 1) & 1u)) sm.err = 1;
+        }
+    } else if (tid == 32) {
+        // MMA issuer
+        for (int kt = 0; kt < nk; ++kt) {
+            const int s = kt % kTmaStages;
+            if (!tc_wait(&sm.full[s], (uint32_t)(kt / kTmaStages) & 1u)) {
+                sm.err = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t idesc = kTmaIdesc | (a_kmajor ? 0u : 1u << 15) | (b_kmajor ? 0u : 1u << 16);
+#pragma unroll
+            for (int j = 0; j < TK / 16; ++j) {
+                // K step j: core matrices 2j and 2j+1 along K
+                const uint64_t da = tc_desc(sm.a[s] + j * 2 * (TM * 16), TM * 16u, 128u);
+                const uint64_t db = tc_desc(sm.b[s] + j * 2 * (TN2 * 16), TN2 * 16u, 128u);
+                const uint32_t acc = (kt == 0 && j == 0) ? 0u : 1u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             tc_smem_addr(&sm.empty[s]))
+                         : "memory");
+        }
+        // arrives once every MMA issued above has completed
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         tc_smem_addr(&sm.done))
+                     : "memory");
+    }
+    if (!tc_wait(&sm.done, 0u)) sm.err = 1;
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (nk > 0 && !sm.err) {
+        const int row = m0 + warp * 32 + lane;
+        const bool split = gridDim.z > 1;
+        const bool vec = !split && beta == 0.f && (ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+#pragma unroll 1
+        for (int c0 = 0; c0 < TN2; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+                float *crow = C + (int64_t)row * ldc;
+                if (vec && n0 + c0 + 16 <= N) {
+#pragma unroll
+                    for (int i = 0; i < 16; i += 4)
+                        *reinterpret_cast<float4 *>(crow + n0 + c0 + i) =
+                            make_float4(alpha * __uint_as_float(r[i]), alpha * __uint_as_float(r[i + 1]),
+                                        alpha * __uint_as_float(r[i + 2]), alpha * __uint_as_float(r[i + 3]));
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        const int col = n0 + c0 + i;
+                        if (col < N) {
+                            float *p = crow + col;
+                            const float v = alpha * __uint_as_float(r[i]);
+                            if (split)
+                                atomicAdd(p, v);
+                            else
+                                *p = (beta != 0.f) ? v + beta * (*p) : v;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN2) : "memory");
+    }
+    if (tid == 0 && sm.err) atomicOr(err_flag, 1);
+}
+
 __global__ void scale_kernel(float *C, int M, int N, int ldc, float beta)
 {
     const int64_t n = (int64_t)M * N;
@@ -667,6 +860,110 @@ __global__ void apply_guarded_kernel(R *U, int pitch, int64_t vs, int nx, int ny
 
 }  // namespace
 
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn nn_encoder()
+{
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(ptr);
+    }
+    return fn;
+}
+
+// tensor map of one GEMM operand (layouts at gemm_tma_kernel): rows = M or N,
+// kmajor = the source is contiguous along K.  false: not expressible (base not
+// 16-byte aligned, ld or K -- or, MN-major, the row count -- not a multiple
+// of 8) or refused by the driver; the caller stages with threads instead.
+bool operand_map(CUtensorMap *map, const void *base, int ld, int rows, int K, int tile_rows, bool kmajor)
+{
+    EncodeTiledFn fn = nn_encoder();
+    if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) || ld % 8 || K % 8 || K <= 0 || rows <= 0) return false;
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r;
+    if (kmajor) {
+        if (ld < K) return false;
+        const cuuint64_t dims[3] = {8, (cuuint64_t)rows, (cuuint64_t)(K / 8)};
+        const cuuint64_t strides[2] = {(cuuint64_t)ld * 2, 16};
+        const cuuint32_t box[3] = {8, (cuuint32_t)tile_rows, 8};
+        r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    } else {
+        if (rows % 8 || ld < rows) return false;
+        const cuuint64_t dims[4] = {8, 8, (cuuint64_t)(rows / 8), (cuuint64_t)(K / 8)};
+        const cuuint64_t strides[3] = {(cuuint64_t)ld * 2, 16, (cuuint64_t)ld * 16};
+        const cuuint32_t box[4] = {8, 8, (cuuint32_t)(tile_rows / 8), 8};
+        r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    }
+    return r == CUDA_SUCCESS;
+}
+
+std::atomic<long long> g_tc_tma_launches{0}, g_tc_staged_launches{0};
+std::atomic<int> g_gemm_path{0};  // amhd_nn_set_gemm_path
+
+// split-K: K per split rounded up to whole K steps of `step`; returns the split count
+int split_k(int K, int splits, int step, int *kps_out)
+{
+    if (splits < 1) splits = 1;
+    int kps = (K + splits - 1) / splits;
+    kps = (kps + step - 1) / step * step;
+    if (kps < step) kps = step;
+    *kps_out = kps;
+    return K > 0 ? (K + kps - 1) / kps : 1;
+}
+
+// the TMA-fed tcgen05 GEMM, if both operands have tensor maps; *launched = false
+// (and nothing enqueued) otherwise
+int tma_gemm(int transA, int transB, int M, int N, int K, const void *A, int lda, const void *B, int ldb, float *C,
+             int ldc, float alpha, float beta, int splits, cudaStream_t s, bool *launched)
+{
+    *launched = false;
+    const bool a_kmajor = !transA, b_kmajor = transB != 0;
+    CUtensorMap map_a, map_b;
+    if (K <= 0 || !operand_map(&map_a, A, lda, M, K, TM, a_kmajor) || !operand_map(&map_b, B, ldb, N, K, TN2, b_kmajor))
+        return AMHD_OK;
+    static bool configured = false;
+    if (!configured) {
+        NNCK(cudaFuncSetAttribute(gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmemBytes));
+        configured = true;
+    }
+    int *err = nullptr;
+    NNCK(cudaGetSymbolAddress(reinterpret_cast<void **>(&err), g_tc_err));
+    int kps;
+    splits = split_k(K, splits, TK, &kps);
+    if (splits > 1) {
+        scale_kernel<<<blocks_for((int64_t)M * N), 256, 0, s>>>(C, M, N, ldc, beta);
+        NNCK(cudaGetLastError());
+    }
+    dim3 grid((N + TN2 - 1) / TN2, (M + TM - 1) / TM, splits);
+    gemm_tma_kernel<<<grid, 128, kTmaSmemBytes, s>>>(map_a, map_b, a_kmajor, b_kmajor, M, N, K, C, ldc, alpha,
+                                                     splits > 1 ? 0.f : beta, kps, err);
+    NNCK(cudaGetLastError());
+    ++g_tc_tma_launches;
+    *launched = true;
+    return AMHD_OK;
+}
+
+// shapes on which the tcgen05 pipeline beats mma.sync (B200): a 128-row MMA
+// tile that is mostly filled and more than one K step per tile, or a long K
+// (weight gradients); the narrow layers (M = 32, 64) stay on mma.sync
+bool prefer_tc(int M, int N, int K) { return (M >= 128 && K >= 128 && N >= 64) || K >= 4096; }
+
+}  // namespace
+
 #pragma GCC visibility push(default)
 extern "C" {
 
@@ -683,24 +980,40 @@ int amhd_nn_gemm_tc(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_
         NNCK(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes));
         configured = true;
     }
+    cudaStream_t s = S(stream);
+    bool launched = false;
+    const int rc = tma_gemm(transA, transB, M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, splits, s, &launched);
+    if (rc != AMHD_OK || launched) return rc;
     int *err = nullptr;
     NNCK(cudaGetSymbolAddress(reinterpret_cast<void **>(&err), g_tc_err));
-    if (splits < 1) splits = 1;
-    int kps = (K + splits - 1) / splits;
-    kps = (kps + TK - 1) / TK * TK;
-    if (kps < TK) kps = TK;
-    splits = K > 0 ? (K + kps - 1) / kps : 1;
-    cudaStream_t s = S(stream);
+    int kps;
+    splits = split_k(K, splits, TK, &kps);
     if (splits > 1 || K == 0) {
         scale_kernel<<<blocks_for((int64_t)M * N), 256, 0, s>>>(C, M, N, ldc, beta);
         NNCK(cudaGetLastError());
         if (K == 0) return AMHD_OK;
     }
+    ++g_tc_staged_launches;
     dim3 grid((N + TN - 1) / TN, (M + TM - 1) / TM, splits);
     gemm_tc_kernel<<<grid, 128, kTcSmemBytes, s>>>(transA, transB, M, N, K, static_cast<const bf16 *>(A), lda,
                                                    static_cast<const bf16 *>(B), ldb, C, ldc, alpha,
                                                    splits > 1 ? 0.f : beta, kps, err);
     NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_set_gemm_path(int32_t mode)
+{
+    if (mode < 0 || mode > 2) return nn_fail(AMHD_ERR_ARG, "gemm path %d (0 auto, 1 mma.sync, 2 tcgen05)", mode);
+    g_gemm_path.store(mode);
+    return AMHD_OK;
+}
+
+int amhd_nn_gemm_tc_paths(int64_t *tma, int64_t *staged)
+{
+    if (!tma || !staged) return nn_fail(AMHD_ERR_ARG, "NULL output");
+    *tma = g_tc_tma_launches.load();
+    *staged = g_tc_staged_launches.load();
     return AMHD_OK;
 }
 
@@ -720,12 +1033,16 @@ int amhd_nn_gemm(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K
 {
     if (M < 0 || N < 0 || K < 0 || !A || !B || !C) return nn_fail(AMHD_ERR_ARG, "bad gemm arguments");
     if (M == 0 || N == 0) return AMHD_OK;
-    if (splits < 1) splits = 1;
-    int kps = (K + splits - 1) / splits;
-    kps = (kps + GBK - 1) / GBK * GBK;
-    if (kps < GBK) kps = GBK;
-    splits = K > 0 ? (K + kps - 1) / kps : 1;
     cudaStream_t s = S(stream);
+    const int path = g_gemm_path.load();
+    if (path == 2) return amhd_nn_gemm_tc(transA, transB, M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, splits, stream);
+    if (path == 0 && prefer_tc(M, N, K)) {
+        bool launched = false;
+        const int rc = tma_gemm(transA, transB, M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, splits, s, &launched);
+        if (rc != AMHD_OK || launched) return rc;
+    }
+    int kps;
+    splits = split_k(K, splits, GBK, &kps);
     if (splits > 1 || K == 0) {
         scale_kernel<<<blocks_for((int64_t)M * N), 256, 0, s>>>(C, M, N, ldc, beta);
         NNCK(cudaGetLastError());

@@ -14,9 +14,13 @@ def bf(t):
     return t.to(torch.bfloat16)
 
 
+@pytest.mark.parametrize("path", [1, 0])
 @pytest.mark.parametrize("transA,transB", [(0, 0), (0, 1), (1, 0), (1, 1)])
-@pytest.mark.parametrize("M,N,K,splits", [(37, 91, 53, 1), (128, 300, 700, 4), (10, 4096, 288, 1), (64, 64, 5000, 7)])
-def test_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
+@pytest.mark.parametrize("M,N,K,splits", [(37, 91, 53, 1), (128, 300, 700, 4), (10, 4096, 288, 1), (64, 64, 5000, 7),
+                                          (256, 320, 704, 4)])
+def test_gemm_matches_float_matmul(transA, transB, M, N, K, splits, path):
+    """amhd_nn_gemm on mma.sync (path 1) and with the per-shape choice of
+    kernel (path 0: tcgen05 for the large shapes whose operands qualify)."""
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200._tensors import stream_ptr
     g = torch.Generator(device="cuda").manual_seed(M * N + K)
@@ -24,8 +28,12 @@ def test_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
     B = bf(torch.randn((N, K) if transB else (K, N), device="cuda", generator=g))
     C = torch.randn((M, N), device="cuda", generator=g)
     C0 = C.clone()
-    _lib.call("amhd_nn_gemm", transA, transB, M, N, K, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1],
-              C.data_ptr(), N, 0.5, 2.0, splits, stream_ptr())
+    _lib.call("amhd_nn_set_gemm_path", path)
+    try:
+        _lib.call("amhd_nn_gemm", transA, transB, M, N, K, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1],
+                  C.data_ptr(), N, 0.5, 2.0, splits, stream_ptr())
+    finally:
+        _lib.call("amhd_nn_set_gemm_path", 0)
     opA = A.float().t() if transA else A.float()
     opB = B.float().t() if transB else B.float()
     ref = 0.5 * (opA.double() @ opB.double()) + 2.0 * C0.double()
@@ -35,11 +43,12 @@ def test_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
 
 @pytest.mark.parametrize("transA,transB", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("M,N,K,splits", [(128, 128, 64, 1), (37, 91, 53, 1), (256, 300, 700, 4), (10, 4096, 288, 1),
-                                          (64, 64, 5000, 7)])
+                                          (64, 64, 5000, 7), (256, 320, 704, 4), (200, 136, 96, 1)])
 def test_tcgen05_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
     """amhd_nn_gemm_tc (tcgen05.mma, FP32 accumulator in tensor memory) against a
     float64 matmul of the same BF16 operands, every transpose and split-K case,
-    partial tiles included; its completion waits never gave up."""
+    partial tiles included, on both operand paths (TMA pipeline where ld and K
+    are multiples of 8, thread staging where not); its waits never gave up."""
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200._tensors import stream_ptr
     import ctypes
@@ -59,6 +68,33 @@ def test_tcgen05_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
     ref = 0.5 * (opA.double() @ opB.double()) + 2.0 * C0.double()
     err = float((C.double() - ref).abs().max() / ref.abs().max())
     assert err < 2e-6, err
+
+
+def test_tcgen05_gemm_operand_paths():
+    """Aligned operands go through the TMA pipeline, a K that is not a multiple
+    of 8 through thread staging; both agree with the float64 matmul."""
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import stream_ptr
+    import ctypes
+
+    def paths():
+        t, s = ctypes.c_int64(-1), ctypes.c_int64(-1)
+        _lib.call("amhd_nn_gemm_tc_paths", ctypes.byref(t), ctypes.byref(s))
+        return t.value, s.value
+
+    for (M, N, K), expect in (((128, 256, 128), (1, 0)), ((128, 256, 90), (0, 1))):
+        g = torch.Generator(device="cuda").manual_seed(K)
+        A = bf(torch.randn((M, K), device="cuda", generator=g))
+        B = bf(torch.randn((K, N), device="cuda", generator=g))
+        C = torch.zeros((M, N), device="cuda")
+        t0, s0 = paths()
+        _lib.call("amhd_nn_gemm_tc", 0, 0, M, N, K, A.data_ptr(), K, B.data_ptr(), N, C.data_ptr(), N, 1.0, 0.0, 1,
+                  stream_ptr())
+        torch.cuda.synchronize()
+        t1, s1 = paths()
+        assert (t1 - t0, s1 - s0) == expect, (M, N, K, t1 - t0, s1 - s0)
+        ref = A.double() @ B.double()
+        assert float((C.double() - ref).abs().max() / ref.abs().max()) < 2e-6
 
 
 def _net_and_oracle(H=32, W=16, B=2, seed=5):
