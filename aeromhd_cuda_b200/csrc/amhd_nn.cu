@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -394,20 +395,21 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, in
 // full[s]); thread 32 waits for a stage, issues its four 128 x 64 x 16 MMAs
 // and commits them to empty[s], which frees the stage for the next load; a
 // last commit on `done` releases the epilogue (all 4 warps, one TMEM lane
-// quadrant each).  Tensor maps (one per operand, built on the host):
-//   K-major (rows contiguous along K):  dims {8, rows, K / 8}, strides
-//     {ld, 8} elements, box {8, tile rows, 8} -> element (r, k) of the tile
-//     at [k / 8][r][k % 8]
-//   MN-major (contiguous along the rows): dims {8, 8, rows / 8, K / 8},
-//     strides {ld, 8, 8 ld}, box {8, 8, tile rows / 8, 8} -> element (r, k)
-//     at [k / 8][r / 8][k % 8][r % 8]
-// which are the canonical no-swizzle layouts of the thread-staged kernel
-// (8 x 16-byte core matrices; K-direction stride tile rows x 16 bytes,
-// row-direction stride 128 bytes).  Out-of-range rows and K groups read as
-// zero.  Every wait is bounded; a timeout marks the CTA, which still waits
-// (bounded) for its loads and MMAs in flight and frees its TMEM columns.
+// quadrant each).  Operand tiles are 128-byte swizzled (2-D tensor maps with
+// SWIZZLE_128B, stage buffers 1024-byte aligned):
+//   K-major (rows contiguous along K): box {64 K, tile rows} -> one 128-byte
+//     row per tile row, 8-row swizzle atoms 1024 bytes apart (descriptor
+//     SBO); the K step j of 16 values starts 32 j bytes into the row
+//   MN-major (contiguous along the rows): box {64 rows, 64 K} per 64 rows ->
+//     one 128-byte row per K index, 8-K-row atoms 1024 bytes apart (SBO),
+//     the second 64 rows of A 8192 bytes on (LBO); K step j starts 2048 j
+//     bytes on
+// Out-of-range rows and K read as zero.  Every wait is bounded; a timeout
+// marks the CTA, which still waits (bounded) for its loads and MMAs in flight
+// and frees its TMEM columns.
 // ---------------------------------------------------------------------------
 constexpr int kTmaStages = 4, TN2 = 64;
+constexpr int kNumSMs = 148;
 constexpr int kTmaABytes = TM * TK * 2, kTmaBBytes = TN2 * TK * 2;
 
 struct TmaSmem {
@@ -422,22 +424,17 @@ constexpr int kTmaSmemBytes = (int)sizeof(TmaSmem) + 1024;  // + alignment slack
 constexpr uint32_t kTmaIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN2 >> 3) << 17) |
                                ((uint32_t)(TM >> 4) << 24);
 
-__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, bool four_d, int c1, int c2, int c3,
-                                         uint64_t *bar)
+// 2-D tiled load, coordinates innermost first; x is a multiple of 64 values (128 bytes)
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int x, int y, uint64_t *bar)
 {
-    if (four_d)
-        asm volatile(
-            "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
-            "%5}], [%6];" ::"r"(tc_smem_addr(dst)),
-            "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(c2), "r"(c3), "r"(tc_smem_addr(bar))
-            : "memory");
-    else
-        asm volatile(
-            "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
-            "%4}], [%5];" ::"r"(tc_smem_addr(dst)),
-            "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(c1), "r"(c3), "r"(tc_smem_addr(bar))
-            : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(tc_smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(tc_smem_addr(bar))
+        : "memory");
 }
+
+constexpr uint64_t kSwizzle128 = 2ull << 61;  // descriptor layout type SWIZZLE_128B
 
 __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ CUtensorMap mapA,
                                                        const __grid_constant__ CUtensorMap mapB, int a_kmajor,
@@ -485,9 +482,17 @@ __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ C
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem_addr(&sm.full[s])),
                          "r"(kTmaABytes + kTmaBBytes)
                          : "memory");
-            const int kg = (kbeg + kt * TK) >> 3;
-            tma_load(sm.a[s], &mapA, !a_kmajor, m0, m0 >> 3, kg, &sm.full[s]);
-            tma_load(sm.b[s], &mapB, !b_kmajor, n0, n0 >> 3, kg, &sm.full[s]);
+            const int k0 = kbeg + kt * TK;
+            if (a_kmajor) {
+                tma_load(sm.a[s], &mapA, k0, m0, &sm.full[s]);
+            } else {
+                tma_load(sm.a[s], &mapA, m0, k0, &sm.full[s]);
+                tma_load(sm.a[s] + kTmaABytes / 2, &mapA, m0 + TM / 2, k0, &sm.full[s]);
+            }
+            if (b_kmajor)
+                tma_load(sm.b[s], &mapB, k0, n0, &sm.full[s]);
+            else
+                tma_load(sm.b[s], &mapB, n0, k0, &sm.full[s]);
             issued = kt + 1;
         }
         // the loads still in flight land before the CTA can leave: the last one of each stage
@@ -507,9 +512,11 @@ __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ C
             const uint32_t idesc = kTmaIdesc | (a_kmajor ? 0u : 1u << 15) | (b_kmajor ? 0u : 1u << 16);
 #pragma unroll
             for (int j = 0; j < TK / 16; ++j) {
-                // K step j: core matrices 2j and 2j+1 along K
-                const uint64_t da = tc_desc(sm.a[s] + j * 2 * (TM * 16), TM * 16u, 128u);
-                const uint64_t db = tc_desc(sm.b[s] + j * 2 * (TN2 * 16), TN2 * 16u, 128u);
+                // K step j: 32 bytes into each swizzled row (K-major) or two 8-row atoms on (MN-major)
+                const uint64_t da = kSwizzle128 | (a_kmajor ? tc_desc(sm.a[s] + j * 32, 16u, 1024u)
+                                                            : tc_desc(sm.a[s] + j * 2048, kTmaABytes / 2, 1024u));
+                const uint64_t db = kSwizzle128 | (b_kmajor ? tc_desc(sm.b[s] + j * 32, 16u, 1024u)
+                                                            : tc_desc(sm.b[s] + j * 2048, kTmaABytes / 2, 1024u));
                 const uint32_t acc = (kt == 0 && j == 0) ? 0u : 1u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -883,31 +890,20 @@ EncodeTiledFn nn_encoder()
 
 // tensor map of one GEMM operand (layouts at gemm_tma_kernel): rows = M or N,
 // kmajor = the source is contiguous along K.  false: not expressible (base not
-// 16-byte aligned, ld or K -- or, MN-major, the row count -- not a multiple
-// of 8) or refused by the driver; the caller stages with threads instead.
+// 16-byte aligned, ld not a multiple of 8) or refused by the driver; the
+// caller stages with threads instead.
 bool operand_map(CUtensorMap *map, const void *base, int ld, int rows, int K, int tile_rows, bool kmajor)
 {
     EncodeTiledFn fn = nn_encoder();
-    if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) || ld % 8 || K % 8 || K <= 0 || rows <= 0) return false;
-    const cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r;
-    if (kmajor) {
-        if (ld < K) return false;
-        const cuuint64_t dims[3] = {8, (cuuint64_t)rows, (cuuint64_t)(K / 8)};
-        const cuuint64_t strides[2] = {(cuuint64_t)ld * 2, 16};
-        const cuuint32_t box[3] = {8, (cuuint32_t)tile_rows, 8};
-        r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    } else {
-        if (rows % 8 || ld < rows) return false;
-        const cuuint64_t dims[4] = {8, 8, (cuuint64_t)(rows / 8), (cuuint64_t)(K / 8)};
-        const cuuint64_t strides[3] = {(cuuint64_t)ld * 2, 16, (cuuint64_t)ld * 16};
-        const cuuint32_t box[4] = {8, 8, (cuuint32_t)(tile_rows / 8), 8};
-        r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void *>(base), dims, strides, box, estr,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    }
+    if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) || ld % 8 || K <= 0 || rows <= 0) return false;
+    if (ld < (kmajor ? K : rows)) return false;
+    const cuuint32_t estr[2] = {1, 1};
+    const cuuint64_t dims[2] = {(cuuint64_t)(kmajor ? K : rows), (cuuint64_t)(kmajor ? rows : K)};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {64, (cuuint32_t)(kmajor ? tile_rows : TK)};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
 
@@ -942,6 +938,13 @@ int tma_gemm(int transA, int transB, int M, int N, int K, const void *A, int lda
     }
     int *err = nullptr;
     NNCK(cudaGetSymbolAddress(reinterpret_cast<void **>(&err), g_tc_err));
+    const int tiles = ((N + TN2 - 1) / TN2) * ((M + TM - 1) / TM);
+    if (splits > 1) {
+        // the caller accepted an atomic split-K: take enough splits for about
+        // 2 CTAs per SM, each with at least 4 K steps
+        const int want = (2 * kNumSMs + tiles - 1) / tiles, by_k = K / (4 * TK);
+        splits = std::max(splits, std::min(want, by_k));
+    }
     int kps;
     splits = split_k(K, splits, TK, &kps);
     if (splits > 1) {
@@ -957,10 +960,9 @@ int tma_gemm(int transA, int transB, int M, int N, int K, const void *A, int lda
     return AMHD_OK;
 }
 
-// shapes on which the tcgen05 pipeline beats mma.sync (B200): a 128-row MMA
-// tile that is mostly filled and more than one K step per tile, or a long K
-// (weight gradients); the narrow layers (M = 32, 64) stay on mma.sync
-bool prefer_tc(int M, int N, int K) { return (M >= 128 && K >= 128 && N >= 64) || K >= 4096; }
+// shapes on which the tcgen05 pipeline beats mma.sync (B200): at least half a
+// 128-row MMA tile, or a long K (weight gradients)
+bool prefer_tc(int M, int N, int K) { return (M >= 64 && N >= 64) || K >= 4096; }
 
 }  // namespace
 

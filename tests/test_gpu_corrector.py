@@ -71,8 +71,9 @@ def test_tcgen05_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
 
 
 def test_tcgen05_gemm_operand_paths():
-    """Aligned operands go through the TMA pipeline, a K that is not a multiple
-    of 8 through thread staging; both agree with the float64 matmul."""
+    """Operands whose leading dimension is a multiple of 8 go through the TMA
+    pipeline (also with a K that is not: the ragged K step reads zeros past
+    K), others through thread staging; all agree with the float64 matmul."""
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200._tensors import stream_ptr
     import ctypes
@@ -82,13 +83,14 @@ def test_tcgen05_gemm_operand_paths():
         _lib.call("amhd_nn_gemm_tc_paths", ctypes.byref(t), ctypes.byref(s))
         return t.value, s.value
 
-    for (M, N, K), expect in (((128, 256, 128), (1, 0)), ((128, 256, 90), (0, 1))):
+    for (M, N, K, lda), expect in (((128, 256, 128, 128), (1, 0)), ((128, 256, 90, 90), (0, 1)),
+                                   ((136, 200, 100, 104), (1, 0))):
         g = torch.Generator(device="cuda").manual_seed(K)
-        A = bf(torch.randn((M, K), device="cuda", generator=g))
+        A = bf(torch.randn((M, lda), device="cuda", generator=g))[:, :K]
         B = bf(torch.randn((K, N), device="cuda", generator=g))
         C = torch.zeros((M, N), device="cuda")
         t0, s0 = paths()
-        _lib.call("amhd_nn_gemm_tc", 0, 0, M, N, K, A.data_ptr(), K, B.data_ptr(), N, C.data_ptr(), N, 1.0, 0.0, 1,
+        _lib.call("amhd_nn_gemm_tc", 0, 0, M, N, K, A.data_ptr(), lda, B.data_ptr(), N, C.data_ptr(), N, 1.0, 0.0, 1,
                   stream_ptr())
         torch.cuda.synchronize()
         t1, s1 = paths()
