@@ -5,8 +5,10 @@ channels, ~0.63 M parameters) maps a coarse solution (the 9 conserved fields
 plus psi, normalised per channel) to a correction that moves it toward the
 fine-grid solution restricted onto the coarse grid (4x4 block averages).
 
-Every convolution is an im2col + GEMM on the BF16 tensor cores (mma.sync
-m16n8k16, FP32 accumulation); forward, backward (data and weight gradients),
+Every convolution is an im2col + GEMM on the BF16 tensor cores with FP32
+accumulation (amhd_nn_gemm: tcgen05.mma fed by TMA for the wide layers,
+mma.sync m16n8k16 for the narrow first one); forward, backward (data and
+weight gradients),
 bias/ReLU, pooling, upsampling, the loss and Adam are the library's own
 kernels (amhd_nn_* in include/aeromhd.h).  Weights keep an FP32 master copy;
 their BF16 copy feeds the GEMMs.  PyTorch only allocates the buffers.

@@ -1,7 +1,8 @@
-// amhd_nn.cu -- kernels of the learned coarse-grid corrector: a BF16
-// tensor-core GEMM (mma.sync m16n8k16, FP32 accumulation) that carries every
-// convolution (im2col form), and the element-wise, pooling, loss and Adam
-// kernels of its training and inference.
+// amhd_nn.cu -- kernels of the learned coarse-grid corrector: the BF16
+// tensor-core GEMMs (FP32 accumulation) that carry every convolution (im2col
+// form) -- tcgen05.mma with the accumulator in tensor memory, operands by
+// TMA, and mma.sync m16n8k16 for the shapes it suits better -- and the
+// element-wise, pooling, loss and Adam kernels of its training and inference.
 //
 // Activations are FP32 in [C][B*H*W] layout (channel-major: the output of a
 // GEMM W[Cout][K] x col[K][N] is the next layer's input as is); GEMM operands
