@@ -88,6 +88,43 @@ def step_cfg(bcx, bcy, By, **kw):
              powell_source=True, bc_x_type=bcx, bc_y_type=bcy, glm_alpha=1.5, **kw)
 
 
+@pytest.mark.parametrize("bcx,bcy", [("periodic", "periodic"), ("extrapolation", "outflow"),
+                                     ("characteristic", "periodic")])
+@pytest.mark.parametrize("nx,ny", [(2, 2), (3, 40), (40, 3), (5, 7), (2, 33)])
+def test_smallest_grids_bit_exact(amhd, oracle, nx, ny, bcx, bcy):
+    """Grids down to 2 x 2 interior cells (ghost layers as wide as the
+    interior, a single short marching item, lanes mostly past the edge):
+    three float64 steps of a seeded random state, Powell and GLM on, equal bit
+    for bit to the oracle's, dt and ch included."""
+    O = oracle
+    cfg = C(nx=nx, ny=ny, x_min=0.0, x_max=0.1 * nx, y_min=0.0, y_max=0.1 * ny, cfl=0.3, gamma=5.0 / 3.0,
+            B_transverse=0.5, powell_source=True, bc_x_type=bcx, bc_y_type=bcy, glm_alpha=1.5)
+    rng = np.random.default_rng(nx * 100 + ny)
+    shape = (nx + 4, ny + 4)
+    W = np.zeros((10,) + shape)
+    W[0] = 1.0 + 0.3 * rng.random(shape)
+    W[1:4] = 0.3 * rng.standard_normal((3,) + shape)
+    W[4:7] = 0.5 * rng.standard_normal((3,) + shape)
+    W[7] = 1.0 + 0.3 * rng.random(shape)
+    W[9] = rng.random(shape)
+    U0 = O.prim_to_cons(W, cfg.gamma)
+    s = amhd.solver.MHDSolver(cfg)
+    s.U = U0.copy()
+    o = O.OracleSolver(C(**{f: getattr(cfg, f) for f in ("nx", "ny", "x_min", "x_max", "y_min", "y_max", "cfl",
+                                                          "gamma", "B_transverse", "powell_source", "bc_x_type",
+                                                          "bc_y_type", "glm_alpha")}))
+    o.U = U0.copy()
+    for n in range(3):
+        s.dt = s.compute_dt(amhd.physics.cons_to_prim(s.U, cfg.gamma))
+        s.step_ssprk3()
+        o.dt = o.compute_dt(O.cons_to_prim(o.U, o.cfg.gamma))
+        o.step_ssprk3()
+        assert s.dt == o.dt, (n, s.dt, o.dt)
+        assert s.cfg.glm_ch == o.cfg.glm_ch
+    got = np_(s.U)
+    assert np.array_equal(got, o.U), float(np.abs(got - o.U).max())
+
+
 # 4, 8, 16: tiled kernel; negative: warp-marching kernel with that many rows per work item
 @pytest.mark.parametrize("tile_x", [8, 4, 16, -4, -6, -24, -64])
 @pytest.mark.parametrize("k", range(len(STEP_CASES)))
