@@ -58,8 +58,10 @@ def parse_args(argv=None):
                          "or 0 (the library default: marching, 24 rows in fp32, 16 in fp64)")
     ap.add_argument("--decomp", action="store_true",
                     help="one n x n grid split over the ranks by x rows (strong scaling) instead of replicas")
-    ap.add_argument("--ensemble", type=int, default=0,
-                    help="also time the batched shock-interface ensemble of this many instances")
+    ap.add_argument("--ensemble", type=int, default=256,
+                    help="also time the batched shock-interface ensemble of this many instances (0: skip)")
+    ap.add_argument("--ensemble-tune", action="store_true",
+                    help="choose the ensemble's work shape, order and grid with the autotuner first")
     return ap.parse_args(argv)
 
 
@@ -475,11 +477,11 @@ def run_ensemble(a, world):
     ens.initialize()
     ens.start()
     tuned = None
-    if a.tile_x == 0:
+    if a.ensemble_tune and a.tile_x == 0:
         # work shape, order and grid chosen by the autotuner (untimed; fresh cache)
         best, timings = tune_ensemble(ens, steps=5, cache=Cache())
         tuned = {"candidates": len(timings), "best_ms_per_step": round(min(timings.values()) / 5 * 1e3, 4)}
-    k = max(3, a.steps // 2)
+    k = max(3, min(a.steps // 5, 200))
     ens.advance(k)  # warm-up + graph capture
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
