@@ -108,3 +108,12 @@ def test_work_shapes_and_counts():
     cfgs = [Config(nx=100, ny=60), Config(nx=64, ny=28)]
     assert list(tile_counts(cfgs, 8)) == [13 * 2, 8 * 1]
     assert list(tile_counts(cfgs, -32)) == [4 * 3, 2 * 1]
+
+
+def test_ensemble_default_geometry():
+    """An ensemble starts with 32-row marching items in float32 and the
+    library default (16 rows) in float64."""
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200.ensemble import default_tile_x
+    assert default_tile_x("fp32") == -32
+    assert default_tile_x("fp64") == _lib.default_tile_x("fp64") == -16
