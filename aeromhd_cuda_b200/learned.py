@@ -11,10 +11,10 @@ coarse grid (4x4 block averages), the coarse solver advances it by delta, and
 the pair (that coarse state, the fine state at t_k + delta restricted) is
 kept; the target is their difference.  Runs use the frame of the shocked gas
 so that the mixing layer stays in the domain until t = 3.  Seeds split 90/10
-into training and validation; separate test seeds judge the result.
+into training and validation; separate test seeds measure the result.
 
 Use: a corrected coarse run adds the corrector's output every `delta` of
-simulated time (all instances of an ensemble together).  It is judged
+simulated time (all instances of an ensemble together).  It is measured
 against the plain fine solve on mixing width, spectral energy and div B; an
 instance falls back to the plain fine solve when its corrected run leaves the
 trusted range (non-finite or far out-of-range corrections, a correction that
