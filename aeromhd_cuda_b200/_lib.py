@@ -97,6 +97,7 @@ _SIGS = {
     "amhd_ensemble_advance": ([_P, _I32, _P, _P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _I32, _P, _P], _c.c_int),
     "amhd_ensemble_tensormaps": ([_P, _I32, _I32, _I32, _P, _P, _P, _P], _c.c_int),
     "amhd_set_tma": ([_I32], _c.c_int),
+    "amhd_selftest_wait": ([_I32, _I64, _P, _P], _c.c_int),
     "amhd_ensemble_continue": ([_P, _P, _I32, _I32, _P, _P, _D, _P], _c.c_int),
     "amhd_ensemble_init": ([_P, _P, _I32, _I32, _P, _P, _D, _I64, _P], _c.c_int),
     "amhd_nn_last_error": ([], _c.c_char_p),

@@ -12,6 +12,7 @@
 
 #include "aeromhd.h"
 #include "amhd_launch.h"
+#include "amhd_tma.cuh"
 
 using namespace amhd;
 
@@ -233,6 +234,22 @@ int control_upload(amhd_control *ctl, double t, double t_end, int64_t step, int6
     return AMHD_OK;
 }
 
+// one thread waits on a CTA-local mbarrier that expects one arrival: after
+// arriving itself (the wait must succeed) or with nothing arriving (the wait
+// must give up after limit_ns); out = {gave up, microseconds waited}
+__global__ void selftest_wait_kernel(int arrive, uint64_t limit_ns, int32_t *out)
+{
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    amhd::tma::mbar_init(&bar, 1);
+    if (arrive) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(amhd::tma::smem_addr(&bar)) : "memory");
+    const uint64_t t0 = amhd::tma::globaltimer_ns();
+    const bool done = amhd::tma::wait_for(&bar, 0u, limit_ns, amhd::tma::kTmaWaitIters);
+    const uint64_t us = (amhd::tma::globaltimer_ns() - t0) / 1000u;
+    out[0] = done ? 0 : 1;
+    out[1] = us > 0x7fffffffull ? 0x7fffffff : (int32_t)us;
+}
+
 using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                    const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -312,6 +329,23 @@ int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm)
 int amhd_set_tma(int32_t on)
 {
     g_use_tma = on ? 1 : 0;
+    return AMHD_OK;
+}
+
+int amhd_selftest_wait(int32_t arrive, int64_t limit_ns, int32_t *timed_out, int32_t *waited_us)
+{
+    if (limit_ns <= 0 || limit_ns > 2000000000LL || !timed_out || !waited_us)
+        return fail(AMHD_ERR_ARG, "limit_ns must be in (0, 2e9] and the outputs non-NULL");
+    int32_t *d = nullptr;
+    CK(cudaMalloc(reinterpret_cast<void **>(&d), 2 * sizeof(int32_t)));
+    selftest_wait_kernel<<<1, 32>>>(arrive ? 1 : 0, (uint64_t)limit_ns, d);
+    cudaError_t e = cudaGetLastError();
+    int32_t h[2] = {-1, -1};
+    if (e == cudaSuccess) e = cudaMemcpy(h, d, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(AMHD_ERR_CUDA, "selftest_wait: %s", cudaGetErrorString(e));
+    *timed_out = h[0];
+    *waited_us = h[1];
     return AMHD_OK;
 }
 

@@ -19,6 +19,7 @@
 #include <string>
 
 #include "aeromhd.h"
+#include "amhd_tma.cuh"
 
 namespace {
 
@@ -184,6 +185,7 @@ __global__ void __launch_bounds__(128) gemm_bf16_kernel(int transA, int transB, 
 constexpr int TM = 128, TN = 128, TK = 64;
 __device__ int g_tc_err;  // set when an MMA wait gave up (amhd_nn_gemm_status reads and clears it)
 constexpr uint32_t kTcWaitIters = 1u << 24;
+constexpr uint64_t kTcWaitNs = 1000000000ull;  // 1 s
 constexpr int kTcSmemBytes = 66 * 1024;  // > 228 KB / 4: at most 3 CTAs per SM (3 x 128 TMEM columns)
 
 // Each operand tile is stored in the layout of its source: K-major, element
@@ -249,19 +251,10 @@ __device__ __forceinline__ uint64_t tc_desc(const void *start, uint32_t lbo_byte
 constexpr uint32_t kTcIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
                               ((uint32_t)(TM >> 4) << 24);
 
+// bounded wait on an mbarrier phase: 1 s, or kTcWaitIters polls
 __device__ __forceinline__ bool tc_wait(uint64_t *bar, uint32_t parity)
 {
-    const uint32_t a = tc_smem_addr(bar);
-    for (uint32_t it = 0; it < kTcWaitIters; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-            : "=r"(done)
-            : "r"(a), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
+    return amhd::tma::wait_for(bar, parity, kTcWaitNs, kTcWaitIters);
 }
 
 __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, int M, int N, int K, const bf16 *A,

@@ -348,6 +348,15 @@ int amhd_nn_gemm_tc_paths(int64_t *tma, int64_t *staged);
  * N >= 64, or K >= 4096 -- when the operands qualify, mma.sync otherwise;
  * 1 always mma.sync; 2 always amhd_nn_gemm_tc. */
 int amhd_nn_set_gemm_path(int32_t mode);
+
+/* Self-test of the bounded device waits every kernel of this library uses on
+ * an mbarrier (TMA staging, tensor-core completion; no counterpart in the
+ * reference).  One thread waits on a shared-memory mbarrier after arriving on
+ * it itself (arrive != 0: the wait must succeed) or with nothing arriving (the
+ * wait must give up after limit_ns, 0 < limit_ns <= 2e9, and say so):
+ * *timed_out = 1 when it gave up, *waited_us = how long it waited.  The
+ * context stays usable either way.  Synchronous. */
+int amhd_selftest_wait(int32_t arrive, int64_t limit_ns, int32_t *timed_out, int32_t *waited_us);
 int amhd_nn_gemm(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K, const void *A, int32_t lda,
                  const void *B, int32_t ldb, float *C, int32_t ldc, float alpha, float beta, int32_t splits,
                  void *stream);

@@ -365,6 +365,23 @@ def test_nonfinite_state_is_reported_not_trapped(amhd):
     assert s2.step == 3 and np.isfinite(np_(s2.U)).all()
 
 
+def test_bounded_device_wait_gives_up_and_reports(amhd):
+    """The mbarrier wait the TMA and tensor-core kernels use, on a barrier that
+    nothing arrives at: it gives up after its limit (20 ms here), reports it to
+    the host, and the context stays usable; on a barrier that has completed it
+    returns at once.  No GPU fault is involved: the wait is a bounded loop."""
+    t, w = ctypes.c_int32(-1), ctypes.c_int32(-1)
+    amhd.lib.call("amhd_selftest_wait", 0, 20_000_000, ctypes.byref(t), ctypes.byref(w))
+    assert t.value == 1, "the wait did not report giving up"
+    assert 0 <= w.value < 2_000_000, w.value  # bounded: well under the 1 s production limit x 2
+    amhd.lib.call("amhd_selftest_wait", 1, 20_000_000, ctypes.byref(t), ctypes.byref(w))
+    assert t.value == 0 and w.value < 20_000, (t.value, w.value)
+    x = torch.arange(8, device="cuda", dtype=torch.float64)
+    assert float(x.sum().item()) == 28.0
+    with pytest.raises(amhd.lib.AmhdError):
+        amhd.lib.call("amhd_selftest_wait", 0, 0, ctypes.byref(t), ctypes.byref(w))
+
+
 def test_device_argument_errors(amhd):
     from aeromhd_cuda_b200 import _tensors
     s = amhd.solver.MHDSolver(ot_cfg(32))
