@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(128) gemm_tc_kernel(int transA, int transB, in
 // marks the CTA, which still waits (bounded) for its loads and MMAs in flight
 // and frees its TMEM columns.
 // ---------------------------------------------------------------------------
-constexpr int kTmaStages = 4, TN2 = 64;
+constexpr int kTmaStages = 3, TN2 = 64;  // 74 KB per CTA: 3 CTAs per SM (4 stages, 2 per SM, ran 1.2-2.4x slower)
 constexpr int kNumSMs = 148;
 constexpr int kTmaABytes = TM * TK * 2, kTmaBBytes = TN2 * TK * 2;
 
