@@ -34,6 +34,7 @@ def default_tile_x(precision: str) -> int:
 AMHD_FLAG_NONFINITE = 1
 AMHD_FLAG_DT_TINY = 2
 AMHD_FLAG_PAUSED = 4
+AMHD_FLAG_TIMEOUT = 8
 
 _c = ctypes
 _I32, _I64, _D, _P, _U32, _U64 = _c.c_int32, _c.c_int64, _c.c_double, _c.c_void_p, _c.c_uint32, _c.c_uint64
@@ -53,7 +54,7 @@ class Control(_c.Structure):
 
 class Instance(_c.Structure):
     _fields_ = [("grid", Grid), ("offset", _I64), ("first_tile", _I32), ("tiles_x", _I32), ("tiles_y", _I32),
-                ("pad_", _I32)]
+                ("cut_x", _I32)]
 
 
 class AmhdError(RuntimeError):
@@ -93,7 +94,7 @@ _SIGS = {
     "amhd_diagnostics_colour": ([_c.POINTER(Grid), _P, _D, _P, _P, _P, _P], _c.c_int),
     "amhd_control_init_split": ([_c.POINTER(Grid), _P, _P, _D, _D, _I64, _I64, _P], _c.c_int),
     "amhd_advance_stage": ([_c.POINTER(Grid), _I32, _P, _P, _P, _P, _P], _c.c_int),
-    "amhd_advance_finish": ([_c.POINTER(Grid), _P, _P, _I32, _P], _c.c_int),
+    "amhd_advance_finish": ([_c.POINTER(Grid), _P, _P, _I32, _I32, _P], _c.c_int),
     "amhd_ensemble_advance": ([_P, _I32, _P, _P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _I32, _P, _P], _c.c_int),
     "amhd_ensemble_tensormaps": ([_P, _I32, _I32, _I32, _P, _P, _P, _P], _c.c_int),
     "amhd_set_tma": ([_I32], _c.c_int),
@@ -162,6 +163,31 @@ def call(name: str, *args) -> None:
     if rc != AMHD_OK and name.startswith("amhd_nn_"):
         raise AmhdError(rc, lib().amhd_nn_last_error().decode(errors="replace"))
     check(rc)
+
+
+def check_control(c, where: str = "run loop") -> None:
+    """Raise on the control flags after which a state must not be used.
+
+    AMHD_FLAG_NONFINITE (a step wrote a non-finite value) raises
+    FloatingPointError; AMHD_FLAG_TIMEOUT (a bounded device wait gave up, so
+    a tile of the state was not updated) raises AmhdError(AMHD_ERR_TIMEOUT).
+    The run loop's finalize kernel stops an instance whose flags carry either."""
+    if c.flags & AMHD_FLAG_TIMEOUT:
+        raise AmhdError(AMHD_ERR_TIMEOUT, f"{where}: a bounded device wait expired at step {c.step}, t={c.t}; "
+                                          "tiles of the state were not updated")
+    if c.flags & AMHD_FLAG_NONFINITE:
+        raise FloatingPointError(f"{where}: non-finite state at step {c.step}, t={c.t}")
+
+
+def check_gemm_status(where: str = "corrector") -> None:
+    """Read (and clear) the tensor-core GEMM wait flag; raise if a GEMM gave up.
+
+    A tcgen05 GEMM whose bounded wait expired skips its epilogue, leaving its
+    output unwritten; nothing else reports it.  The call synchronises."""
+    flag = _I32(0)
+    call("amhd_nn_gemm_status", _c.byref(flag))
+    if flag.value:
+        raise AmhdError(AMHD_ERR_TIMEOUT, f"{where}: a tensor-core GEMM wait expired; its output was not written")
 
 
 def padded_layout(nx: int, ny: int, dtype_code: int):

@@ -245,8 +245,15 @@ class Corrector:
             _lib.call("amhd_nn_adam", ptr(P["b"]), ptr(P["gb"]), ptr(P["mb"]), ptr(P["vb"]), None,
                       P["b"].numel(), lr, beta1, beta2, eps, self.t, 0.0, st)
 
+    def check_gemm_status(self) -> None:
+        """Raise if a tensor-core GEMM of the work queued so far gave up its bounded
+        wait (its output then was not written).  Synchronises; the training loop
+        calls it once per epoch, loss() and correct_state() on every call."""
+        _lib.check_gemm_status("corrector")
+
     def train_step(self, x: torch.Tensor, target: torch.Tensor, B: int, lr: float = 1e-3) -> torch.Tensor:
-        """One Adam step on mean squared error; returns the loss (device scalar, before the step)."""
+        """One Adam step on mean squared error; returns the loss (device scalar, before
+        the step).  Asynchronous: check_gemm_status() reports a GEMM that gave up."""
         out = self.forward(x, B)
         dout = self._buf("dout", out.shape)
         loss = self._buf("loss", (1,))
@@ -261,6 +268,7 @@ class Corrector:
         loss = self._buf("loss", (1,))
         loss.zero_()
         _lib.call("amhd_nn_mse", ptr(out), ptr(target), out.numel(), None, ptr(loss), stream_ptr())
+        self.check_gemm_status()
         return float(loss.item())
 
     # ------------------------------------------------- solver interaction
@@ -275,6 +283,7 @@ class Corrector:
         x = self._buf("infer.x", (10, N))
         _lib.call("amhd_nn_pack", grid, ptr(state), ptr(self.in_mean), ptr(self.in_istd), ptr(x), N, 0, stream_ptr())
         y = self.forward(x, 1)
+        self.check_gemm_status()  # an unwritten output must not reach the state
         _lib.call("amhd_nn_apply", grid, ptr(state), ptr(self.out_scale), ptr(y), N, 0, stream_ptr())
 
     def correct_solver(self, solver) -> None:

@@ -674,11 +674,14 @@ int amhd_advance_stage(const amhd_grid *g, int32_t stage, void *U, void *U1, voi
     return AMHD_OK;
 }
 
-int amhd_advance_finish(const amhd_grid *g, void *U, amhd_control *ctl, int32_t advance, void *stream)
+int amhd_advance_finish(const amhd_grid *g, void *U, amhd_control *ctl, int32_t advance, int32_t cut_x,
+                        void *stream)
 {
     if (int e = check_grid(g)) return e;
     if (!U || !ctl) return fail(AMHD_ERR_ARG, "NULL argument");
-    const amhd_instance one = single_instance(g, tile_of(g));
+    if (cut_x < 0 || cut_x > 3) return fail(AMHD_ERR_ARG, "cut_x must be a mask of bits 0 and 1, got %d", cut_x);
+    amhd_instance one = single_instance(g, tile_of(g));
+    one.cut_x = cut_x;
     CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, advance ? 1 : 0, 0, S(stream)));
     return AMHD_OK;
 }
@@ -789,6 +792,7 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
         out_host[2] = r.ch;
         out_host[3] = r.e_bnd;
     }
+    if (r.flags & AMHD_FLAG_TIMEOUT) return fail(AMHD_ERR_TIMEOUT, "a bounded device wait expired; tiles not updated");
     if (r.flags & AMHD_FLAG_NONFINITE) return fail(AMHD_ERR_NONFINITE, "non-finite value in the new state");
     return AMHD_OK;
 }

@@ -1195,14 +1195,14 @@ __global__ void dt_reduce_kernel(const Layout l, const R *A, int from_prim, doub
 
 // _compute_boundary_energy_flux, solver.py:225-240: one block sums both columns
 template <typename R>
-__device__ double boundary_flux_block(const amhd_grid &g, const R *U)
+__device__ double boundary_flux_block(const amhd_grid &g, const R *U, int cut_x = 0)
 {
     __shared__ double part[2][32];
     const int nyt = g.ny + 2 * NG;
     const int cols[2] = {NG, g.nx + NG - 1};
     double acc[2] = {0.0, 0.0};
     for (int s = 0; s < 2; ++s)
-        for (int j = NG + threadIdx.x; j < nyt - NG; j += blockDim.x) {
+        for (int j = NG + threadIdx.x; j < nyt - NG && !(cut_x >> s & 1); j += blockDim.x) {
             const int64_t c = (int64_t)cols[s] * g.pitch + j;
             double u[NV], w[NV];
 #pragma unroll
@@ -1274,7 +1274,10 @@ __global__ void finalize_kernel(const amhd_instance *insts, const amhd_instance 
                 ctl->last_dt = ctl->dt;
                 ctl->step += 1;
             }
-            const bool loop_on = set_only || (ctl->t < ctl->t_end && ctl->step < ctl->max_steps);
+            // a step that wrote a non-finite value, or whose bounded wait gave up and
+            // left tiles stale, ends the loop: the host reads the flag and raises
+            const bool healthy = !(ctl->flags & (AMHD_FLAG_NONFINITE | AMHD_FLAG_TIMEOUT));
+            const bool loop_on = set_only || (healthy && ctl->t < ctl->t_end && ctl->step < ctl->max_steps);
             if (loop_on) {
                 // compute_dt, solver.py:213-223 (max cf = sqrt of max cf^2; max(cf, ch) == ch)
                 double cf_max = sqrt(__longlong_as_double((long long)ctl->red[0]));
@@ -1315,7 +1318,7 @@ __global__ void finalize_kernel(const amhd_instance *insts, const amhd_instance 
     }
     __syncthreads();
     if (go) {
-        double bf = boundary_flux_block(g, U);  // solver.py:316-317
+        double bf = boundary_flux_block(g, U, in.cut_x);  // solver.py:316-317
         if (threadIdx.x == 0) ctl->e_bnd += bf * dt_next;
     }
 }

@@ -1,12 +1,33 @@
 // amhd_launch_impl.cuh -- definitions of Launch<R>; included once per
 // precision translation unit, which then instantiates Launch<R>.
 #pragma once
+#include <atomic>
+#include <cstdint>
 #include <cstring>
 #include <utility>
 
 #include "amhd_kernels.cuh"
 
 namespace amhd {
+
+// A set-up step that must run once per device (kernel function attributes such
+// as the shared-memory opt-in are per device): one bit per device ordinal.
+// Two threads may both run the step for the same device; it is idempotent.
+struct PerDeviceOnce {
+    std::atomic<uint64_t> done{0};
+    template <typename F>
+    cudaError_t run(F &&step)
+    {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        const uint64_t bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+        if (bit && (done.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+        e = step();
+        if (e == cudaSuccess) done.fetch_or(bit, std::memory_order_acq_rel);
+        return e;
+    }
+};
 
 static inline int elem_blocks(int64_t n, int threads = 256)
 {
@@ -32,22 +53,15 @@ size_t Launch<R>::stage_smem(int tile_x)
     }
 }
 
-// shared-memory opt-in of one stage instantiation, set once per process
-template <typename R, int TX, int ST>
-struct StageConfigured {
-    static bool done;
-};
-template <typename R, int TX, int ST>
-bool StageConfigured<R, TX, ST>::done = false;
-
+// shared-memory opt-in of one stage instantiation, set once per device
 template <typename R, int TX, int ST>
 static cudaError_t configure_t()
 {
-    if (StageConfigured<R, TX, ST>::done) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(rk_stage_kernel<R, TX, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(TileSmem<R, TX>));
-    if (e == cudaSuccess) StageConfigured<R, TX, ST>::done = true;
-    return e;
+    static PerDeviceOnce once;
+    return once.run([] {
+        return cudaFuncSetAttribute(rk_stage_kernel<R, TX, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(TileSmem<R, TX>));
+    });
 }
 
 template <typename R, int TX, int ST>
@@ -114,13 +128,12 @@ static cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 bl
 template <typename R, int ST>
 static cudaError_t launch_march_t(const StageParams &p, int grid, cudaStream_t s)
 {
-    static bool configured = false;  // shared-memory opt-in, once per process
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(march_stage_kernel<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)kMarchSmem<R>);
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    static PerDeviceOnce once;  // shared-memory opt-in, once per device
+    cudaError_t e = once.run([] {
+        return cudaFuncSetAttribute(march_stage_kernel<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kMarchSmem<R>);
+    });
+    if (e != cudaSuccess) return e;
     if (p.pdl) return launch_dependent(march_stage_kernel<R, ST>, dim3(grid), dim3(kMarchThreads), kMarchSmem<R>, s, p);
     march_stage_kernel<R, ST><<<grid, kMarchThreads, kMarchSmem<R>, s>>>(p);
     return cudaGetLastError();

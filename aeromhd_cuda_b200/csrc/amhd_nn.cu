@@ -925,11 +925,9 @@ int tma_gemm(int transA, int transB, int M, int N, int K, const void *A, int lda
     CUtensorMap map_a, map_b;
     if (K <= 0 || !operand_map(&map_a, A, lda, M, K, TM, a_kmajor) || !operand_map(&map_b, B, ldb, N, K, TN2, b_kmajor))
         return AMHD_OK;
-    static bool configured = false;
-    if (!configured) {
-        NNCK(cudaFuncSetAttribute(gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmemBytes));
-        configured = true;
-    }
+    // function attributes are per device: set on every call (cheap), so that any
+    // device current in this thread has the opt-in before the launch
+    NNCK(cudaFuncSetAttribute(gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmaSmemBytes));
     int *err = nullptr;
     NNCK(cudaGetSymbolAddress(reinterpret_cast<void **>(&err), g_tc_err));
     const int tiles = ((N + TN2 - 1) / TN2) * ((M + TM - 1) / TM);
@@ -971,11 +969,9 @@ int amhd_nn_gemm_tc(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_
 {
     if (M < 0 || N < 0 || K < 0 || !A || !B || !C) return nn_fail(AMHD_ERR_ARG, "bad gemm arguments");
     if (M == 0 || N == 0) return AMHD_OK;
-    static bool configured = false;
-    if (!configured) {
-        NNCK(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes));
-        configured = true;
-    }
+    // function attributes are per device: set on every call (cheap), so that any
+    // device current in this thread has the opt-in before the launch
+    NNCK(cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmemBytes));
     cudaStream_t s = S(stream);
     bool launched = false;
     const int rc = tma_gemm(transA, transB, M, N, K, A, lda, B, ldb, C, ldc, alpha, beta, splits, s, &launched);

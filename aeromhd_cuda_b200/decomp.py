@@ -15,15 +15,18 @@ the device loop taken apart (amhd_advance_stage / amhd_advance_finish):
     CFL maxima    -- max-all-reduce of ctl->red[4] (ordered float64 bits, so an
                      int64 max is exact) over the ranks
     finish        -- t, step, and the next dt / ch / psi damping from the
-                     global maxima, identical on every rank
+                     global maxima, identical on every rank; the boundary
+                     energy (solver.py:225-240, :316-317) of the block's
+                     physical x sides only (the cut sides are masked), so the
+                     sum over the ranks is the whole grid's
 
 Every cell's arithmetic sees the same inputs as in the unsplit grid, so the
 split run reproduces the single-grid run bit for bit (state, t, dt).  The
 exchange is point-to-point (torch.distributed isend/irecv: NCCL over NVLink
 between GPUs, gloo between CPU processes in tests); each rank talks to two
-neighbours only.  The boundary-energy diagnostic is not accumulated by split
-runs (a rank cannot tell its physical boundary columns from the cut ones in
-the finalize step).
+neighbours only.  The boundary energy is accumulated per rank on the sides
+that are physical boundaries; its sum over the ranks equals the unsplit
+grid's to rounding (the two sides are added per rank instead of per step).
 
 The reference runs one grid on one GPU; this has no counterpart there.
 """
@@ -52,6 +55,12 @@ def split_rows(nx: int, world: int) -> List[Tuple[int, int]]:
         out.append((r0, r0 + n))
         r0 += n
     return out
+
+
+def cut_sides(r0: int, r1: int, nx: int) -> int:
+    """Mask of a block's x sides that are cuts between blocks rather than the
+    grid's boundary: bit 0 its first row (r0 > 0), bit 1 its last (r1 < nx)."""
+    return (1 if r0 > 0 else 0) | (2 if r1 < nx else 0)
 
 
 def neighbours(rank: int, world: int, periodic: bool) -> Tuple[Optional[int], Optional[int]]:
@@ -148,6 +157,7 @@ class GpuBackend:
         from .solver import MHDSolver
         self._lib, self._ptr, self._stream = _lib, ptr, stream_ptr
         self.n = r1 - r0
+        self.cut_x = cut_sides(r0, r1, cfg.nx)
         local = replace(cfg, nx=self.n, x_min=cfg.x_min + r0 * cfg.dx, x_max=cfg.x_min + r1 * cfg.dx)
         self.solver = MHDSolver(local)
         s = self.solver
@@ -177,7 +187,7 @@ class GpuBackend:
     def finish(self, advance: int) -> None:
         s = self.solver
         self._lib.call("amhd_advance_finish", self.grid, self._ptr(s._U), self._ptr(s._ctl), int(advance),
-                       self._stream())
+                       int(self.cut_x), self._stream())
 
     def control(self):
         from ._tensors import read_controls
@@ -253,3 +263,13 @@ class DecomposedSolver:
             self.loop.step()
         c = self.backend.control()
         self.t, self.step = float(c.t), int(c.step)
+
+    def boundary_energy(self) -> float:
+        """The whole grid's cumulative boundary energy (solver.py:225-240, :316-317):
+        the sum over the ranks of each block's physical sides.  A collective:
+        every rank calls it."""
+        import torch.distributed as dist
+        e = torch.tensor([float(self.backend.control().e_bnd)], dtype=torch.float64, device=self.U.device)
+        if self.world > 1:
+            dist.all_reduce(e, op=dist.ReduceOp.SUM, group=self.group)
+        return float(e.item())

@@ -311,9 +311,8 @@ class Ensemble:
         for _ in range(max_chunks):
             self.advance(chunk)
             c = self.controls()
-            if any(x.flags & _lib.AMHD_FLAG_NONFINITE for x in c):
-                bad = [k for k, x in enumerate(c) if x.flags & _lib.AMHD_FLAG_NONFINITE]
-                raise FloatingPointError(f"non-finite state in instances {bad[:8]}")
+            for k, x in enumerate(c):
+                _lib.check_control(x, f"Ensemble.run, instance {k}")
             if not any(x.active for x in c):
                 break
         return np.array([x.step for x in self.controls()])

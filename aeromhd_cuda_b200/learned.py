@@ -180,6 +180,7 @@ def train(X: torch.Tensor, Y: torch.Tensor, train_seeds: Sequence[int], val_seed
             x = norm.inputs(tr[idx])
             t = norm.targets(ttr[idx])
             losses.append(net.train_step(x, t, batch, lr=sched(ep)))
+        net.check_gemm_status()  # once per epoch: a GEMM that gave up invalidates the epoch
         tl = float(torch.stack([l.reshape(()) for l in losses]).mean()) if losses else float("nan")
         vl = []
         for b0 in range(0, va.shape[0], batch):
@@ -444,6 +445,7 @@ def _apply_batch(net: Corrector, norm: Normaliser, e: Ensemble, idx, corr_sigma:
         _lib.call("amhd_nn_pack", e._grid(i), ptr(e.state(i)), ptr(net.in_mean), ptr(net.in_istd), ptr(x), B * N,
                   int(b), stream_ptr())
     y = net.forward(x, B)
+    net.check_gemm_status()  # an unwritten GEMM output must not reach the states
     if getattr(net, "project_y", False):
         y = project_rows(y.view(10, B, net.H, net.W)).reshape(10, B * N).contiguous()
     lim = (norm.out_max * corr_sigma).view(10, 1, 1)

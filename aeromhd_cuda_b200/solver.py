@@ -357,8 +357,7 @@ class MHDSolver:
         while True:
             self._advance(chunk, graph)
             c = self._read_loop_state()
-            if c.flags & _lib.AMHD_FLAG_NONFINITE:
-                raise FloatingPointError(f"non-finite state at step {self.step}, t={self.t}")
+            _lib.check_control(c, "MHDSolver.advance")
             if not c.active:
                 break
         self._loop_ready = False
@@ -381,8 +380,7 @@ class MHDSolver:
             n = min(cfg.diag_interval - self.step % cfg.diag_interval, 200 - self.step % 200)
             self._advance(n)
             c = self._read_loop_state()
-            if c.flags & _lib.AMHD_FLAG_NONFINITE:
-                raise FloatingPointError(f"non-finite state at step {self.step}, t={self.t}")
+            _lib.check_control(c, "MHDSolver.run")
             if self.step % cfg.diag_interval == 0:
                 self.compute_diagnostics()
             for st in cfg.snapshot_times:

@@ -20,6 +20,14 @@ over ranks, value = zone-updates of all ranks / that time.
 ``--impl reference`` times the reference scheme on the host cores (the
 float64 CPU restatement under oracle/, all OpenMP threads) on the same
 workload and prints the same JSON line with "impl": "reference".
+
+The default line also carries the reference's own modules, unchanged,
+timed on the same workload by baseline/run_reference.py in a child process:
+``reference_cupy_shim`` (its CuPy path on this GPU, torch standing in for
+CuPy, its HLLD kernel string compiled by NVRTC) and ``reference_numpy_shim``
+(on the host cores, numpy standing in for CuPy; a 512^2 sample), or an
+"unavailable" reason when the reference modules are not installed in
+baseline/_ref.
 """
 from __future__ import annotations
 
@@ -52,6 +60,8 @@ def parse_args(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-reference-paths", action="store_true",
+                    help="skip timing the reference's own modules on the GPU and on the host cores")
     ap.add_argument("--tma", type=int, default=1, help="stage tiles with TMA (1) or 128-bit loads (0)")
     ap.add_argument("--tile-x", type=int, default=0,
                     help="stage kernel geometry: 4, 8, 16 (tiled kernel rows), negative (warp-marching rows) "
@@ -123,7 +133,7 @@ def profile_traffic(tile_x):
 class ClockSampler:
     """NVML clock / throttle-reason sampling during the timed region (read only)."""
 
-    def __init__(self, device_index: int, period_s: float = 0.002):
+    def __init__(self, device_index: int, period_s: float = 0.0005):
         self.samples = []
         self.period = period_s
         self._stop = threading.Event()
@@ -149,10 +159,14 @@ class ClockSampler:
                 mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
                 reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
                 util = nv.nvmlDeviceGetUtilizationRates(self.h).gpu
-                self.samples.append((mhz, reasons, util))
+                self.samples.append((mhz, reasons, util, time.perf_counter()))
             except Exception:
                 pass
             self._stop.wait(self.period)
+
+    def mark(self, name):
+        """Host time stamp of a point of the run (the timed region's ends)."""
+        setattr(self, name, time.perf_counter())
 
     def __enter__(self):
         if self.ok:
@@ -179,12 +193,19 @@ class ClockSampler:
         }
         loaded = [s for s in self.samples if s[2] >= 50] or self.samples
         seen = set()
-        for _, r, _ in loaded:
+        for _, r, _, _ in loaded:
             for k, bit in names.items():
                 if r & bit:
                     seen.add(k)
-        return {"sm_mhz": statistics.median(s[0] for s in loaded), "sm_max_mhz": self.max_mhz,
-                "reasons": sorted(seen), "samples": len(loaded)}
+        t0, t1 = getattr(self, "timed_start", None), getattr(self, "timed_end", None)
+        timed = [x for x in self.samples if t0 is not None and t1 is not None and t0 <= x[3] <= t1]
+        out = {"sm_mhz": statistics.median(x[0] for x in loaded), "sm_max_mhz": self.max_mhz,
+               "reasons": sorted(seen), "samples": len(loaded),
+               "window": "from the warm-up to the end of the profiled steps (same workload)",
+               "samples_in_timed_region": len(timed)}
+        if timed:
+            out["sm_mhz_timed_region"] = statistics.median(x[0] for x in timed)
+        return out
 
 
 # ------------------------------------------------------------ distributed
@@ -292,30 +313,35 @@ def run_ours(a, world, rank, local):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1)
 
-    if a.warmup > 0:
-        advance(a.warmup)
-        advance_profiled(min(a.warmup, 3))
-    torch.cuda.synchronize()
-    barrier(world)
-    torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clk:
+        if a.warmup > 0:
+            advance(a.warmup)
+            advance_profiled(min(a.warmup, 3))
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        clk.mark("timed_start")
         loop_ms = advance(a.steps)
-    barrier(world)
-    total_ms = max_over_ranks(loop_ms, world)
-    # up to 200 more steps with an event after every launch, for the stage times
-    prof_steps = max(1, min(a.steps, 200))
-    prof = advance_profiled(prof_steps)
-    torch.cuda.synchronize()
+        clk.mark("timed_end")
+        barrier(world)
+        total_ms = max_over_ranks(loop_ms, world)
+        # up to 200 more steps with an event after every launch: how the step splits over the kernels
+        prof_steps = max(1, min(a.steps, 200))
+        prof = advance_profiled(prof_steps)
+        torch.cuda.synchronize()
     c = _tensors.read_controls(s._ctl)[0]
-    if c.flags & _lib.AMHD_FLAG_NONFINITE:
-        raise SystemExit("non-finite state during the benchmark")
+    _lib.check_control(c, "benchmark")
     value = world * cells * a.steps / (total_ms / 1e3)
 
-    # roofline of the fused stage kernel: 80 state values per zone-update per step
+    # roofline of the fused stage kernel: 80 state values per zone-update per step.
+    # achieved: the algorithmic bytes of a step over the timed region's time per step
+    # (the whole step, finalize and launch overlap included: a lower bound for the
+    # stage kernels alone); the profiled loop gives the split over the kernels.
     hbm, hbm_kind = peaks()
     stage_ms = prof[0] + prof[1] + prof[2]
     alg_bytes_step = 80 * es * cells
-    achieved = alg_bytes_step * prof_steps / (stage_ms / 1e3) / 1e9
+    achieved = alg_bytes_step / (total_ms / a.steps / 1e3) / 1e9
+    achieved_stages = alg_bytes_step * prof_steps / (stage_ms / 1e3) / 1e9
     tr = profile_traffic(tx)
     traffic = None
     if tr.get("precision") == a.precision and tr.get("n"):
@@ -333,6 +359,8 @@ def run_ours(a, world, rank, local):
                 "frac": round(achieved / hbm, 4), "traffic": traffic, "peak_kind": hbm_kind,
                 "kernel": stage_kernel_name(tx) + " (3 launches/step)", "sm_utilisation": limiter,
                 "algorithmic_bytes_per_step": alg_bytes_step,
+                "achieved_from": "timed region: algorithmic bytes per step / ms per step (whole step)",
+                "achieved_stage_kernels_only": round(achieved_stages, 1),
                 "ms_per_step": {"stage1": prof[0] / prof_steps, "stage2": prof[1] / prof_steps,
                                 "stage3_fused_dt": prof[2] / prof_steps, "finalize": prof[3] / prof_steps},
                 "stage_times": f"{prof_steps} steps with an event after every launch (no launch overlap)"}
@@ -340,33 +368,7 @@ def run_ours(a, world, rank, local):
     # ---- end to end: host state in pinned memory, one C-ABI call per step
     e2e = None
     if a.e2e_steps > 0:
-        host = torch.empty((10, n + 4, n + 4), dtype=s.dtype).pin_memory()
-        host.copy_(s.U.cpu())
-        out = (ctypes.c_double * 4)()
-        t_now = float(c.t)
-
-        def e2e_step(t):
-            _lib.call("amhd_step_host", g, host.data_ptr(), _tensors.ptr(s._U), _tensors.ptr(s._U1),
-                      _tensors.ptr(s._U2), _tensors.ptr(s._ctl), t, cfg.t_end, out, stream)
-            return out[0]
-
-        for _ in range(2):
-            t_now = e2e_step(t_now)
-        torch.cuda.synchronize()
-        barrier(world)
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev0.record()
-        for _ in range(a.e2e_steps):
-            t_now = e2e_step(t_now)
-        ev1.record()
-        torch.cuda.synchronize()
-        e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), world)
-        state_bytes = 10 * (n + 4) * (n + 4) * es
-        ctl_bytes = ctypes.sizeof(_lib.Control)
-        e2e = {"value": world * cells * a.e2e_steps / (e2e_ms / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": state_bytes + ctl_bytes, "d2h_bytes_per_step": state_bytes + ctl_bytes,
-               "ms_per_step": e2e_ms / a.e2e_steps,
-               "path": "amhd_step_host: pinned host state -> device, one run-loop step, -> host"}
+        e2e = run_e2e(s, a.e2e_steps, world)
 
     # ---- float64 side by side (shorter run)
     fp64 = None
@@ -389,6 +391,8 @@ def run_ours(a, world, rank, local):
         _lib.call("amhd_advance_profile", *p64, k64p, ms, stream)
         fp64 = {"value": world * cells * k64 / (t64 / 1e3), "steps": k64,
                 "stage_hbm_frac": round(80 * 8 * cells * k64p / ((ms[0] + ms[1] + ms[2]) / 1e3) / 1e9 / hbm, 4)}
+        if a.e2e_steps > 0:
+            fp64["e2e"] = run_e2e(s64, a.e2e_steps, world)
         del s64
 
     ens_line = None
@@ -396,10 +400,16 @@ def run_ours(a, world, rank, local):
         ens_line = run_ensemble(a, world)
 
     cpu = None
+    ref_gpu = ref_host = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         rate, k, el, cores = cpu_oracle_rate(512, target_s=10.0)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"float64 CPU restatement (oracle/), Orszag-Tang 512x512, {k} steps in {el:.1f} s"}
+    if rank == 0 and world == 1 and not a.no_reference_paths:
+        # the reference's own modules, unchanged, on the same GPU (its CuPy path with
+        # torch standing in for CuPy) and on the host cores (numpy standing in)
+        ref_gpu = reference_path("torch", n, steps=3, warmup=1, device=f"cuda:{torch.cuda.current_device()}")
+        ref_host = reference_path("numpy", 512, steps=2, warmup=1)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
@@ -413,6 +423,7 @@ def run_ours(a, world, rank, local):
                                "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads")},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": loop_launches(tx, a.steps),
         "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
+        "reference_cupy_shim": ref_gpu, "reference_numpy_shim": ref_host,
         # the metric's "learned vs plain" half: not timed here (training takes minutes)
         "learned": {"timed": False, "corrector": "python -m aeromhd_cuda_b200.learned",
                     "status": "not used by default: corrected 256x64 runs are 7-17x faster than the "
@@ -420,6 +431,66 @@ def run_ours(a, world, rank, local):
                               "below the plain coarse run's (0.28), so the plain solve stands"},
     }
     return line
+
+
+def run_e2e(s, steps, world):
+    """Zone-updates/s through the host-buffer entry point (amhd_step_host): every step
+    copies the state from pinned host memory to the device, advances one run-loop
+    step and copies it back, timed with events on the launching stream."""
+    import torch
+    from aeromhd_cuda_b200 import _lib, _tensors
+    cfg, g, stream = s.cfg, s._grid(), _tensors.stream_ptr()
+    host = torch.empty(tuple(s.U.shape), dtype=s.dtype).pin_memory()
+    host.copy_(s.U.cpu())
+    out = (ctypes.c_double * 4)()
+    t_now = float(s.t)
+
+    def e2e_step(t):
+        _lib.call("amhd_step_host", g, host.data_ptr(), _tensors.ptr(s._U), _tensors.ptr(s._U1),
+                  _tensors.ptr(s._U2), _tensors.ptr(s._ctl), t, cfg.t_end, out, stream)
+        return out[0]
+
+    for _ in range(2):
+        t_now = e2e_step(t_now)
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(steps):
+        t_now = e2e_step(t_now)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    state_bytes = host.numel() * host.element_size()
+    ctl_bytes = ctypes.sizeof(_lib.Control)
+    return {"value": world * cfg.nx * cfg.ny * steps / (ms / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": state_bytes + ctl_bytes, "d2h_bytes_per_step": state_bytes + ctl_bytes,
+            "ms_per_step": ms / steps, "precision": cfg.precision,
+            "path": "amhd_step_host: pinned host state -> device, one run-loop step, -> host"}
+
+
+def reference_path(backend, n, steps, warmup, device="cuda"):
+    """The reference's modules, unchanged, timed in a child process by
+    baseline/run_reference.py (main.py:66-73 loop on Orszag-Tang n x n, float64)."""
+    import subprocess
+    cmd = [sys.executable, os.path.join(ROOT, "baseline", "run_reference.py"), "--backend", backend,
+           "--device", device, "--n", str(n), "--steps", str(steps), "--warmup", str(warmup)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+        line = json.loads(r.stdout.strip().splitlines()[-1]) if r.stdout.strip() else {}
+    except Exception as e:
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    if r.returncode != 0 or not line:
+        return {"unavailable": f"exit {r.returncode}: {r.stderr.strip()[-300:]}"}
+    if "unavailable" in line:
+        return line
+    label = ("the reference's CuPy path on this GPU, torch standing in for CuPy, its HLLD kernel "
+             "string compiled by NVRTC" if backend == "torch" else
+             "the reference on the host cores, numpy standing in for CuPy, its HLLD kernel string "
+             "compiled as host C++ with OpenMP")
+    return {"value": line["zone_updates_per_s"], "unit": UNIT, "label": label, "n": n, "steps": steps,
+            "ms_per_step": line["ms_per_step"], "dtype": "f64", "stand_in": line["stand_in"],
+            "host_threads": line["host_threads"], "finite": line["finite"]}
 
 
 def run_decomp(a, world, rank):

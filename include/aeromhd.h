@@ -54,7 +54,8 @@ extern "C" {
 #define AMHD_FLAG_NONFINITE 1   /* a non-finite value was written by a step */
 #define AMHD_FLAG_DT_TINY 2     /* dt <= 1e-16 stopped the loop (solver.py:479) */
 #define AMHD_FLAG_PAUSED 4      /* loop paused at a snapshot time (amhd_control.snap_t) */
-#define AMHD_FLAG_TIMEOUT 8     /* a bounded device wait (TMA completion) expired */
+#define AMHD_FLAG_TIMEOUT 8     /* a bounded device wait (TMA completion) expired; finalize
+                                   stops the loop on this flag and on AMHD_FLAG_NONFINITE */
 
 /* Grid and physics parameters of one instance (reference Config,
  * config.py:47-89, flattened; dx, dy precomputed as config.py:78-84 does). */
@@ -215,14 +216,20 @@ int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *
  *     ch and the psi damping from ctl, ghost cells of the output filled;
  *   amhd_advance_finish -- advance = 1: t += dt, step += 1 (as at the end of
  *     an amhd_advance iteration), then in both cases dt / ch / damping / the
- *     stop flags from ctl->red, which is cleared.
+ *     stop flags from ctl->red, which is cleared, and the boundary energy of
+ *     the block's physical x sides into ctl->e_bnd (non-periodic x;
+ *     solver.py:225-240, :316-317).  cut_x marks the sides that are cuts
+ *     between blocks and carry no boundary flux: bit 0 the block's first
+ *     row, bit 1 its last row (0 for a whole grid).  The whole grid's
+ *     boundary energy is the sum of the blocks' e_bnd.
  * amhd_advance(n) == n x (stage 1, 2, 3, finish(1)).  Asynchronous.  No
  * counterpart in the reference. */
 int amhd_control_init_split(const amhd_grid *g, void *U, amhd_control *ctl, double t, double t_end, int64_t step,
                             int64_t max_steps, void *stream);
 int amhd_advance_stage(const amhd_grid *g, int32_t stage, void *U, void *U1, void *U2, amhd_control *ctl,
                        void *stream);
-int amhd_advance_finish(const amhd_grid *g, void *U, amhd_control *ctl, int32_t advance, void *stream);
+int amhd_advance_finish(const amhd_grid *g, void *U, amhd_control *ctl, int32_t advance, int32_t cut_x,
+                        void *stream);
 /* amhd_advance with a CUDA event recorded after every launch: ms_out[0..3]
  * receive the summed device time of the stage-1, stage-2, stage-3 and
  * finalize launches, ms_out[4] the whole interval.  Synchronises.  For
@@ -235,7 +242,8 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
  * advances one SSP-RK3 step, and copies the new state back into U_host.
  * out_host (may be NULL) receives {t + dt, dt, glm_ch, boundary energy
  * flux x dt}.  dev_U/dev_U1/dev_U2 and ctl are caller device buffers (padded
- * layout).  Returns AMHD_ERR_NONFINITE if the new state holds a NaN/Inf.
+ * layout).  Returns AMHD_ERR_NONFINITE if the new state holds a NaN/Inf,
+ * AMHD_ERR_TIMEOUT if a bounded device wait gave up (tiles not updated).
  * Synchronises. */
 int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, void *dev_U2, amhd_control *ctl,
                    double t, double t_end, double *out_host, void *stream);
@@ -261,16 +269,17 @@ int amhd_diagnostics_colour(const amhd_grid *g, const void *U, double x0, const 
                             double *pos_dev, void *stream);
 
 /* The same diagnostics for callers that cannot allocate device memory: a
- * caller running inside CUDA stream capture (where an allocation is not a
- * capturable operation), a host framework that owns every device allocation
- * and hands plugins only their inputs and outputs, or a loop with a strict
- * time budget that must not risk an allocation synchronising the device.
- * No counterpart in the reference.  The row scratch is a fixed device array
- * compiled into this library (room for nx <= AMHD_NOALLOC_MAX_NX interior
- * rows; larger grids get AMHD_ERR_ARG); it is resident on every GPU that
- * loads the library until the process exits.  The first call on a device
- * looks the array up (cudaGetSymbolAddress) and must be made with that
- * device current and before any stream capture that contains later calls.
+ * host framework that owns every device allocation and hands its plugins
+ * only their inputs and outputs, or a loop with a strict time budget that
+ * must not risk an allocation synchronising the device.  No counterpart in
+ * the reference.  The row scratch is a fixed device array compiled into this
+ * library (room for nx <= AMHD_NOALLOC_MAX_NX interior rows; larger grids
+ * get AMHD_ERR_ARG); it is resident on every GPU that loads the library until
+ * the process exits.  The first call on a device looks the array up
+ * (cudaGetSymbolAddress) and must be made with that device current and
+ * before any stream capture that contains later calls; the address is kept
+ * per device ordinal for the life of the process, so after a
+ * cudaDeviceReset of that device this entry point must not be called again.
  * All calls share the one array: calls whose kernels may overlap on the GPU
  * (different streams without ordering) race on it.  out_dev: 7 doubles as
  * for amhd_diagnostics.  Asynchronous. */
@@ -285,7 +294,9 @@ typedef struct amhd_instance {
     int64_t offset;          /* element offset of plane 0, row 0, col 0          */
     int32_t first_tile;      /* index of the instance's first tile in the list   */
     int32_t tiles_x, tiles_y;/* tiles of this instance (tile_x rows x 32 cols)   */
-    int32_t pad_;
+    int32_t cut_x;           /* x sides that are cuts, not boundaries (bit 0 the
+                                first row, bit 1 the last): excluded from the
+                                boundary energy; 0 for a whole grid             */
 } amhd_instance;
 
 /* Advance every active instance of a packed ensemble by n_steps run-loop

@@ -20,6 +20,29 @@ def golden(name):
     return np.load(os.path.join(GOLDEN, name))
 
 
+def baseline_refshim():
+    """baseline/refshim.py, loaded under its own module name (tests/golden has a
+    refshim module of its own)."""
+    import importlib.util
+    mod = sys.modules.get("amhd_baseline_refshim")
+    if mod is None:
+        spec = importlib.util.spec_from_file_location("amhd_baseline_refshim",
+                                                      os.path.join(ROOT, "baseline", "refshim.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["amhd_baseline_refshim"] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_available() -> bool:
+    """Are the reference's modules installed (baseline/_ref) or named by AMHD_REFERENCE_DIR?"""
+    try:
+        baseline_refshim().reference_dir()
+        return True
+    except FileNotFoundError:
+        return False
+
+
 @pytest.fixture(scope="session")
 def oracle():
     from oracle import oracle as O

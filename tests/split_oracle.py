@@ -6,7 +6,8 @@ with its ghosts as given (oracle compute_rhs with x ghosts left alone), the
 scalar clamp, psi damping on stage 3, then the local boundary fill; stage 3
 and the loop start collect the CFL maxima (ordered float64 bits); finish
 restates the device finalize (t, step, dt = min(cfl / max speed, t_end - t),
-ch, damping)."""
+ch, damping, and the boundary energy of the block's physical x sides,
+solver.py:225-240)."""
 import ctypes
 import math
 
@@ -29,14 +30,32 @@ def _val(b):
 
 class OracleBackend:
     def __init__(self, cfg, r0, r1):
-        from aeromhd_cuda_b200.config import bc_x_code, bc_y_code
+        from aeromhd_cuda_b200.config import BC_PERIODIC, bc_x_code, bc_y_code
+        from aeromhd_cuda_b200.decomp import cut_sides
         self.cfg = cfg
         self.n = r1 - r0
+        self.cut_x = cut_sides(r0, r1, cfg.nx)
+        self.periodic_x = bc_x_code(cfg) == BC_PERIODIC
         self.bc_x, self.bc_y = bc_x_code(cfg), bc_y_code(cfg)
         shape = (10, self.n + 2 * NG, cfg.ny + 2 * NG)
         self.bufs = tuple(torch.zeros(shape, dtype=torch.float64) for _ in range(3))
         self._red = torch.zeros(4, dtype=torch.int64)
-        self.c = dict(t=0.0, t_end=0.0, dt=0.0, ch=0.0, decay=1.0, step=0, max_steps=0, active=0)
+        self.c = dict(t=0.0, t_end=0.0, dt=0.0, ch=0.0, decay=1.0, step=0, max_steps=0, active=0, e_bnd=0.0)
+
+    def _boundary_flux(self, U):
+        """solver.py:225-240 on the block's physical sides: the flux in through
+        its first row minus the flux out through its last."""
+        g, dy = self.cfg.gamma, self.cfg.dy
+        W = O.cons_to_prim(U, g)
+
+        def side(i):
+            w, e = W[:, i, NG:-NG], U[7, i, NG:-NG]
+            pt = w[7] + 0.5 * (w[4] ** 2 + w[5] ** 2 + w[6] ** 2)
+            vb = w[1] * w[4] + w[2] * w[5] + w[3] * w[6]
+            return float(np.sum(((e + pt) * w[1] - w[4] * vb) * dy))
+        left = 0.0 if self.cut_x & 1 else side(NG)
+        right = 0.0 if self.cut_x & 2 else side(self.n + NG - 1)
+        return left - right
 
     def state(self, k):
         return self.bufs[k]
@@ -57,7 +76,7 @@ class OracleBackend:
         self._red.copy_(torch.maximum(self._red, m))
 
     def control_init_split(self, t, t_end, step, max_steps):
-        self.c.update(t=t, t_end=t_end, step=step, max_steps=max_steps, active=1, decay=1.0)
+        self.c.update(t=t, t_end=t_end, step=step, max_steps=max_steps, active=1, decay=1.0, e_bnd=0.0)
         self._red.zero_()
         self._maxima(self.bufs[0], interior=False)
         self._fill(self.bufs[0])
@@ -106,6 +125,8 @@ class OracleBackend:
             dt = min(c["t_end"] - c["t"], dtc)
             c.update(ch=ch, dt=dt, active=int(dt > 1e-16),
                      decay=math.exp(-cfg.glm_alpha * ch * dt / min(cfg.dx, cfg.dy)))
+            if c["active"] and not self.periodic_x:
+                c["e_bnd"] += self._boundary_flux(self.bufs[0].numpy()) * dt
         else:
             c["active"] = 0
         self._red.zero_()

@@ -112,8 +112,8 @@ def test_config_matches_reference_dataclass_when_available():
     import sys
     sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
     import refshim
-    if not os.path.isdir(refshim.REFERENCE_DIR):
-        pytest.skip("reference checkout not present")
+    if refshim.REFERENCE_DIR is None:
+        pytest.skip("reference modules not available")
     code = (
         "import sys; sys.path[:0] = [%r, %r]\n"
         "import refshim\n"

@@ -100,6 +100,13 @@ def test_split_loop_equals_single_block(world, bcx):
         p.join(timeout=60)
         assert p.exitcode == 0
     rows = split_rows(cfg.nx, world)
+    # boundary energy: the ranks' physical sides add up to the single block's
+    e_split = sum(c["e_bnd"] for _, _, c in parts)
+    if bcx == "periodic":
+        assert e_split == one.c["e_bnd"] == 0.0
+    else:
+        assert one.c["e_bnd"] != 0.0
+        assert abs(e_split - one.c["e_bnd"]) <= 1e-12 * abs(one.c["e_bnd"]), (e_split, one.c["e_bnd"])
     for rank, U, c in parts:
         r0, r1 = rows[rank]
         assert c["step"] == one.c["step"] == steps

@@ -3,7 +3,8 @@ device loop (amhd_advance) bit for bit.  (2) Two and three blocks of one grid
 advanced in lockstep in one process -- the GPU stages of every block, then the
 ghost-row exchange and the CFL max reduction done here by plain copies --
 equal the unsplit grid bit for bit, so the multi-GPU run (the same stages,
-with NCCL doing the copies and the reduction) does too."""
+with NCCL doing the copies and the reduction) does too; their boundary
+energies add up to the unsplit grid's."""
 import pytest
 import torch
 
@@ -45,6 +46,7 @@ def test_one_rank_split_loop_equals_device_loop(name, precision):
     d.advance(25)
     assert d.step == a.step == 25 and d.t == a.t
     assert torch.equal(d.gather_state(), a.U)
+    assert d.boundary_energy() == a._cumulative_boundary_energy
 
 
 @pytest.mark.parametrize("world", [2, 3])
@@ -95,3 +97,10 @@ def test_blocks_in_lockstep_equal_unsplit_grid(name, world):
         c = b.control()
         assert c.step == steps and c.t == a.t
         assert torch.equal(b.state(0), a.U[:, r0:r1 + 2 * NG])
+    # boundary energy: only the first and the last block hold physical x sides
+    e_split = sum(float(b.control().e_bnd) for b in bs)
+    e_ref = a._cumulative_boundary_energy
+    if periodic:
+        assert e_split == e_ref == 0.0
+    else:
+        assert e_ref != 0.0 and abs(e_split - e_ref) <= 1e-12 * abs(e_ref), (e_split, e_ref)

@@ -365,6 +365,26 @@ def test_nonfinite_state_is_reported_not_trapped(amhd):
     assert s2.step == 3 and np.isfinite(np_(s2.U)).all()
 
 
+def test_timeout_flag_stops_the_loop_and_raises(amhd):
+    """AMHD_FLAG_TIMEOUT (a bounded wait gave up and left tiles stale), planted
+    in the control block on the host: the finalize kernel ends the loop after
+    the step in which it is seen, and the host check raises AmhdError."""
+    from aeromhd_cuda_b200 import _lib, _tensors, initial_conditions as ic
+    s = amhd.solver.MHDSolver(ot_cfg(32, precision="fp32"))
+    s.set_primitive(ic.orszag_tang(s))
+    s._loop_init(1.0, 100)
+    c = _tensors.read_controls(s._ctl)[0]
+    assert c.active == 1
+    c.flags |= _lib.AMHD_FLAG_TIMEOUT
+    _tensors.write_controls(s._ctl, [c])
+    s._advance(4, graph=False)
+    c = _tensors.read_controls(s._ctl)[0]
+    assert c.active == 0 and c.step == 1, (c.active, c.step)
+    with pytest.raises(_lib.AmhdError) as e:
+        _lib.check_control(c)
+    assert e.value.code == _lib.AMHD_ERR_TIMEOUT
+
+
 def test_bounded_device_wait_gives_up_and_reports(amhd):
     """The mbarrier wait the TMA and tensor-core kernels use, on a barrier that
     nothing arrives at: it gives up after its limit (20 ms here), reports it to

@@ -1,8 +1,8 @@
 """amhd_diagnostics_noalloc: the diagnostics entry point for callers that may
-not allocate device memory (for example code running under CUDA stream
-capture, or a host framework that owns all device memory and only passes its
-plugins inputs and outputs).  Its row scratch is a fixed array inside the
-library instead of a caller buffer.
+not allocate device memory (a host framework that owns all device memory and
+only passes its plugins inputs and outputs, or a loop that must not risk an
+allocation synchronising the device).  Its row scratch is a fixed array
+inside the library instead of a caller buffer.
 
 Checked through the C ABI against amhd_diagnostics (caller-provided scratch)
 on two calls in a row on different states, so that the second call also
@@ -42,8 +42,12 @@ def test_noalloc_diagnostics_match_the_allocating_entry_point(precision):
         rows = torch.zeros(7 * s.cfg.nx, dtype=torch.float64, device="cuda")
         _lib.call("amhd_diagnostics", g, ptr(s.U), float(s.cfg.x_min), ptr(ref), ptr(rows), stream_ptr())
         got = torch.full((8,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         _lib.call("amhd_diagnostics_noalloc", g, ptr(s.U), float(s.cfg.x_min), ptr(got), stream_ptr())
         torch.cuda.synchronize()
+        if call == 1:  # the first call may load the library's kernels; later calls take no device memory
+            assert torch.cuda.mem_get_info()[0] == free_before
         r, o = ref.cpu().numpy()[:7], got.cpu().numpy()[:7]
         assert np.all(np.isfinite(r)), call
         np.testing.assert_allclose(o, r, rtol=1e-12, atol=0.0, err_msg=f"call {call}")
