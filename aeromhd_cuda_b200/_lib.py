@@ -95,7 +95,8 @@ _SIGS = {
     "amhd_control_init_split": ([_c.POINTER(Grid), _P, _P, _D, _D, _I64, _I64, _P], _c.c_int),
     "amhd_advance_stage": ([_c.POINTER(Grid), _I32, _P, _P, _P, _P, _P], _c.c_int),
     "amhd_advance_finish": ([_c.POINTER(Grid), _P, _P, _I32, _I32, _P], _c.c_int),
-    "amhd_ensemble_advance": ([_P, _I32, _P, _P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _I32, _P, _P], _c.c_int),
+    "amhd_ensemble_advance": ([_P, _I32, _P, _P, _I32, _I32, _I32, _P, _P, _P, _P, _I32, _I32, _P, _P, _P],
+                              _c.c_int),
     "amhd_ensemble_tensormaps": ([_P, _I32, _I32, _I32, _P, _P, _P, _P], _c.c_int),
     "amhd_set_tma": ([_I32], _c.c_int),
     "amhd_selftest_wait": ([_I32, _I64, _P, _P], _c.c_int),

@@ -166,10 +166,11 @@ cudaError_t run_dt_reduce(const amhd_grid *g, const void *A, int from_prim, amhd
 int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instance *insts, const int32_t *tile_inst,
                  int n_tiles, int tile_x, int grid, void *U, void *U1, void *U2, amhd_control *ctl, int use_ctl,
                  double dt, double ch, double decay, int fuse_dt, cudaStream_t s, const int32_t *tile_order = nullptr,
-                 const CUtensorMap *tmaps = nullptr, int n_inst = 1, int defer_fill = 0)
+                 const CUtensorMap *tmaps = nullptr, int n_inst = 1, int defer_fill = 0, int32_t *queue = nullptr)
 {
     StageParams p;
     memset(&p, 0, sizeof p);
+    p.queue = is_march(tile_x) ? queue : nullptr;
     p.inst = insts;
     p.n_inst = n_inst;
     p.pull_ghosts = 1;  // the run loop: U1 and U2 are internal, their ghost cells are never stored
@@ -879,7 +880,7 @@ int amhd_ensemble_continue(const amhd_instance *inst_host, const amhd_instance *
 int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev,
                           const int32_t *tile_order_dev, int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U,
                           void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas,
-                          const void *tmaps_dev, void *stream)
+                          const void *tmaps_dev, int32_t *queue_dev, void *stream)
 {
     if (!inst_dev || !tile_inst_dev || !U || !U1 || !U2 || !ctl_dev || n_inst <= 0 || n_tiles <= 0)
         return fail(AMHD_ERR_ARG, "bad ensemble arguments");
@@ -901,7 +902,8 @@ int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const i
     const int defer = is_march(tile_x);
     for (int k = 0; k < n_steps; ++k) {
         if (int e = three_stages(&gdt, dummy, inst_dev, tile_inst_dev, n_tiles, tile_x, grid, U, U1, U2, ctl_dev, 1, 0,
-                                 0, 1, 1, s, tile_order_dev, static_cast<const CUtensorMap *>(tmaps_dev), n_inst, defer))
+                                 0, 1, 1, s, tile_order_dev, static_cast<const CUtensorMap *>(tmaps_dev), n_inst, defer,
+                                 queue_dev))
             return e;
         CK(run_finalize(dtype, inst_dev, n_inst, dummy, U, ctl_dev, 1, 0, s, defer));
     }

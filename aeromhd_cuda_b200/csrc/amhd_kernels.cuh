@@ -161,8 +161,13 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
     if (g.powell) {
         // _compute_powell_source, solver.py:242-266 (centred face-average divB)
         const PowellIn<R> pw = powell_in();
-        R divb = (R(0.5) * (pw.bxc + pw.bxp) - R(0.5) * (pw.bxm + pw.bxc)) / dx +
-                 (R(0.5) * (pw.byc + pw.byp) - R(0.5) * (pw.bym + pw.byc)) / dy;
+        R divb;
+        if constexpr (kFast<R>)  // float32: reciprocal spacings instead of two divisions
+            divb = (R(0.5) * (pw.bxc + pw.bxp) - R(0.5) * (pw.bxm + pw.bxc)) * float(1.0 / g.dx) +
+                   (R(0.5) * (pw.byc + pw.byp) - R(0.5) * (pw.bym + pw.byc)) * float(1.0 / g.dy);
+        else
+            divb = (R(0.5) * (pw.bxc + pw.bxp) - R(0.5) * (pw.bxm + pw.bxc)) / dx +
+                   (R(0.5) * (pw.byc + pw.byp) - R(0.5) * (pw.bym + pw.byc)) / dy;
         R vb = pw.vx * pw.bxc + pw.vy * pw.byc + pw.vz * pw.bzc;
         rhs[MX] += -divb * pw.bxc;
         rhs[MY] += -divb * pw.byc;
@@ -931,7 +936,16 @@ __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) ma
     const int lane = threadIdx.x & 31;
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int n_warps = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
-    for (int pos = warp; pos < p.n_tiles; pos += n_warps) {
+    // work positions: from the queue (each warp takes the next free position when it
+    // is done with its item, so uneven items leave no warp idle while work remains),
+    // or the static split w, w + n_warps, ...
+    auto next_pos = [&](int prev) {
+        if (p.queue == nullptr) return prev < 0 ? warp : prev + n_warps;
+        int t = 0;
+        if (lane == 0) t = atomicAdd(&p.queue[0], 1);
+        return __shfl_sync(0xffffffffu, t, 0);
+    };
+    for (int pos = next_pos(-1); pos < p.n_tiles; pos = next_pos(pos)) {
         const int item = p.tile_order ? p.tile_order[pos] : pos;
         unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
         bool bad = false;
@@ -949,6 +963,14 @@ __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) ma
                         if (q[k]) atomicMax(reinterpret_cast<unsigned long long *>(&ctl->red[k]), q[k]);
                 if (any_bad) atomicOr(&ctl->flags, AMHD_FLAG_NONFINITE);
             }
+        }
+    }
+    if (p.queue != nullptr && lane == 0) {
+        // every warp has drawn a position past the end before it counts itself out, so
+        // the last one out may reset the queue for the next launch of the stream
+        if (atomicAdd(&p.queue[1], 1) == n_warps - 1) {
+            atomicExch(&p.queue[0], 0);
+            atomicExch(&p.queue[1], 0);
         }
     }
 }

@@ -37,6 +37,9 @@ struct StageParams {
                                    // loop fills them once after its last step, Launch::march_fill)
     int32_t pdl;                   // marching kernel: launch as a programmatic dependent of the
                                    // previous kernel in the stream (run loop)
+    int32_t *queue;                // marching kernel: device work queue {next position, warps
+                                   // finished}, zero between launches; nullptr: warp w takes
+                                   // positions w, w + warps, ... (static split)
 };
 
 // Work geometry of the stage kernels, passed around as one int "tile_x":

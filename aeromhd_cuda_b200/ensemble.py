@@ -155,7 +155,7 @@ def default_tile_x(precision: str) -> int:
 
 class Ensemble:
     def __init__(self, configs: Sequence[Config], tile_x: int = 0, order: str = "instance", ctas: int = -1,
-                 device=None, use_tma: bool = True):
+                 device=None, use_tma: bool = True, dynamic: bool = True):
         if not configs:
             raise ValueError("empty ensemble")
         precs = {c.precision for c in configs}
@@ -180,6 +180,10 @@ class Ensemble:
         self.U1 = torch.zeros_like(self.U)
         self.U2 = torch.zeros_like(self.U)
         self.ctl = control_tensor(self.n, self.device)
+        # work queue of a persistent marching grid: {next position, warps finished},
+        # zero between launches (the kernel's last warp resets it)
+        self.queue = torch.zeros(2, dtype=torch.int32, device=self.device)
+        self.dynamic = bool(dynamic)
         self._graphs = {}
         self.set_schedule(tile_x, order, ctas)
 
@@ -190,9 +194,12 @@ class Ensemble:
         marching kernel), work-list order and grid size (chosen by autotune).
         ctas: -1 (default) = one CTA per tile (tiled) / per 4 work items
         (marching), the hardware handing CTAs to SMs as they free up; 0 = a
-        persistent grid of resident CTAs per SM x SM count, each warp taking
-        every n-th item (on the uneven 256-instance ensemble 20-30 % slower:
-        the static split leaves warps idle at the end)."""
+        persistent grid of resident CTAs per SM x SM count (> 0: that many
+        CTAs).  On a persistent marching grid each warp takes the next free
+        item from a device work queue when it finishes one (``dynamic``,
+        the default); with dynamic=False warp w takes items w, w + warps, ...
+        (on the uneven 256-instance ensemble 20-30 % slower than one CTA per
+        4 items: the static split leaves warps idle at the end)."""
         rows, cols = work_shape(tile_x)
         self.tile_x, self.order, self.ctas = int(tile_x), order, int(ctas)
         counts = tile_counts(self.configs, tile_x)
@@ -268,7 +275,12 @@ class Ensemble:
                   self.tile_order.data_ptr(), self.n_tiles, self.code, self.tile_x, self.U.data_ptr(),
                   self.U1.data_ptr(), self.U2.data_ptr(), self.ctl.data_ptr(), int(n),
                   self.n_tiles if self.ctas < 0 else self.ctas,
-                  self.tmaps_dev.data_ptr() if self.tmaps_dev is not None else None, stream_ptr())
+                  self.tmaps_dev.data_ptr() if self.tmaps_dev is not None else None,
+                  self.queue.data_ptr() if self.uses_queue() else None, stream_ptr())
+
+    def uses_queue(self) -> bool:
+        """Does the stage kernel draw work items from the device queue?"""
+        return self.dynamic and self.ctas >= 0 and self.tile_x < 0
 
     def advance(self, n: int, graph: bool = True):
         """n run-loop steps of every active instance (one graph replay)."""

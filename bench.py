@@ -70,6 +70,8 @@ def parse_args(argv=None):
                     help="one n x n grid split over the ranks by x rows (strong scaling) instead of replicas")
     ap.add_argument("--ensemble", type=int, default=256,
                     help="also time the batched shock-interface ensemble of this many instances (0: skip)")
+    ap.add_argument("--ensemble-ctas", type=int, default=-1,
+                    help="ensemble grid: -1 one CTA per 4 items, 0 persistent (work queue), >0 that many CTAs")
     ap.add_argument("--ensemble-tune", action="store_true",
                     help="choose the ensemble's work shape, order and grid with the autotuner first")
     return ap.parse_args(argv)
@@ -544,7 +546,7 @@ def run_ensemble(a, world):
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200.autotune import Cache, tune_ensemble
     cfgs = draw_configs(a.ensemble, seed=0, t_end=3.0, precision=a.precision)
-    ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=-1, use_tma=bool(a.tma))
+    ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=a.ensemble_ctas, use_tma=bool(a.tma))
     ens.initialize()
     ens.start()
     tuned = None

@@ -305,16 +305,20 @@ typedef struct amhd_instance {
  * buffers; inst and ctl are device arrays.  Tiles are numbered per instance
  * from inst[k].first_tile (tile_x rows x 32 columns, y fastest);
  * tile_inst[tile] is the instance of each tile; tile_order (may be NULL for
- * the identity) is the order in which the persistent CTAs take them
- * (CTA b takes positions b, b + ctas, ...).  ctas is the persistent grid size
- * (0: resident CTAs per SM x SM count).  tmaps_dev: device copy of
+ * the identity) is the order in which work positions are taken.  ctas is the
+ * grid size (0: resident CTAs per SM x SM count).  Without a queue, CTA /
+ * warp b takes positions b, b + ctas (warps), ...  queue_dev (marching
+ * kernel; may be NULL): two device int32 that are zero before the first call
+ * and between launches -- each warp of a persistent grid then takes the next
+ * free position as it finishes an item, and the last warp of a launch resets
+ * the pair; one pair per stream of calls.  tmaps_dev: device copy of
  * amhd_ensemble_tensormaps for this tile_x (NULL: 128-bit loads instead of
  * TMA).  Capturable in a CUDA graph.
  * No counterpart in the reference (one grid per solver there). */
 int amhd_ensemble_advance(const amhd_instance *inst_dev, int32_t n_inst, const int32_t *tile_inst_dev,
                           const int32_t *tile_order_dev, int32_t n_tiles, int32_t dtype, int32_t tile_x, void *U,
                           void *U1, void *U2, amhd_control *ctl_dev, int32_t n_steps, int32_t ctas,
-                          const void *tmaps_dev, void *stream);
+                          const void *tmaps_dev, int32_t *queue_dev, void *stream);
 /* Continue every instance from its current t and step to a new t_end: dt,
  * ch and the loop flags are recomputed from the current states (as
  * amhd_ensemble_init does, but keeping t, step, flags and the boundary

@@ -63,6 +63,32 @@ def test_schedules_give_identical_results(precision):
             assert rel < 1e-6, (tx, rel)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_marching_work_queue_gives_identical_results(precision):
+    """A persistent marching grid whose warps draw items from the device work
+    queue, over several graph replays and eager calls in a row (each launch
+    resets the queue for the next), equals one CTA per 4 items and the static
+    split bit for bit; the queue is back at zero after every call."""
+    from aeromhd_cuda_b200.ensemble import Ensemble
+    cfgs = small_configs(precision, n=5, seed=16)
+    out = []
+    for order, ctas, dynamic in [("instance", -1, True), ("instance", 0, True), ("largest_first", 0, True),
+                                 ("interleave", 37, True), ("instance", 0, False)]:
+        ens = Ensemble(cfgs, tile_x=-16, order=order, ctas=ctas, dynamic=dynamic)
+        assert ens.uses_queue() == (ctas >= 0 and dynamic)
+        ens.initialize()
+        ens.start(max_steps=9)
+        ens.advance(3)
+        ens.advance(3)
+        ens.advance(3, graph=False)
+        torch.cuda.synchronize()
+        assert ens.queue.tolist() == [0, 0], (order, ctas, dynamic)
+        assert all(c.step == 9 for c in ens.controls())
+        out.append(ens.U.clone())
+    for u in out[1:]:
+        assert torch.equal(u, out[0])
+
+
 def test_instances_stop_at_their_end_time():
     from aeromhd_cuda_b200.ensemble import Ensemble
     cfgs = small_configs("fp32", n=4, seed=13)
