@@ -31,6 +31,10 @@ def default_tile_x(precision: str) -> int:
     (float64 runs 2 CTAs per SM, where 16-row items fill whole waves at 2048^2)."""
     return -24 if precision == "fp32" else -16
 
+# amhd_set_tma mode the library starts with: bit 0 the tiled kernel's tile + halo,
+# bit 1 the marching kernel's rows staged by TMA
+DEFAULT_TMA = 1
+
 AMHD_FLAG_NONFINITE = 1
 AMHD_FLAG_DT_TINY = 2
 AMHD_FLAG_PAUSED = 4

@@ -123,12 +123,19 @@ int stage_grid(int dtype, int tile_x, int n_tiles, int ctas_per_sm)
     return grid < n_tiles ? grid : n_tiles;
 }
 
-// stage input: pointer, and its tensor map when TMA staging is on
-void set_input(StageParams &p, const void *uin, const amhd_grid *g, int tile_x)
+// stage input and base state: pointers, and their tensor maps when TMA staging
+// is on for the kernel of this geometry (bit 0 of amhd_set_tma: tiled kernel,
+// bit 1: marching kernel, which also stages the base state's rows)
+void set_input(StageParams &p, const void *uin, const void *u0, const amhd_grid *g, int tile_x)
 {
     p.uin = uin;
+    p.u0 = u0;
     p.use_tma = 0;
-    if (g_use_tma && !is_march(tile_x) && encode_state_map(&p.tmap, uin, g->dtype, g->pitch, g->var_stride, tile_x) == 0) p.use_tma = 1;
+    const int want = is_march(tile_x) ? (g_use_tma & 2) : (g_use_tma & 1);
+    if (!want || encode_state_map(&p.tmap, uin, g->dtype, g->pitch, g->var_stride, tile_x) != 0) return;
+    if (is_march(tile_x) && encode_state_map(&p.tmap_base, u0, g->dtype, g->pitch, g->var_stride, tile_x) != 0)
+        return;
+    p.use_tma = 1;
 }
 
 cudaError_t run_stage(int dtype, int stage, int tile_x, const StageParams &p, int grid, cudaStream_t s)
@@ -195,7 +202,7 @@ int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instan
             p.tmaps = tmaps;
             p.in_buf = st - 1;
         } else {
-            set_input(p, in[st - 1], g, tile_x);
+            set_input(p, in[st - 1], U, g, tile_x);
         }
         p.u0 = U;
         p.uout = out[st - 1];
@@ -280,7 +287,9 @@ int encode_state_map(CUtensorMap *map, const void *base, int dtype, int pitch, i
     const size_t es = elem_size(dtype);
     const cuuint64_t dims[3] = {(cuuint64_t)pitch, (cuuint64_t)(var_stride / pitch), 10};
     const cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)var_stride * es};
-    const cuuint32_t box[3] = {(cuuint32_t)(kTY + 2 * kNG), (cuuint32_t)(tile_x + 2 * kNG), 10};
+    // tiled kernel: the tile and its halo; marching kernel: one row of a 32-lane strip
+    const cuuint32_t box[3] = {(cuuint32_t)(is_march(tile_x) ? 32 : kTY + 2 * kNG),
+                               (cuuint32_t)(is_march(tile_x) ? 1 : tile_x + 2 * kNG), 10};
     const cuuint32_t estr[3] = {1, 1, 1};
     CUresult r = fn(map, dtype == AMHD_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
                     const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -327,9 +336,10 @@ int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm)
     return AMHD_OK;
 }
 
-int amhd_set_tma(int32_t on)
+int amhd_set_tma(int32_t mode)
 {
-    g_use_tma = on ? 1 : 0;
+    if (mode < 0 || mode > 3) return fail(AMHD_ERR_ARG, "TMA mode must be 0..3, got %d", mode);
+    g_use_tma = mode;
     return AMHD_OK;
 }
 
@@ -354,7 +364,7 @@ int amhd_ensemble_tensormaps(const amhd_instance *inst_host, int32_t n_inst, int
                              const void *U, const void *U1, const void *U2, void *maps_host)
 {
     if (!inst_host || n_inst <= 0 || !U || !U1 || !U2 || !maps_host) return fail(AMHD_ERR_ARG, "bad arguments");
-    if (tile_x != 4 && tile_x != 8 && tile_x != 16) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8 or 16 (the marching kernel takes no tensor maps)");
+    if (!valid_geometry(tile_x)) return fail(AMHD_ERR_ARG, "tile_x must be 4, 8, 16 or -1024..-4 (marching rows)");
     const size_t es = elem_size(dtype);
     CUtensorMap *maps = static_cast<CUtensorMap *>(maps_host);
     const void *bufs[3] = {U, U1, U2};
@@ -536,8 +546,7 @@ int amhd_compute_rhs(const amhd_grid *g, void *U, void *R, double ch, void *stre
     const amhd_instance one = single_instance(g, tx);
     StageParams p;
     memset(&p, 0, sizeof p);
-    set_input(p, U, g, tx);
-    p.u0 = U;
+    set_input(p, U, U, g, tx);
     p.uout = R;
     p.one = one;
     p.n_tiles = one.tiles_x * one.tiles_y;
@@ -579,8 +588,7 @@ int amhd_rk_stage(const amhd_grid *g, int32_t stage, const void *Uin, const void
     const amhd_instance one = single_instance(g, tx);
     StageParams p;
     memset(&p, 0, sizeof p);
-    set_input(p, Uin, g, tx);
-    p.u0 = U0;
+    set_input(p, Uin, U0, g, tx);
     p.uout = Uout;
     p.one = one;
     p.n_tiles = one.tiles_x * one.tiles_y;
@@ -663,8 +671,7 @@ int amhd_advance_stage(const amhd_grid *g, int32_t stage, void *U, void *U1, voi
     memset(&p, 0, sizeof p);
     void *in[3] = {U, U1, U2};
     void *out[3] = {U1, U2, U};
-    set_input(p, in[stage - 1], g, tx);
-    p.u0 = U;
+    set_input(p, in[stage - 1], U, g, tx);
     p.uout = out[stage - 1];
     p.one = one;
     p.n_tiles = one.tiles_x * one.tiles_y;
@@ -714,8 +721,7 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
     cudaError_t ce = cudaEventRecord(ev[0], s);
     for (int k = 0; k < n_steps && ce == cudaSuccess; ++k) {
         for (int st = 1; st <= 3 && ce == cudaSuccess; ++st) {
-            set_input(p, st == 1 ? U : (st == 2 ? U1 : U2), g, tx);
-            p.u0 = U;
+            set_input(p, st == 1 ? U : (st == 2 ? U1 : U2), U, g, tx);
             p.uout = st == 1 ? U1 : (st == 2 ? U2 : U);
             p.fuse_dt = st == 3;
             ce = run_stage(g->dtype, st, tx, p, grid, s);

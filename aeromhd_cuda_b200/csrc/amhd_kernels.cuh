@@ -602,14 +602,31 @@ __device__ __forceinline__ void face_flux(R wl[NV], R wr[NV], R gam, float igm1,
 // Every row but fy is private to its lane.
 template <typename R>
 using MarchRow = R[NV / 2][32][2];
-
+// one row of the 10 planes as a TMA box {32 columns, 1 row, 10 planes} lands: plane-major
 template <typename R>
-struct MarchSmem {
+using MarchPlanes = R[NV][32];
+
+// TMA: the staged rows are plane-major boxes written by the tensor-memory
+// accelerator (one copy per row for the whole warp, completion on an mbarrier
+// per slot); otherwise pair-interleaved rows that each lane fills with cp.async
+template <typename R, bool TMA>
+struct MarchSmem;
+template <typename R>
+struct MarchSmem<R, false> {
     MarchRow<R> raw[3];  // conserved stage-input rows i .. i+2 (cp.async), row r in slot r % 3
     MarchRow<R> base;    // U0 of row i when U0 is not the stage input
     MarchRow<R> sx;      // limited x-slope of the current row
     MarchRow<R> fx;      // flux through the x face below the current row
     MarchRow<R> fy;      // flux through each lane's left y face of the current row (read by the lane on the left)
+};
+template <typename R>
+struct __align__(128) MarchSmem<R, true> {
+    MarchPlanes<R> raw[3];  // conserved stage-input rows i .. i+2 (TMA), row r in slot r % 3
+    MarchPlanes<R> base;    // U0 of row i when U0 is not the stage input (TMA)
+    MarchRow<R> sx;
+    MarchRow<R> fx;
+    MarchRow<R> fy;
+    uint64_t bar[4];        // completion of raw[0..2] and base
 };
 
 template <typename R>
@@ -679,10 +696,10 @@ __device__ __forceinline__ void fetch_wait() { asm volatile("cp.async.wait_group
 // One work item: rows [ib, ie) of a 28-column strip.  SPEC: the item runs the
 // van Leer limiter with GLM on (ch > 0), known at compile time -- the walk the
 // solver's loop takes; otherwise both are read at run time.
-template <typename R, int STAGE, bool SPEC>
-__device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &ms, const amhd_instance &in,
-                                           const amhd_grid &g, int item, int lane, double dt, double ch, double decay,
-                                           unsigned long long q[4], bool &bad)
+template <typename R, int STAGE, bool SPEC, bool TMA>
+__device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TMA> &ms, const amhd_instance &in,
+                                           int ii, const amhd_grid &g, int item, int lane, double dt, double ch,
+                                           double decay, unsigned long long q[4], bool &bad, uint32_t &phase)
 {
     const int local = item - in.first_tile;
     const int strip = local % in.tiles_y, chunk = local / in.tiles_y;
@@ -708,6 +725,91 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
     // U0 comes from its own buffer unless it is the stage input (stage 1 of a step)
     const bool own_base = STAGE >= 1 && p.u0 != p.uin;
 
+    // ---- row staging: per-lane cp.async into pair rows, or one TMA box per row
+    const int x0 = j - lane;  // column of lane 0 (28 x strip: 16-byte aligned for 4- and 8-byte values)
+    const CUtensorMap *map_in = nullptr, *map_base = nullptr;
+    if constexpr (TMA) {
+        map_in = p.inst ? &p.tmaps[3 * ii + p.in_buf] : &p.tmap;
+        map_base = p.inst ? &p.tmaps[3 * ii] : &p.tmap_base;
+    }
+    uint32_t pending = 0;  // TMA: slots (bits 0-2) and the base row (bit 3) with a copy in flight
+    bool gave_up = false;
+    auto fetch_in = [&](int slot, int r) {
+        if constexpr (TMA) {
+            __syncwarp();  // every lane is done reading the slot
+            if (lane == 0) {
+                tma::fence_proxy_async();
+                tma::arrive_expect_tx(&ms.bar[slot], (uint32_t)sizeof(MarchPlanes<R>));
+                tma::load_3d(&ms.raw[slot][0][0], map_in, x0, src_row(r), 0, &ms.bar[slot]);
+            }
+            pending |= 1u << slot;
+        } else {
+            fetch_row(ms.raw[slot], uin, vs, (int64_t)src_row(r) * pitch + jl, lane);
+        }
+    };
+    auto fetch_base = [&](int r) {
+        if constexpr (TMA) {
+            __syncwarp();
+            if (lane == 0) {
+                tma::fence_proxy_async();
+                tma::arrive_expect_tx(&ms.bar[3], (uint32_t)sizeof(MarchPlanes<R>));
+                tma::load_3d(&ms.base[0][0], map_base, x0, r, 0, &ms.bar[3]);
+            }
+            pending |= 8u;
+        } else {
+            fetch_row(ms.base, u0, vs, (int64_t)r * pitch + jl, lane);
+        }
+    };
+    // wait for the copies of the slots in `mask` (TMA) or for every copy (cp.async)
+    auto wait_rows = [&](uint32_t mask) {
+        if constexpr (TMA) {
+            mask &= pending;
+            for (int k = 0; k < 4; ++k)
+                if (mask >> k & 1u) {
+                    if (tma::wait(&ms.bar[k], phase >> k & 1u)) {
+                        phase ^= 1u << k;
+                        pending &= ~(1u << k);
+                    } else {
+                        gave_up = true;  // still in flight: the abort path waits for it once more
+                    }
+                }
+        } else {
+            fetch_wait();
+        }
+    };
+    // this lane's column of an input row; in TMA boxes the ghost columns hold what
+    // is stored, so a lane whose column is a ghost the row pulls reads its source
+    const bool fix_col = TMA && pull && (j < NG || j >= NG + g.ny) && j < NG + g.ny + NG;
+    auto load_in = [&](int slot, int r, R u[NV]) {
+        if constexpr (TMA) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u[v] = ms.raw[slot][v][lane];
+            if (fix_col) {
+                const R *src = uin + (int64_t)src_row(r) * pitch + jl;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) u[v] = src[v * vs];
+            }
+        } else {
+            row_load(ms.raw[slot], lane, u);
+        }
+    };
+    auto load_cell = [&](int slot, R u[NV]) {  // interior cells: as staged
+        if constexpr (TMA) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u[v] = ms.raw[slot][v][lane];
+        } else {
+            row_load(ms.raw[slot], lane, u);
+        }
+    };
+    auto load_base = [&](R u[NV]) {
+        if constexpr (TMA) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) u[v] = ms.base[v][lane];
+        } else {
+            row_load(ms.base, lane, u);
+        }
+    };
+
     const R gam = R(g.gamma), chr = R(ch);
     const int lim = SPEC ? AMHD_LIMITER_VANLEER : g.limiter;
     const bool glm = SPEC || chr > R(0);
@@ -722,21 +824,21 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
     // slots they replace, and waits for them just before the x faces.
     int s0 = (ib - 2) % 3;  // slot of row i (ib-2 here)
     const int s1i = s0 == 2 ? 0 : s0 + 1, s2i = s1i == 2 ? 0 : s1i + 1;
-    fetch_row(ms.raw[s0], uin, vs, (int64_t)src_row(ib - 2) * pitch + jl, lane);
-    fetch_row(ms.raw[s1i], uin, vs, (int64_t)src_row(ib - 1) * pitch + jl, lane);
-    fetch_row(ms.raw[s2i], uin, vs, (int64_t)ib * pitch + jl, lane);
-    fetch_wait();
+    fetch_in(s0, ib - 2);
+    fetch_in(s1i, ib - 1);
+    fetch_in(s2i, ib);
+    wait_rows(7u);
     R w0[NV], w1[NV], bxm = R(0);
     {
         R u[NV], wa[NV];
-        row_load(ms.raw[s0], lane, u);
+        load_in(s0, ib - 2, u);
         ghost_psi(ib - 2, u);
         to_prim(u, g.gamma, wa);
-        fetch_row(ms.raw[s0], uin, vs, (int64_t)src_row(ib + 1) * pitch + jl, lane);  // row ib-2 is converted
-        row_load(ms.raw[s1i], lane, u);
+        fetch_in(s0, ib + 1);  // row ib-2 is converted
+        load_in(s1i, ib - 1, u);
         ghost_psi(ib - 1, u);
         to_prim(u, g.gamma, w0);
-        row_load(ms.raw[s2i], lane, u);
+        load_in(s2i, ib, u);
         to_prim(u, g.gamma, w1);
 #pragma unroll
         for (int v = 0; v < NV; ++v) wa[v] = cell_slope(wa[v], w0[v], w1[v], lim);
@@ -804,11 +906,17 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
         }
         // x: primitives of row i+2, slope of row i+1, flux through face i+1/2 and
         // the x-flux difference of row i
-        fetch_wait();  // input row i+2 and U0 of row i have landed
+        wait_rows((1u << s2) | 8u);  // input row i+2 and U0 of row i have landed
+        if (TMA && __any_sync(0xffffffffu, gave_up)) {
+            // a copy never completed: give the others in flight a bounded chance to
+            // land (the shared rows must not be written after the CTA leaves), then stop
+            wait_rows(15u);
+            return false;
+        }
         R w2[NV], dfx[NV];
         {
             R u[NV], wl[NV], wr[NV], f[NV];
-            row_load(ms.raw[s2], lane, u);
+            load_in(s2, i + 2, u);
             ghost_psi(i + 2, u);
             to_prim(u, g.gamma, w2);
             if constexpr (kFast<R>) {
@@ -872,8 +980,11 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
                     return PowellIn<R>{w0[BX], bxm, w1[BX], w0[BY], bym, byp, w0[IVX], w0[IVY], w0[IVZ], w0[BZ]};
                 };
                 R us[NV], ub[NV];
-                row_load(ms.raw[s0], lane, us);
-                row_load(own_base ? ms.base : ms.raw[s0], lane, ub);
+                load_cell(s0, us);
+                if (own_base)
+                    load_base(ub);
+                else
+                    load_cell(s0, ub);
                 auto in_at = [&](int v) { return us[v]; };
                 auto base_at = [&](int v) { return ub[v]; };
                 update_cell_d<R, STAGE, false>(p, g, uout, i, j, dfx, dfy, pw, base_at, in_at, dt, ch, decay, q, bad);
@@ -881,8 +992,8 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
         }
         // rows done with: input row i (slot s0) -> row i+3; U0 of row i -> row i+1
         if (i + 1 < ie) {
-            fetch_row(ms.raw[s0], uin, vs, (int64_t)src_row(i + 3) * pitch + jl, lane);
-            if (own_base) fetch_row(ms.base, u0, vs, (int64_t)(i + 1) * pitch + jl, lane);
+            fetch_in(s0, i + 3);
+            if (own_base) fetch_base(i + 1);
         }
         s0 = s0 == 2 ? 0 : s0 + 1;
         bxm = w0[BX];
@@ -893,11 +1004,14 @@ __device__ __forceinline__ void march_walk(const StageParams &p, MarchSmem<R> &m
         }
     }
     __syncwarp();  // the next item reuses the shared rows
+    return true;
 }
 
-template <typename R, int STAGE>
-__device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &ms, int item, int lane,
-                                           unsigned long long q[4], bool &bad, amhd_control *&ctl_out)
+// false when a row copy never completed (TMA): the warp then stops
+template <typename R, int STAGE, bool TMA>
+__device__ __forceinline__ bool march_item(const StageParams &p, MarchSmem<R, TMA> &ms, int item, int lane,
+                                           unsigned long long q[4], bool &bad, amhd_control *&ctl_out,
+                                           uint32_t &phase)
 {
     int ii;
     const amhd_instance &in = inst_of(p, item, ii);
@@ -906,15 +1020,18 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
     ctl_out = ctl;
     double dt = p.dt, ch = p.ch, decay = p.decay;
     if (p.use_ctl) {
-        if (!ctl->active) return;
+        if (!ctl->active) return true;
         dt = ctl->dt;
         ch = ctl->ch;
         decay = ctl->decay;
     }
+    bool ok;
     if (g.limiter == AMHD_LIMITER_VANLEER && R(ch) > R(0))
-        march_walk<R, STAGE, true>(p, ms, in, g, item, lane, dt, ch, decay, q, bad);
+        ok = march_walk<R, STAGE, true, TMA>(p, ms, in, ii, g, item, lane, dt, ch, decay, q, bad, phase);
     else
-        march_walk<R, STAGE, false>(p, ms, in, g, item, lane, dt, ch, decay, q, bad);
+        ok = march_walk<R, STAGE, false, TMA>(p, ms, in, ii, g, item, lane, dt, ch, decay, q, bad, phase);
+    if (!ok && lane == 0 && ctl != nullptr) atomicOr(&ctl->flags, AMHD_FLAG_TIMEOUT);
+    return ok;
 }
 
 // resident CTAs of kMarchThreads per SM the register budget is shaped for:
@@ -923,17 +1040,22 @@ __device__ __forceinline__ void march_item(const StageParams &p, MarchSmem<R> &m
 template <typename R, int STAGE>
 constexpr int kMarchMinBlocks = kFast<R> ? 4 : 2;
 
-template <typename R, int STAGE>
+template <typename R, int STAGE, bool TMA>
 __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) march_stage_kernel(
     const __grid_constant__ StageParams p)
 {
-    extern __shared__ __align__(16) unsigned char march_smem[];
+    extern __shared__ __align__(128) unsigned char march_smem[];
     // run loop: the next launch may take SM slots as this grid drains; nothing
     // of the previous launch (stage input, controls) is read before it is done
     pdl_trigger();
     pdl_wait();
-    MarchSmem<R> &ms = reinterpret_cast<MarchSmem<R> *>(march_smem)[threadIdx.x >> 5];
+    MarchSmem<R, TMA> &ms = reinterpret_cast<MarchSmem<R, TMA> *>(march_smem)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
+    uint32_t phase = 0;  // TMA: parity of the next completion of each of the warp's 4 barriers
+    if constexpr (TMA) {
+        if (lane < 4) tma::mbar_init(&ms.bar[lane], 1);
+        __syncwarp();
+    }
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int n_warps = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
     // work positions: from the queue (each warp takes the next free position when it
@@ -950,7 +1072,7 @@ __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) ma
         unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
         bool bad = false;
         amhd_control *ctl = nullptr;
-        march_item<R, STAGE>(p, ms, item, lane, q, bad, ctl);
+        if (!march_item<R, STAGE, TMA>(p, ms, item, lane, q, bad, ctl, phase)) break;
         if (STAGE == 3 && ctl != nullptr) {
             // warp reduction of the CFL maxima and of the non-finite flag of the item
 #pragma unroll

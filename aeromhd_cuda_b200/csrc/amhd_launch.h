@@ -14,6 +14,7 @@ namespace amhd {
 // must live there or in global memory for the TMA unit to read it)
 struct StageParams {
     CUtensorMap tmap;              // single grid: tensor map of uin (when use_tma)
+    CUtensorMap tmap_base;         // single grid, marching kernel: tensor map of u0 (when use_tma)
     const CUtensorMap *tmaps;      // ensemble: 3 maps per instance (U, U1, U2), device memory
     int32_t use_tma;               // stage the tile + halo with TMA
     int32_t in_buf;                // ensemble: which of the 3 maps is uin
@@ -88,7 +89,9 @@ struct Launch {
     static cudaError_t bflux_accum(const amhd_grid &g, const R *U, amhd_control *ctl, double dt, cudaStream_t s);
 };
 
-// tensor map of one state buffer for tiles of tile_x rows (0 on success)
+// tensor map of one state buffer for the boxes of a stage kernel geometry (0 on success):
+// tiled kernel (tile_x > 0) [10 planes][tile_x + 4 rows][36 columns];
+// marching kernel (tile_x < 0) [10 planes][1 row][32 columns]
 int encode_state_map(CUtensorMap *map, const void *base, int dtype, int pitch, int64_t var_stride, int tile_x);
 
 cudaError_t launch_control_resume(amhd_control *ctl, int n, double snap_t, cudaStream_t s);

@@ -38,13 +38,13 @@ static inline int elem_blocks(int64_t n, int threads = 256)
     return (int)b;
 }
 
-template <typename R>
-constexpr size_t kMarchSmem = sizeof(MarchSmem<R>) * (kMarchThreads / 32);
+template <typename R, bool TMA = false>
+constexpr size_t kMarchSmem = sizeof(MarchSmem<R, TMA>) * (kMarchThreads / 32);
 
 template <typename R>
 size_t Launch<R>::stage_smem(int tile_x)
 {
-    if (is_march(tile_x)) return kMarchSmem<R>;
+    if (is_march(tile_x)) return kMarchSmem<R, true> > kMarchSmem<R> ? kMarchSmem<R, true> : kMarchSmem<R>;
     switch (tile_x) {
     case 4: return sizeof(TileSmem<R, 4>);
     case 8: return sizeof(TileSmem<R, 8>);
@@ -125,18 +125,26 @@ static cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 bl
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
+template <typename R, int ST, bool TMA>
+static cudaError_t launch_march_tt(const StageParams &p, int grid, cudaStream_t s)
+{
+    constexpr size_t smem = kMarchSmem<R, TMA>;
+    static PerDeviceOnce once;  // shared-memory opt-in, once per device
+    cudaError_t e = once.run([] {
+        return cudaFuncSetAttribute(march_stage_kernel<R, ST, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem);
+    });
+    if (e != cudaSuccess) return e;
+    if (p.pdl) return launch_dependent(march_stage_kernel<R, ST, TMA>, dim3(grid), dim3(kMarchThreads), smem, s, p);
+    march_stage_kernel<R, ST, TMA><<<grid, kMarchThreads, smem, s>>>(p);
+    return cudaGetLastError();
+}
+
+// rows staged by TMA (p.use_tma: the tensor maps are in p) or by per-lane cp.async
 template <typename R, int ST>
 static cudaError_t launch_march_t(const StageParams &p, int grid, cudaStream_t s)
 {
-    static PerDeviceOnce once;  // shared-memory opt-in, once per device
-    cudaError_t e = once.run([] {
-        return cudaFuncSetAttribute(march_stage_kernel<R, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)kMarchSmem<R>);
-    });
-    if (e != cudaSuccess) return e;
-    if (p.pdl) return launch_dependent(march_stage_kernel<R, ST>, dim3(grid), dim3(kMarchThreads), kMarchSmem<R>, s, p);
-    march_stage_kernel<R, ST><<<grid, kMarchThreads, kMarchSmem<R>, s>>>(p);
-    return cudaGetLastError();
+    return p.use_tma ? launch_march_tt<R, ST, true>(p, grid, s) : launch_march_tt<R, ST, false>(p, grid, s);
 }
 
 template <typename R>
@@ -194,9 +202,9 @@ int Launch<R>::stage_ctas_per_sm(int tile_x)
 {
     if (is_march(tile_x)) {
         int n = 0;
-        cudaFuncSetAttribute(march_stage_kernel<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(march_stage_kernel<R, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kMarchSmem<R>);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, march_stage_kernel<R, 3>, kMarchThreads,
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, march_stage_kernel<R, 3, false>, kMarchThreads,
                                                           kMarchSmem<R>) != cudaSuccess)
             return 1;
         return n > 0 ? n : 1;

@@ -155,7 +155,7 @@ def default_tile_x(precision: str) -> int:
 
 class Ensemble:
     def __init__(self, configs: Sequence[Config], tile_x: int = 0, order: str = "instance", ctas: int = -1,
-                 device=None, use_tma: bool = True, dynamic: bool = True):
+                 device=None, use_tma: bool | None = None, dynamic: bool = True):
         if not configs:
             raise ValueError("empty ensemble")
         precs = {c.precision for c in configs}
@@ -173,7 +173,7 @@ class Ensemble:
         tile_x = int(tile_x) or default_tile_x(self.precision)  # 0: the ensemble default
         self.tile_x = tile_x
         self.ctas = int(ctas)
-        self.use_tma = bool(use_tma)
+        self.use_tma = use_tma  # None: the library default of the stage kernel in use (_lib.DEFAULT_TMA)
         self.layouts, off = pack_layout(self.configs, self.code)
         self.total = off
         self.U = torch.zeros(off, dtype=self.dtype, device=self.device)
@@ -219,13 +219,19 @@ class Ensemble:
         self.tile_inst = torch.from_numpy(tile_inst).to(self.device)
         self.tile_order = torch.from_numpy(tile_order).to(self.device)
         self.tmaps_dev = None
-        if self.use_tma and tile_x > 0:
-            # TMA descriptors of every instance's box in U, U1, U2 for this tile shape
+        if self.tma_staging():
+            # TMA descriptors of every instance's box in U, U1, U2 for this work shape
             maps = torch.empty(3 * self.n * 128, dtype=torch.uint8)
             _lib.call("amhd_ensemble_tensormaps", ctypes.byref(table), self.n, self.code, self.tile_x,
                       self.U.data_ptr(), self.U1.data_ptr(), self.U2.data_ptr(), maps.data_ptr())
             self.tmaps_dev = maps.to(self.device)
         self._graphs = {}
+
+    def tma_staging(self) -> bool:
+        """Does the stage kernel stage its tiles (tiled) or rows (marching) with TMA?"""
+        if self.use_tma is None:
+            return bool(_lib.DEFAULT_TMA & (2 if self.tile_x < 0 else 1))
+        return bool(self.use_tma)
 
     def _grid(self, k: int) -> _lib.Grid:
         c = self.configs[k]

@@ -62,7 +62,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-reference-paths", action="store_true",
                     help="skip timing the reference's own modules on the GPU and on the host cores")
-    ap.add_argument("--tma", type=int, default=1, help="stage tiles with TMA (1) or 128-bit loads (0)")
+    ap.add_argument("--tma", type=int, default=None,
+                    help="TMA staging mode: bit 0 the tiled kernel's tiles, bit 1 the marching kernel's rows "
+                         "(default: the library's)")
     ap.add_argument("--tile-x", type=int, default=0,
                     help="stage kernel geometry: 4, 8, 16 (tiled kernel rows), negative (warp-marching rows) "
                          "or 0 (the library default: marching, 24 rows in fp32, 16 in fp64)")
@@ -113,7 +115,7 @@ def stage_kernel_name(tile_x):
 
 def stage_geometry(tile_x):
     if tile_x < 0:
-        return f"warp-marching, {-tile_x} rows x 28 columns per warp, cp.async row staging"
+        return f"warp-marching, {-tile_x} rows x 28 columns per warp"
     return f"tiled, {tile_x}x32 cells per CTA"
 
 
@@ -284,7 +286,8 @@ def run_ours(a, world, rank, local):
 
     n = a.n
     _lib.call("amhd_init")
-    _lib.call("amhd_set_tma", int(a.tma))
+    tma = _lib.DEFAULT_TMA if a.tma is None else int(a.tma)
+    _lib.call("amhd_set_tma", tma)
     _lib.call("amhd_set_tiling", int(a.tile_x), 0)
     tx = int(a.tile_x) or _lib.default_tile_x(a.precision)  # the geometry the fp32 / fp64 run uses
     cfg = ot_config(n, a.precision)
@@ -421,8 +424,8 @@ def run_ours(a, world, rank, local):
                    "pressure_recovery": "f64", "dt_reduction": "f64",
                    "l2": "inputs larger than L2 (3 state buffers of %.0f MB)" % (10 * (n + 4) * (n + 4) * es / 1e6),
                    "parallelism": f"replicas x{world}", "stage_kernel": stage_geometry(tx),
-                   "staging": ("cp.async rows" if tx < 0 else
-                               "TMA cp.async.bulk.tensor" if a.tma else "128-bit loads")},
+                   "staging": (("TMA rows (cp.async.bulk.tensor, one box per row)" if tma & 2 else "cp.async rows")
+                               if tx < 0 else "TMA cp.async.bulk.tensor" if tma & 1 else "128-bit loads")},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": loop_launches(tx, a.steps),
         "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
         "reference_cupy_shim": ref_gpu, "reference_numpy_shim": ref_host,
@@ -546,7 +549,8 @@ def run_ensemble(a, world):
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200.autotune import Cache, tune_ensemble
     cfgs = draw_configs(a.ensemble, seed=0, t_end=3.0, precision=a.precision)
-    ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=a.ensemble_ctas, use_tma=bool(a.tma))
+    ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=a.ensemble_ctas,
+                   use_tma=None if a.tma is None else bool(a.tma & (2 if (a.tile_x or -1) < 0 else 1)))
     ens.initialize()
     ens.start()
     tuned = None

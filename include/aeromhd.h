@@ -123,9 +123,12 @@ size_t amhd_control_size(void);
  * same nonzero tile_x values are accepted by amhd_stage_info and
  * amhd_ensemble_advance.  No counterpart in the reference. */
 int amhd_set_tiling(int32_t tile_x, int32_t ctas_per_sm);
-/* Stage the tile + halo with TMA (cp.async.bulk.tensor) when on (default) or
- * with 128-bit loads when off.  Process-wide.  No counterpart in the reference. */
-int amhd_set_tma(int32_t on);
+/* TMA staging (cp.async.bulk.tensor) per stage kernel, as a bit mask: bit 0
+ * the tiled kernel's tile + halo (else 128-bit loads), bit 1 the marching
+ * kernel's rows, one box of 32 columns x 10 planes per row for the warp
+ * (else per-lane cp.async).  Results are identical either way.  Default 1.
+ * Process-wide.  No counterpart in the reference. */
+int amhd_set_tma(int32_t mode);
 /* shared memory per CTA and resident CTAs per SM of the stage kernel of this geometry */
 int amhd_stage_info(int32_t dtype, int32_t tile_x, int32_t *smem_bytes, int32_t *ctas_per_sm, int32_t *sm_count);
 

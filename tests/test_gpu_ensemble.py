@@ -114,13 +114,17 @@ def test_autotuner_picks_a_candidate_and_restores_state():
     assert torch.equal(ens.U, before)
 
 
-def test_tma_staging_matches_plain_loads():
-    """The tile + halo staged by TMA (cp.async.bulk.tensor) or by 128-bit loads: identical results."""
+@pytest.mark.parametrize("tile_x", [8, -16])
+def test_tma_staging_matches_plain_loads(tile_x):
+    """The tile + halo (tiled kernel) or the rows (marching kernel, per-instance
+    tensor maps in device memory) staged by TMA (cp.async.bulk.tensor), or by
+    128-bit loads / per-lane cp.async: identical results."""
     from aeromhd_cuda_b200.ensemble import Ensemble
     cfgs = small_configs("fp32", n=4, seed=15)
     out = []
     for tma in (True, False):
-        ens = Ensemble(cfgs, tile_x=8, use_tma=tma)
+        ens = Ensemble(cfgs, tile_x=tile_x, use_tma=tma, ctas=0)
+        assert ens.tma_staging() == tma
         ens.initialize()
         ens.start(max_steps=5)
         ens.advance(5)

@@ -413,9 +413,11 @@ def test_device_argument_errors(amhd):
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_tma_staging_matches_plain_loads_single_grid(amhd, precision):
+    """Tiled kernel: tile + halo staged by TMA or by 128-bit loads."""
     from aeromhd_cuda_b200 import initial_conditions as ic
     res = []
     try:
+        amhd.lib.call("amhd_set_tiling", 8, 0)
         for tma in (1, 0):
             amhd.lib.call("amhd_set_tma", tma)
             s = amhd.solver.MHDSolver(ot_cfg(80, precision=precision))
@@ -423,7 +425,40 @@ def test_tma_staging_matches_plain_loads_single_grid(amhd, precision):
             s.advance(max_steps=7, chunk=7, graph=False)
             res.append(s.U.clone())
     finally:
-        amhd.lib.call("amhd_set_tma", 1)
+        amhd.lib.call("amhd_set_tma", amhd.lib.DEFAULT_TMA)
+        amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, 0)
+    assert torch.equal(res[0], res[1])
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape,rows,bcy", [((80, 80), -8, "periodic"), ((75, 61), -24, "periodic"),
+                                            ((33, 29), -5, "extrapolation"), ((40, 57), -16, "extrapolation"),
+                                            ((24, 4), -4, "periodic")])
+def test_marching_tma_rows_match_cp_async_rows(amhd, precision, shape, rows, bcy):
+    """Marching kernel: rows staged as TMA boxes (one copy per row for the warp,
+    the lanes on pulled ghost columns reading their sources) or by per-lane
+    cp.async -- identical bits, in the run loop (ghost cells pulled, Powell on,
+    outflow x) and in the drop-in step (ghost cells as stored)."""
+    nx, ny = shape
+    cfg = dict(nx=nx, ny=ny, x_min=0.0, x_max=1.0, y_min=0.0, y_max=ny / nx, t_end=0.5, cfl=0.4,
+               gamma=5.0 / 3.0, B_transverse=0.3, powell_source=True, bc_x_type="extrapolation", bc_y_type=bcy,
+               interface_x=0.5, perturbation_amp=0.03, precision=precision)
+    res = []
+    try:
+        amhd.lib.call("amhd_set_tiling", rows, 0)
+        for tma in (2, 0):
+            amhd.lib.call("amhd_set_tma", tma)
+            s = amhd.solver.MHDSolver(C(**cfg))
+            s.initialize()
+            s.advance(max_steps=6, chunk=6, graph=False)
+            for _ in range(2):  # drop-in step: ghost cells as stored
+                s.dt = s.compute_dt(amhd.physics.cons_to_prim(s.U, s.cfg.gamma))
+                s.step_ssprk3()
+            res.append(s.U.clone())
+    finally:
+        amhd.lib.call("amhd_set_tma", amhd.lib.DEFAULT_TMA)
+        amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, 0)
+    assert torch.isfinite(res[0]).all()
     assert torch.equal(res[0], res[1])
 
 
