@@ -61,6 +61,11 @@ class Instance(_c.Structure):
                 ("cut_x", _I32)]
 
 
+class NNTensor(_c.Structure):
+    _fields_ = [("w", _P), ("g", _P), ("m", _P), ("v", _P), ("w_bf16", _P), ("n", _I64), ("weight_decay", _c.c_float),
+                ("pad_", _I32)]
+
+
 class AmhdError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"libaeromhd error {code}: {msg}")
@@ -126,6 +131,7 @@ _SIGS = {
     "amhd_nn_mse": ([_P, _P, _I64, _P, _P, _P], _c.c_int),
     "amhd_nn_adam": ([_P, _P, _P, _P, _P, _I64, _c.c_float, _c.c_float, _c.c_float, _c.c_float, _I32, _c.c_float, _P],
                      _c.c_int),
+    "amhd_nn_adam_multi": ([_P, _I32, _I64, _P, _P], _c.c_int),
     "amhd_nn_restrict": ([_c.POINTER(Grid), _P, _I32, _P, _I64, _I32, _I32, _P], _c.c_int),
     "amhd_nn_pack": ([_c.POINTER(Grid), _P, _P, _P, _P, _I64, _I32, _P], _c.c_int),
     "amhd_nn_apply": ([_c.POINTER(Grid), _P, _P, _P, _I64, _I32, _P], _c.c_int),

@@ -88,6 +88,9 @@ class Corrector:
                               "mw": torch.zeros_like(w), "vw": torch.zeros_like(w),
                               "mb": torch.zeros_like(b), "vb": torch.zeros_like(b)}
         self.t = 0
+        self._adam = None      # (device table of amhd_nn_tensor, count, largest size, weight decay)
+        self._hyper = torch.zeros(6, dtype=F32, device=self.device)  # lr, b1, b2, eps, c1, c2
+        self._graphs: Dict[int, tuple] = {}
         self._ws: Dict[str, torch.Tensor] = {}
         self._act: Dict[str, torch.Tensor] = {}
         self.in_mean = torch.zeros(10, device=self.device)
@@ -234,16 +237,43 @@ class Corrector:
         self._pool_bwd_add(d_p1, S["e1"].cout, B, H, W, d_e1)
         self._conv_bwd(S["e1"], d_e1, a["e1"], B, H, W, need_dx=False)
 
+    def _adam_table(self, weight_decay: float):
+        """Device records of every parameter tensor for amhd_nn_adam_multi (weights
+        with their BF16 copies and weight decay, biases without)."""
+        if self._adam is None or self._adam[3] != weight_decay:
+            recs = []
+            for s in self.specs:
+                P = self.p[s.name]
+                recs.append((P["w"], P["gw"], P["mw"], P["vw"], P["wb"], weight_decay))
+                recs.append((P["b"], P["gb"], P["mb"], P["vb"], None, 0.0))
+            table = (_lib.NNTensor * len(recs))()
+            for r, (w, g, m, v, wb, wd) in zip(table, recs):
+                r.w, r.g, r.m, r.v = ptr(w), ptr(g), ptr(m), ptr(v)
+                r.w_bf16 = ptr(wb) if wb is not None else None
+                r.n, r.weight_decay = w.numel(), wd
+            dev = torch.frombuffer(bytearray(bytes(table)), dtype=torch.uint8).to(self.device)
+            self._adam = (dev, len(recs), max(r[0].numel() for r in recs), weight_decay)
+            self._graphs = {}
+        return self._adam
+
+    def _set_hyper(self, lr, beta1, beta2, eps) -> None:
+        """The step's Adam scalars into device memory (read by the kernel, also inside a graph)."""
+        t = np.float32(self.t)
+        c1 = np.float32(1) / (np.float32(1) - np.power(np.float32(beta1), t))
+        c2 = np.float32(1) / (np.float32(1) - np.power(np.float32(beta2), t))
+        self._hyper.copy_(torch.tensor([lr, beta1, beta2, eps, c1, c2], dtype=F32))
+
+    def _adam_launch(self, weight_decay: float) -> None:
+        table, n, big, _ = self._adam_table(weight_decay)
+        _lib.call("amhd_nn_adam_multi", ptr(table), n, big, ptr(self._hyper), stream_ptr())
+
     def adam_step(self, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999, eps: float = 1e-8,
                   weight_decay: float = 0.0) -> None:
+        """One Adam step of every parameter (one launch: amhd_nn_adam_multi)."""
         self.t += 1
-        st = stream_ptr()
-        for s in self.specs:
-            P = self.p[s.name]
-            _lib.call("amhd_nn_adam", ptr(P["w"]), ptr(P["gw"]), ptr(P["mw"]), ptr(P["vw"]), ptr(P["wb"]),
-                      P["w"].numel(), lr, beta1, beta2, eps, self.t, weight_decay, st)
-            _lib.call("amhd_nn_adam", ptr(P["b"]), ptr(P["gb"]), ptr(P["mb"]), ptr(P["vb"]), None,
-                      P["b"].numel(), lr, beta1, beta2, eps, self.t, 0.0, st)
+        self._adam_table(weight_decay)
+        self._set_hyper(lr, beta1, beta2, eps)
+        self._adam_launch(weight_decay)
 
     def check_gemm_status(self) -> None:
         """Raise if a tensor-core GEMM of the work queued so far gave up its bounded
@@ -262,6 +292,37 @@ class Corrector:
         self.backward(dout, B)
         self.adam_step(lr)
         return loss
+
+    def train_step_graphed(self, x: torch.Tensor, target: torch.Tensor, B: int, lr: float = 1e-3) -> torch.Tensor:
+        """train_step replayed as one CUDA graph: forward, loss, backward and the
+        Adam step captured once per batch size (after one eager step that sizes
+        every buffer), then every call copies the batch into the graph's input
+        buffers, writes the step's Adam scalars to device memory and replays.
+        Same kernels and arithmetic as train_step; returns a copy of the loss."""
+        g = self._graphs.get(B)
+        if g is None:
+            loss = self.train_step(x, target, B, lr)  # eager: sizes every workspace buffer
+            xs = torch.empty_like(x)
+            ts = torch.empty_like(target)
+            self._adam_table(0.0)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                out = self.forward(xs, B)
+                dout = self._buf("dout", out.shape)
+                lbuf = self._buf("loss", (1,))
+                lbuf.zero_()
+                _lib.call("amhd_nn_mse", ptr(out), ptr(ts), out.numel(), ptr(dout), ptr(lbuf), stream_ptr())
+                self.backward(dout, B)
+                self._adam_launch(0.0)
+            self._graphs[B] = (graph, xs, ts, lbuf)
+            return loss.clone()
+        graph, xs, ts, lbuf = g
+        xs.copy_(x)
+        ts.copy_(target)
+        self.t += 1
+        self._set_hyper(lr, 0.9, 0.999, 1e-8)
+        graph.replay()
+        return lbuf.clone()
 
     def loss(self, x: torch.Tensor, target: torch.Tensor, B: int) -> float:
         out = self.forward(x, B)

@@ -763,6 +763,25 @@ __global__ void adam_kernel(float *w, const float *g, float *m, float *v, bf16 *
     }
 }
 
+// all tensors of a network in one launch: blockIdx.y picks the tensor, the step's
+// scalars come from device memory (hyper = lr, b1, b2, eps, c1, c2)
+__global__ void adam_multi_kernel(const amhd_nn_tensor *ts, const float *hyper)
+{
+    const amhd_nn_tensor t = ts[blockIdx.y];
+    const float lr = hyper[0], b1 = hyper[1], b2 = hyper[2], eps = hyper[3], c1 = hyper[4], c2 = hyper[5];
+    bf16 *wb = static_cast<bf16 *>(t.w_bf16);
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < t.n; k += (int64_t)gridDim.x * blockDim.x) {
+        const float gk = t.g[k] + t.weight_decay * t.w[k];
+        const float mk = b1 * t.m[k] + (1.f - b1) * gk;
+        const float vk = b2 * t.v[k] + (1.f - b2) * gk * gk;
+        t.m[k] = mk;
+        t.v[k] = vk;
+        const float wk = t.w[k] - lr * (mk * c1) / (sqrtf(vk * c2) + eps);
+        t.w[k] = wk;
+        if (wb) wb[k] = __float2bfloat16(wk);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // solver <-> network data movement
 // ---------------------------------------------------------------------------
@@ -1142,6 +1161,19 @@ int amhd_nn_adam(float *w, const float *g, float *m, float *v, void *w_bf16, int
     const float c1 = 1.f / (1.f - powf(beta1, (float)t)), c2 = 1.f / (1.f - powf(beta2, (float)t));
     if (n) adam_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(w, g, m, v, static_cast<bf16 *>(w_bf16), n, lr, beta1,
                                                              beta2, eps, c1, c2, weight_decay);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_adam_multi(const amhd_nn_tensor *tensors_dev, int32_t n_tensors, int64_t max_n, const float *hyper_dev,
+                       void *stream)
+{
+    if (!tensors_dev || !hyper_dev || n_tensors < 0 || n_tensors > 65535 || max_n < 0)
+        return nn_fail(AMHD_ERR_ARG, "bad adam_multi arguments");
+    if (n_tensors == 0 || max_n == 0) return AMHD_OK;
+    int64_t bx = (max_n + 255) / 256;
+    if (bx > 1024) bx = 1024;
+    adam_multi_kernel<<<dim3((unsigned)bx, (unsigned)n_tensors), 256, 0, S(stream)>>>(tensors_dev, hyper_dev);
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }

@@ -88,6 +88,9 @@ def time_train_step(iters: int, warmup: int, H: int = 256, W: int = 64, batch: i
             _lib.call("amhd_nn_set_gemm_path", mode)
             ms = _events_ms(lambda: net.train_step(x, t, batch, lr=1e-5), iters, warmup)
             out[name] = {"ms": round(ms, 3)}
+        # the same step replayed as one CUDA graph (library GEMM choice)
+        ms = _events_ms(lambda: net.train_step_graphed(x, t, batch, lr=1e-5), iters, warmup)
+        out["auto, CUDA graph"] = {"ms": round(ms, 3)}
     finally:
         _lib.call("amhd_nn_set_gemm_path", 0)
     _check_waits()

@@ -179,7 +179,7 @@ def train(X: torch.Tensor, Y: torch.Tensor, train_seeds: Sequence[int], val_seed
             idx = perm[b0:b0 + batch].to(X.device)
             x = norm.inputs(tr[idx])
             t = norm.targets(ttr[idx])
-            losses.append(net.train_step(x, t, batch, lr=sched(ep)))
+            losses.append(net.train_step_graphed(x, t, batch, lr=sched(ep)))
         net.check_gemm_status()  # once per epoch: a GEMM that gave up invalidates the epoch
         tl = float(torch.stack([l.reshape(()) for l in losses]).mean()) if losses else float("nan")
         vl = []

@@ -401,6 +401,24 @@ int amhd_nn_mse(const float *pred, const float *target, int64_t n, float *grad, 
  * decay; refreshes the BF16 copy w_bf16 (may be NULL) */
 int amhd_nn_adam(float *w, const float *g, float *m, float *v, void *w_bf16, int64_t n, float lr, float beta1,
                  float beta2, float eps, int32_t t, float weight_decay, void *stream);
+/* One parameter tensor of amhd_nn_adam_multi (device pointers). */
+typedef struct amhd_nn_tensor {
+    float *w;             /* float32 master weights                          */
+    const float *g;       /* gradient                                        */
+    float *m, *v;         /* Adam moments                                    */
+    void *w_bf16;         /* bfloat16 copy refreshed after the step, or NULL */
+    int64_t n;            /* elements                                        */
+    float weight_decay;
+    int32_t pad_;
+} amhd_nn_tensor;
+/* The Adam step of amhd_nn_adam on n_tensors tensors in one launch, with the
+ * step's scalars read from device memory -- hyper_dev = {lr, beta1, beta2,
+ * eps, 1/(1 - beta1^t), 1/(1 - beta2^t)} -- so that the launch can be part of
+ * a captured CUDA graph replayed every step.  tensors_dev: the records in
+ * device memory; max_n: the largest n among them.  Same arithmetic as
+ * amhd_nn_adam.  No counterpart in the reference. */
+int amhd_nn_adam_multi(const amhd_nn_tensor *tensors_dev, int32_t n_tensors, int64_t max_n, const float *hyper_dev,
+                       void *stream);
 /* factor x factor block average of a fine state's interior (float64 sums)
  * into sample b of out[10][B][nx/f][ny/f] (plane stride out_vs) */
 int amhd_nn_restrict(const amhd_grid *fine, const void *Uf, int32_t factor, float *out, int64_t out_vs, int32_t b,
