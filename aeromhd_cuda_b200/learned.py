@@ -239,6 +239,75 @@ def rollout_pairs(net: Corrector, norm: "Normaliser", seeds: Sequence[int], delt
     return X, Y
 
 
+def prolong_linear(Uc: torch.Tensor, factor: int) -> torch.Tensor:
+    """Coarse interior [10][nx][ny] -> fine interior [10][f nx][f ny]: in every
+    coarse cell a linear profile with minmod-limited slopes in x (one-sided at
+    the two ends) and y (periodic); the sub-cell offsets average to zero, so
+    each coarse cell's mean -- mass, momentum, energy, field -- is kept."""
+    U = Uc.double()
+
+    def minmod(a, b):
+        return torch.where(a * b > 0, torch.sign(a) * torch.minimum(a.abs(), b.abs()), torch.zeros_like(a))
+
+    sx = minmod(U - torch.cat([U[:, :1], U[:, :-1]], 1), torch.cat([U[:, 1:], U[:, -1:]], 1) - U)
+    sy = minmod(U - U.roll(1, 2), U.roll(-1, 2) - U)
+    off = (torch.arange(factor, dtype=torch.float64, device=U.device) + 0.5) / factor - 0.5
+    f = (U[:, :, None, :, None] + sx[:, :, None, :, None] * off.view(1, 1, -1, 1, 1)
+         + sy[:, :, None, :, None] * off.view(1, 1, 1, 1, -1))
+    nx, ny = U.shape[1], U.shape[2]
+    return f.reshape(10, nx * factor, ny * factor).to(Uc.dtype)
+
+
+def closure_pairs(net: Corrector, norm: "Normaliser", seeds: Sequence[int], delta: float = DELTA,
+                  t_end: float = 3.0, alpha: float = 1.0, scalar_mode: int = 3, every: int = 3, nyc: int = 64,
+                  factor: int = 4, precision: str = "fp32", log=print):
+    """Pairs along the corrector's own runs with targets consistent with them: at
+    every `every`-th correction time the corrected coarse state is prolonged onto
+    the fine grid (prolong_linear), the fine solver advances it by `delta` and the
+    result is restricted; the coarse solver advances the same state by `delta`.
+    The pair (coarse result, restricted fine result) is what the fine solver
+    would have added over that interval from where the corrected run actually
+    is -- a closure target -- instead of the distance to a fine trajectory the
+    chaotic run has decorrelated from.  Returns (X, Y) shaped like
+    generate_pairs'."""
+    coarse, fine = paired_configs(seeds, nyc, factor, precision)
+    ef, ec = Ensemble(fine), Ensemble(coarse)
+    ef.initialize()
+    nxc, nyc_ = coarse[0].nx, coarse[0].ny
+    buf = torch.empty((10, nxc * nyc_), dtype=torch.float32, device=ec.device)
+    _load_restricted(ef, ec, factor, buf)
+    n = len(seeds)
+    m_total = int(round(t_end / delta))
+    keep = [q for q in range(1, m_total + 1) if q % every == 0]
+    X = torch.empty((len(keep), n, 10, nxc, nyc_), dtype=torch.float32, device=ec.device)
+    Y = torch.empty_like(X)
+    ec.start(t_end=delta)
+    idx = np.arange(n)
+    zeros = [0] * n
+    j = 0
+    for q in range(1, m_total + 1):
+        tc = q * delta
+        if q % every == 0:
+            for i in range(n):
+                _interior(ef, i).copy_(prolong_linear(_interior(ec, i), factor))
+                _lib.call("amhd_apply_bc", ef._grid(i), ptr(ef.state(i)), stream_ptr())
+            ef.resume([tc - delta] * n, zeros, [0.0] * n, tc)
+            ef.run(chunk=64)
+            for i in range(n):
+                _lib.call("amhd_nn_restrict", ef._grid(i), ptr(ef.state(i)), factor, ptr(Y[j, i]), nxc * nyc_, 0, 1,
+                          stream_ptr())
+        ec.continue_to(tc)
+        ec.run(chunk=32)
+        if q % every == 0:
+            for i in range(n):
+                X[j, i].copy_(_interior(ec, i))
+            j += 1
+        _apply_batch(net, norm, ec, idx, 8.0, alpha, 0.5, None, scalar_mode)
+        if log and q % 30 == 0:
+            log(f"  closure pairs to t={tc:.2f}")
+    return X, Y
+
+
 def _mixing_width(ens: Ensemble, k: int) -> float:
     c = ens.configs[k]
     out = torch.zeros(8, dtype=torch.float64, device=ens.device)
@@ -497,6 +566,9 @@ def main(argv=None) -> int:
                     help="rounds of training on pairs from the corrector's own runs")
     ap.add_argument("--dagger-epochs", type=int, default=20)
     ap.add_argument("--dagger-mode", type=int, default=3, help="correction mode of those runs")
+    ap.add_argument("--closure-rounds", type=int, default=0,
+                    help="rounds of training on closure pairs along the corrector's own runs (closure_pairs)")
+    ap.add_argument("--closure-every", type=int, default=3)
     ap.add_argument("--project-y", action="store_true",
                     help="train on and apply the row averages of the corrections (project_rows)")
     ap.add_argument("--save", default=None)
@@ -523,6 +595,16 @@ def main(argv=None) -> int:
             net, norm, h2 = train(X, Y, range(n_val, a.train_seeds), range(n_val), epochs=a.dagger_epochs,
                                   batch=a.batch, lr=a.lr * 0.5, net=net, norm=norm, log=log)
             hist[f"round{r + 1}"] = h2
+        for r in range(a.closure_rounds):
+            log(f"closure round {r + 1}: fine evolution from the corrected runs' states ...")
+            X2, Y2 = closure_pairs(net, norm, seeds, delta=a.delta, scalar_mode=a.dagger_mode,
+                                   every=a.closure_every, nyc=a.nyc, log=log)
+            X, Y = torch.cat([X, X2]), torch.cat([Y, Y2])
+            del X2, Y2
+            n_pairs = int(X.shape[0] * X.shape[1])
+            net, norm, h2 = train(X, Y, range(n_val, a.train_seeds), range(n_val), epochs=a.dagger_epochs,
+                                  batch=a.batch, lr=a.lr * 0.5, net=net, norm=norm, log=log)
+            hist[f"closure{r + 1}"] = h2
         del X, Y
     log("evaluating on held-out seeds ...")
     test = list(range(10000, 10000 + a.test_seeds))

@@ -39,3 +39,18 @@ def test_pairs_share_parameters_and_differ_by_4x_resolution():
                (b.mach, b.density_ratio, b.bx0, b.b1, b.perturbation_mode)
         assert a.ic_frame == "post_shock" and a.noise_amp == 0.0
     assert len(T_SNAPS) == 30 and abs(T_SNAPS[-1] - 3.0) < 1e-12
+
+
+def test_linear_prolongation_keeps_every_coarse_mean():
+    """prolong_linear: 4x4 sub-cells whose average is the coarse cell, exact on a
+    linear field away from the limited x ends."""
+    from aeromhd_cuda_b200.learned import prolong_linear
+    g = torch.Generator().manual_seed(3)
+    U = torch.randn(10, 12, 8, generator=g, dtype=torch.float64)
+    F = prolong_linear(U, 4)
+    assert F.shape == (10, 48, 32)
+    assert torch.allclose(F.reshape(10, 12, 4, 8, 4).mean(dim=(2, 4)), U, atol=1e-13)
+    x = torch.arange(12, dtype=torch.float64)[:, None].expand(12, 8)
+    lin = prolong_linear(x.expand(10, 12, 8).clone(), 4)
+    fine_x = (torch.arange(48, dtype=torch.float64) + 0.5) / 4 - 0.5
+    assert torch.allclose(lin[0, 4:-4, 0], fine_x[4:-4])
