@@ -68,6 +68,9 @@ def parse_args(argv=None):
     ap.add_argument("--tile-x", type=int, default=0,
                     help="stage kernel geometry: 4, 8, 16 (tiled kernel rows), negative (warp-marching rows) "
                          "or 0 (the library default: marching, 24 rows in fp32, 16 in fp64)")
+    ap.add_argument("--ctas-per-sm", type=int, default=0,
+                    help="stage grid: 0 one CTA per tile / per 4 marching items, else a persistent grid of "
+                         "this many CTAs per SM")
     ap.add_argument("--decomp", action="store_true",
                     help="one n x n grid split over the ranks by x rows (strong scaling) instead of replicas")
     ap.add_argument("--ensemble", type=int, default=256,
@@ -288,7 +291,7 @@ def run_ours(a, world, rank, local):
     _lib.call("amhd_init")
     tma = _lib.DEFAULT_TMA if a.tma is None else int(a.tma)
     _lib.call("amhd_set_tma", tma)
-    _lib.call("amhd_set_tiling", int(a.tile_x), 0)
+    _lib.call("amhd_set_tiling", int(a.tile_x), int(a.ctas_per_sm))
     tx = int(a.tile_x) or _lib.default_tile_x(a.precision)  # the geometry the fp32 / fp64 run uses
     cfg = ot_config(n, a.precision)
     s = MHDSolver(cfg)
