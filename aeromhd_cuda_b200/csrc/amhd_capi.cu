@@ -514,10 +514,10 @@ int amhd_boundary_energy_flux(const amhd_grid *g, const void *U, amhd_control *c
     }
     cudaStream_t s = S(stream);
     if (g->dtype == AMHD_F64)
-        CK(Launch<double>::bflux(*g, static_cast<const double *>(U), &ctl->reserved[0], s));
+        CK(Launch<double>::bflux(*g, static_cast<const double *>(U), &ctl->scratch, s));
     else
-        CK(Launch<float>::bflux(*g, static_cast<const float *>(U), &ctl->reserved[0], s));
-    CK(cudaMemcpyAsync(out_host, &ctl->reserved[0], sizeof(double), cudaMemcpyDeviceToHost, s));
+        CK(Launch<float>::bflux(*g, static_cast<const float *>(U), &ctl->scratch, s));
+    CK(cudaMemcpyAsync(out_host, &ctl->scratch, sizeof(double), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
     return AMHD_OK;
 }

@@ -1417,6 +1417,8 @@ __global__ void finalize_kernel(const amhd_instance *insts, const amhd_instance 
                 ctl->t += ctl->dt;  // solver.py:481-482
                 ctl->last_dt = ctl->dt;
                 ctl->step += 1;
+                ctl->e_bnd += ctl->e_bnd_next;  // the step just taken (solver.py:316-317)
+                ctl->e_bnd_next = 0.0;
             }
             // a step that wrote a non-finite value, or whose bounded wait gave up and
             // left tiles stale, ends the loop: the host reads the flag and raises
@@ -1463,7 +1465,7 @@ __global__ void finalize_kernel(const amhd_instance *insts, const amhd_instance 
     __syncthreads();
     if (go) {
         double bf = boundary_flux_block(g, U, in.cut_x);  // solver.py:316-317
-        if (threadIdx.x == 0) ctl->e_bnd += bf * dt_next;
+        if (threadIdx.x == 0) ctl->e_bnd_next = bf * dt_next;  // counted once the step is taken
     }
 }
 

@@ -98,7 +98,11 @@ typedef struct amhd_control {
     double snap_t;       /* pause the loop after the step that brings t within */
                          /* 1.5 dt of snap_t (run(), solver.py:487-490);       */
                          /* +inf or NaN: never                                 */
-    double reserved[3];
+    double scratch;      /* device scratch of amhd_boundary_energy_flux          */
+    double e_bnd_next;   /* boundary energy flux x dt of the step the loop takes */
+                         /* next; added to e_bnd once that step is taken, so    */
+                         /* e_bnd counts the steps taken (solver.py:316-317)    */
+    double reserved;
 } amhd_control;
 
 /* ---- library ---------------------------------------------------------- */
@@ -162,7 +166,7 @@ int amhd_compute_dt(const amhd_grid *g, const void *W, amhd_control *ctl, double
 int amhd_compute_dt_cons(const amhd_grid *g, const void *U, amhd_control *ctl, double *dt_host, double *ch_host,
                          void *stream);
 /* _compute_boundary_energy_flux, solver.py:225-240 (0 for periodic x).
- * ctl is used as device scratch (its reserved[0] receives the flux, nothing
+ * ctl is used as device scratch (its scratch field receives the flux, nothing
  * else changes); synchronises. */
 int amhd_boundary_energy_flux(const amhd_grid *g, const void *U, amhd_control *ctl, double *out_host, void *stream);
 /* _compute_powell_source, solver.py:242-266: S from primitive W (same layout
