@@ -154,7 +154,7 @@ def default_tile_x(precision: str) -> int:
 
 
 class Ensemble:
-    def __init__(self, configs: Sequence[Config], tile_x: int = 0, order: str = "instance", ctas: int = -1,
+    def __init__(self, configs: Sequence[Config], tile_x: int = 0, order: str = "instance", ctas: int = 0,
                  device=None, use_tma: bool | None = None, dynamic: bool = True):
         if not configs:
             raise ValueError("empty ensemble")
@@ -192,14 +192,15 @@ class Ensemble:
         """Stage-kernel geometry (tile_x: 4, 8, 16 rows x 32 columns per CTA of the
         tiled kernel, or negative: -tile_x rows x 28 columns per warp of the
         marching kernel), work-list order and grid size (chosen by autotune).
-        ctas: -1 (default) = one CTA per tile (tiled) / per 4 work items
-        (marching), the hardware handing CTAs to SMs as they free up; 0 = a
-        persistent grid of resident CTAs per SM x SM count (> 0: that many
-        CTAs).  On a persistent marching grid each warp takes the next free
-        item from a device work queue when it finishes one (``dynamic``,
-        the default); with dynamic=False warp w takes items w, w + warps, ...
-        (on the uneven 256-instance ensemble 20-30 % slower than one CTA per
-        4 items: the static split leaves warps idle at the end)."""
+        ctas: 0 (default) = a persistent grid of resident CTAs per SM x SM
+        count (> 0: that many CTAs), one launch per RK stage; -1 = one CTA per
+        tile (tiled) / per 4 work items (marching), the hardware handing CTAs
+        to SMs as they free up.  On a persistent marching grid each warp takes
+        the next free item from a device work queue when it finishes one
+        (``dynamic``, the default): on the uneven 256-instance ensemble as fast
+        as one CTA per 4 items (6.67 against 6.69 G zone-updates/s); with
+        dynamic=False warp w takes items w, w + warps, ... (20-30 % slower:
+        the static split leaves warps idle at the end)."""
         rows, cols = work_shape(tile_x)
         self.tile_x, self.order, self.ctas = int(tile_x), order, int(ctas)
         counts = tile_counts(self.configs, tile_x)

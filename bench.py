@@ -75,8 +75,9 @@ def parse_args(argv=None):
                     help="one n x n grid split over the ranks by x rows (strong scaling) instead of replicas")
     ap.add_argument("--ensemble", type=int, default=256,
                     help="also time the batched shock-interface ensemble of this many instances (0: skip)")
-    ap.add_argument("--ensemble-ctas", type=int, default=-1,
-                    help="ensemble grid: -1 one CTA per 4 items, 0 persistent (work queue), >0 that many CTAs")
+    ap.add_argument("--ensemble-ctas", type=int, default=0,
+                    help="ensemble grid: 0 persistent (work queue, the default), -1 one CTA per 4 items, "
+                         ">0 that many CTAs")
     ap.add_argument("--ensemble-tune", action="store_true",
                     help="choose the ensemble's work shape, order and grid with the autotuner first")
     return ap.parse_args(argv)
@@ -577,7 +578,8 @@ def run_ensemble(a, world):
     return {"value": world * cells * k / (ms / 1e3), "unit": "zone-updates/s", "instances": a.ensemble,
             "cells": cells, "steps": k, "ms_per_step": ms / k,
             "schedule": {"tile_x": ens.tile_x, "order": ens.order,
-                         "grid": "persistent" if ens.ctas >= 0 else "one CTA per work group", "autotuned": tuned}}
+                         "grid": ("persistent, device work queue" if ens.uses_queue() else "persistent")
+                         if ens.ctas >= 0 else "one CTA per work group", "autotuned": tuned}}
 
 
 def run_reference(a, world, rank):
