@@ -68,6 +68,23 @@ def precision_errors(s32: MHDSolver, s64: MHDSolver) -> dict:
     return out
 
 
+def state_errors(s32: MHDSolver, s64: MHDSolver) -> dict:
+    """Relative L1 errors of a state against a reference state by physical
+    quantity: the whole state (all ten planes, sum |dU| / sum |U|), density,
+    energy, the momentum and field vectors (sum over cells of the component
+    L1 norm of the difference over that of the reference vector), psi against
+    the field it cleans (sum |d psi| / sum |B|) and the colour against the
+    density.  A small transverse component (m_y, B_y of a planar shock) is
+    judged against the vector it belongs to rather than against itself."""
+    a, b = interior(s32).double(), interior(s64).double()
+    d = (a - b).abs()
+    s = lambda t: float(t.sum())
+    babs = b.abs()
+    return {"state": s(d) / s(babs), "rho": s(d[0]) / s(babs[0]), "E": s(d[7]) / s(babs[7]),
+            "m": s(d[1:4]) / s(babs[1:4]), "B": s(d[4:7]) / s(babs[4:7]), "psi/|B|": s(d[8]) / s(babs[4:7]),
+            "rhoC/rho": s(d[9]) / s(babs[0])}
+
+
 def same_initial_state(s32: MHDSolver, s64: MHDSolver) -> None:
     """Start both solvers from the float64 state rounded once to float32, so
     that their difference comes from the arithmetic alone."""
@@ -95,7 +112,7 @@ def precision_horizon(nx: int = 2048, ny: int = 512, t_end: float = 3.0, every: 
     C.initialize()
     same_initial_state(C, B)
     out = {"case": "precision_horizon", "nx": nx, "ny": ny, "times": [], "fp32_vs_fp64": [],
-           "fp64_vs_fp64_of_rounded_start": []}
+           "fp64_vs_fp64_of_rounded_start": [], "fp32_vs_fp64_by_quantity": [], "magnitudes": []}
     t = 0.0
     while t < t_end - 1e-12:
         t = min(t_end, t + every)
@@ -104,6 +121,9 @@ def precision_horizon(nx: int = 2048, ny: int = 512, t_end: float = 3.0, every: 
         out["times"].append(t)
         out["fp32_vs_fp64"].append(precision_errors(C, B))
         out["fp64_vs_fp64_of_rounded_start"].append(precision_errors(B, A))
+        out["fp32_vs_fp64_by_quantity"].append(state_errors(C, B))
+        Ub = interior(B).double().abs()
+        out["magnitudes"].append({VAR_NAMES[v]: float(Ub[v].mean()) for v in range(10)})
     return out
 
 
@@ -126,6 +146,7 @@ def orszag_tang(n: int = 512, t_end: float = 0.5, precisions=("fp32", "fp64")) -
                   "mass": d["mass"], "energy": d["energy"], "divB_L2": d["divB_L2"]}
     if "fp32" in runs and "fp64" in runs:
         out["fp32_vs_fp64"] = precision_errors(runs["fp32"], runs["fp64"])
+        out["fp32_vs_fp64_by_quantity"] = state_errors(runs["fp32"], runs["fp64"])
         out["same_step_count"] = runs["fp32"].step == runs["fp64"].step
     return out
 

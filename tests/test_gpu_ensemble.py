@@ -114,13 +114,15 @@ def test_autotuner_picks_a_candidate_and_restores_state():
     assert torch.equal(ens.U, before)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("tile_x", [8, -16])
-def test_tma_staging_matches_plain_loads(tile_x):
+def test_tma_staging_matches_plain_loads(tile_x, precision):
     """The tile + halo (tiled kernel) or the rows (marching kernel, per-instance
     tensor maps in device memory) staged by TMA (cp.async.bulk.tensor), or by
-    128-bit loads / per-lane cp.async: identical results."""
+    128-bit loads / per-lane cp.async: identical results (float32 marching: the
+    two instantiations may contract multiply-adds differently, bar 1e-6)."""
     from aeromhd_cuda_b200.ensemble import Ensemble
-    cfgs = small_configs("fp32", n=4, seed=15)
+    cfgs = small_configs(precision, n=4, seed=15)
     out = []
     for tma in (True, False):
         ens = Ensemble(cfgs, tile_x=tile_x, use_tma=tma, ctas=0)
@@ -129,4 +131,8 @@ def test_tma_staging_matches_plain_loads(tile_x):
         ens.start(max_steps=5)
         ens.advance(5)
         out.append(ens.U.clone())
-    assert torch.equal(out[0], out[1])
+    if precision == "fp64" or tile_x > 0:
+        assert torch.equal(out[0], out[1])
+    else:
+        rel = float((out[0].double() - out[1].double()).abs().sum() / out[1].double().abs().sum())
+        assert rel < 1e-6, rel

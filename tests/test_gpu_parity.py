@@ -437,8 +437,10 @@ def test_tma_staging_matches_plain_loads_single_grid(amhd, precision):
 def test_marching_tma_rows_match_cp_async_rows(amhd, precision, shape, rows, bcy):
     """Marching kernel: rows staged as TMA boxes (one copy per row for the warp,
     the lanes on pulled ghost columns reading their sources) or by per-lane
-    cp.async -- identical bits, in the run loop (ghost cells pulled, Powell on,
-    outflow x) and in the drop-in step (ghost cells as stored)."""
+    cp.async, in the run loop (ghost cells pulled, Powell on, outflow x) and in
+    the drop-in step (ghost cells as stored): identical bits in float64 (built
+    without contraction); in float32 the two instantiations may contract
+    multiply-adds differently, so there the bar is 1e-6 relative."""
     nx, ny = shape
     cfg = dict(nx=nx, ny=ny, x_min=0.0, x_max=1.0, y_min=0.0, y_max=ny / nx, t_end=0.5, cfl=0.4,
                gamma=5.0 / 3.0, B_transverse=0.3, powell_source=True, bc_x_type="extrapolation", bc_y_type=bcy,
@@ -459,7 +461,11 @@ def test_marching_tma_rows_match_cp_async_rows(amhd, precision, shape, rows, bcy
         amhd.lib.call("amhd_set_tma", amhd.lib.DEFAULT_TMA)
         amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, 0)
     assert torch.isfinite(res[0]).all()
-    assert torch.equal(res[0], res[1])
+    if precision == "fp64":
+        assert torch.equal(res[0], res[1])
+    else:
+        rel = float((res[0].double() - res[1].double()).abs().sum() / res[1].double().abs().sum())
+        assert rel < 1e-6, rel
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
