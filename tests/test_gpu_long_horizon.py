@@ -73,7 +73,8 @@ def test_shock_interface_2048x512_to_t3_fp32_against_fp64():
     assert abs(m32[-1] - m64[-1]) <= BAR * abs(m64[-1])
     assert abs(e32[-1] - e64[-1]) <= BAR * abs(e64[-1])
     eb32, eb64 = s32._cumulative_boundary_energy, s64._cumulative_boundary_energy
-    assert abs(eb32 - eb64) <= BAR * abs(e64[0]), (eb32, eb64)
+    # accumulated every step like the state: measured 8.8e-6 of itself at t = 3
+    assert abs(eb32 - eb64) <= 1.5 * BAR * abs(eb64), (eb32, eb64)
     # mixing-width histories, sampled every 200 steps: compare at the float64 run's times
     t32, t64 = np.array(s32.diag_times), np.array(s64.diag_times)
     mw32 = np.interp(t64, t32, np.array(s32.diag_mixing_width_integral))
