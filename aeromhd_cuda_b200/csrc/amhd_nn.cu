@@ -13,6 +13,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -591,45 +592,42 @@ __global__ void scale_kernel(float *C, int M, int N, int ldc, float beta)
 // ---------------------------------------------------------------------------
 // convolution helpers, activations [C][B][H][W] (FP32) / columns (BF16)
 // ---------------------------------------------------------------------------
+// grid: x over the output pixels n (256 per block), y over the rows c * 9 + tap
+// of col; pixel coordinates from 32-bit divisions once per thread
 __global__ void im2col3_kernel(const float *X, int C, int B, int H, int W, bf16 *col)
 {
-    const int64_t N = (int64_t)B * H * W;
-    const int64_t total = (int64_t)C * 9 * N;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t n = k % N;
-        const int row = (int)(k / N);
-        const int c = row / 9, tap = row % 9, dy = tap / 3 - 1, dx = tap % 3 - 1;
-        const int w = (int)(n % W), h = (int)((n / W) % H);
-        const int64_t b = n / ((int64_t)H * W);
-        const int hh = h + dy, ww = w + dx;
-        float v = 0.f;
-        if (hh >= 0 && hh < H && ww >= 0 && ww < W) v = X[((int64_t)c * B + b) * H * W + (int64_t)hh * W + ww];
-        col[k] = __float2bfloat16(v);
-    }
+    const int N = B * H * W;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int row = blockIdx.y;
+    const int c = row / 9, tap = row - 9 * (row / 9), dy = tap / 3 - 1, dx = tap % 3 - 1;
+    const int q = n / W, w = n - q * W;
+    const int b = q / H, h = q - b * H;
+    const int hh = h + dy, ww = w + dx;
+    float v = 0.f;
+    if (hh >= 0 && hh < H && ww >= 0 && ww < W) v = X[((int64_t)c * B + b) * H * W + (int64_t)hh * W + ww];
+    col[(int64_t)row * N + n] = __float2bfloat16(v);
 }
 
-// dX[c][b][h][w] = sum over taps of dcol[c*9+tap][output pixel that read (h,w) through that tap]
+// dX[c][b][h][w] = sum over taps of dcol[c*9+tap][output pixel that read (h,w) through that tap];
+// grid: x over the pixels (256 per block), y over the channels
 __global__ void col2im3_kernel(const float *dcol, int C, int B, int H, int W, float *dX)
 {
-    const int64_t N = (int64_t)B * H * W;
-    const int64_t total = (int64_t)C * N;
-    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < total;
-         k += (int64_t)gridDim.x * blockDim.x) {
-        const int c = (int)(k / N);
-        const int64_t n = k % N;
-        const int w = (int)(n % W), h = (int)((n / W) % H);
-        const int64_t b = n / ((int64_t)H * W);
-        float s = 0.f;
+    const int N = B * H * W;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= N) return;
+    const int c = blockIdx.y;
+    const int q = n / W, w = n - q * W;
+    const int b = q / H, h = q - b * H;
+    float s = 0.f;
 #pragma unroll
-        for (int tap = 0; tap < 9; ++tap) {
-            const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-            const int ho = h - dy, wo = w - dx;
-            if (ho >= 0 && ho < H && wo >= 0 && wo < W)
-                s += dcol[(int64_t)(c * 9 + tap) * N + (b * H + ho) * W + wo];
-        }
-        dX[k] = s;
+    for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        const int ho = h - dy, wo = w - dx;
+        if (ho >= 0 && ho < H && wo >= 0 && wo < W)
+            s += dcol[(int64_t)(c * 9 + tap) * N + (b * H + ho) * W + wo];
     }
+    dX[(int64_t)c * N + n] = s;
 }
 
 __global__ void cast_bf16_kernel(const float *x, bf16 *y, int64_t n)
@@ -655,19 +653,30 @@ __global__ void relu_bwd_kernel(float *dY, const float *Y, int64_t n)
 }
 
 // db[c] = sum_n dY[c][n]; one block per channel, fixed reduction order
+// one block of 1024 threads per channel; four values per load where the row allows
 __global__ void bias_grad_kernel(const float *dY, int64_t N, float *db)
 {
-    __shared__ float red[256];
+    __shared__ float red[32];
     const int c = blockIdx.x;
+    const float *row = dY + (int64_t)c * N;
     float s = 0.f;
-    for (int64_t n = threadIdx.x; n < N; n += blockDim.x) s += dY[(int64_t)c * N + n];
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
-        if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
-        __syncthreads();
+    if ((N & 3) == 0 && (reinterpret_cast<uintptr_t>(row) & 15) == 0) {
+        const float4 *r4 = reinterpret_cast<const float4 *>(row);
+        for (int64_t n = threadIdx.x; n < N / 4; n += blockDim.x) {
+            const float4 v = r4[n];
+            s += (v.x + v.y) + (v.z + v.w);
+        }
+    } else {
+        for (int64_t n = threadIdx.x; n < N; n += blockDim.x) s += row[n];
     }
-    if (threadIdx.x == 0) db[c] = red[0];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        float t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (threadIdx.x == 0) db[c] = t;
+    }
 }
 
 // 2x2 average pooling: X [C*B][H][W] -> Y [C*B][H/2][W/2]
@@ -1070,8 +1079,10 @@ int amhd_nn_gemm(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K
 int amhd_nn_im2col3(const float *X, int32_t C, int32_t B, int32_t H, int32_t W, void *col, void *stream)
 {
     if (!X || !col || C <= 0 || B <= 0 || H <= 0 || W <= 0) return nn_fail(AMHD_ERR_ARG, "bad im2col arguments");
-    im2col3_kernel<<<blocks_for((int64_t)C * 9 * B * H * W), 256, 0, S(stream)>>>(X, C, B, H, W,
-                                                                                 static_cast<bf16 *>(col));
+    const int64_t n_pix = (int64_t)B * H * W;
+    if (n_pix > INT32_MAX || (int64_t)C * 9 > 65535) return nn_fail(AMHD_ERR_ARG, "im2col size beyond the grid");
+    im2col3_kernel<<<dim3((unsigned)((n_pix + 255) / 256), (unsigned)(C * 9)), 256, 0, S(stream)>>>(
+        X, C, B, H, W, static_cast<bf16 *>(col));
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }
@@ -1079,7 +1090,9 @@ int amhd_nn_im2col3(const float *X, int32_t C, int32_t B, int32_t H, int32_t W, 
 int amhd_nn_col2im3(const float *dcol, int32_t C, int32_t B, int32_t H, int32_t W, float *dX, void *stream)
 {
     if (!dcol || !dX || C <= 0 || B <= 0 || H <= 0 || W <= 0) return nn_fail(AMHD_ERR_ARG, "bad col2im arguments");
-    col2im3_kernel<<<blocks_for((int64_t)C * B * H * W), 256, 0, S(stream)>>>(dcol, C, B, H, W, dX);
+    const int64_t n_pix = (int64_t)B * H * W;
+    if (n_pix > INT32_MAX || C > 65535) return nn_fail(AMHD_ERR_ARG, "col2im size beyond the grid");
+    col2im3_kernel<<<dim3((unsigned)((n_pix + 255) / 256), (unsigned)C), 256, 0, S(stream)>>>(dcol, C, B, H, W, dX);
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }
@@ -1111,7 +1124,7 @@ int amhd_nn_relu_bwd(float *dY, const float *Y, int64_t n, void *stream)
 int amhd_nn_bias_grad(const float *dY, int32_t C, int64_t N, float *db, void *stream)
 {
     if (!dY || !db || C <= 0 || N <= 0) return nn_fail(AMHD_ERR_ARG, "bad bias-grad arguments");
-    bias_grad_kernel<<<C, 256, 0, S(stream)>>>(dY, N, db);
+    bias_grad_kernel<<<C, 1024, 0, S(stream)>>>(dY, N, db);
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }

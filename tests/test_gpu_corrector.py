@@ -227,6 +227,34 @@ def test_graphed_training_step_matches_eager():
     assert float((wa - wb).abs().max()) <= 1e-4 * float(wa.abs().max())
 
 
+@pytest.mark.parametrize("C,B,H,W", [(3, 2, 5, 7), (10, 4, 32, 16), (16, 1, 8, 8)])
+def test_im2col_col2im_bias_grad_against_torch(C, B, H, W):
+    """The convolution helpers against torch: im2col3 (3x3, zero padding) as
+    unfold, col2im3 as its adjoint (fold), bias_grad as a row sum (N both a
+    multiple of 4 and not)."""
+    import torch.nn.functional as Fn
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import stream_ptr
+    g = torch.Generator(device="cuda").manual_seed(C * 100 + H)
+    X = torch.randn((C, B, H, W), device="cuda", generator=g)
+    N = B * H * W
+    col = torch.empty((C * 9, N), dtype=torch.bfloat16, device="cuda")
+    _lib.call("amhd_nn_im2col3", X.data_ptr(), C, B, H, W, col.data_ptr(), stream_ptr())
+    ref = Fn.unfold(X.permute(1, 0, 2, 3), 3, padding=1)            # [B][C*9][H*W]
+    ref = ref.permute(1, 0, 2).reshape(C * 9, N)
+    assert torch.equal(col, ref.to(torch.bfloat16))
+    dcol = torch.randn((C * 9, N), device="cuda", generator=g)
+    dX = torch.empty((C, N), device="cuda")
+    _lib.call("amhd_nn_col2im3", dcol.data_ptr(), C, B, H, W, dX.data_ptr(), stream_ptr())
+    fold = Fn.fold(dcol.view(C * 9, B, H * W).permute(1, 0, 2), (H, W), 3, padding=1)   # [B][C][H][W]
+    assert torch.allclose(dX.view(C, B, H, W), fold.permute(1, 0, 2, 3), atol=1e-5)
+    for n in (N, N - 1):
+        dY = torch.randn((C, n), device="cuda", generator=g)
+        db = torch.empty(C, device="cuda")
+        _lib.call("amhd_nn_bias_grad", dY.data_ptr(), C, n, db.data_ptr(), stream_ptr())
+        assert torch.allclose(db, dY.double().sum(1).float(), atol=1e-3, rtol=1e-5)
+
+
 def test_restrict_pack_apply():
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200._tensors import make_grid, padded_state, stream_ptr
