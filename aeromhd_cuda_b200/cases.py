@@ -105,23 +105,28 @@ def precision_horizon(nx: int = 2048, ny: int = 512, t_end: float = 3.0, every: 
     precision can bring the difference of two runs of an unstable flow.
     Both are reported per variable (precision_errors) every `every` of
     simulated time."""
+    from dataclasses import replace
     cfg = lambda p: shock_interface_config(nx, ny, p, t_end)
     A, B, C = MHDSolver(cfg("fp64")), MHDSolver(cfg("fp64")), MHDSolver(cfg("fp32"))
-    A.initialize()
-    B.initialize()
-    C.initialize()
+    D = MHDSolver(replace(cfg("fp32"), fp32_compensation=True))
+    for s in (A, B, C, D):
+        s.initialize()
     same_initial_state(C, B)
+    D.U = C.U.clone()
     out = {"case": "precision_horizon", "nx": nx, "ny": ny, "times": [], "fp32_vs_fp64": [],
-           "fp64_vs_fp64_of_rounded_start": [], "fp32_vs_fp64_by_quantity": [], "magnitudes": []}
+           "fp64_vs_fp64_of_rounded_start": [], "fp32_vs_fp64_by_quantity": [], "magnitudes": [],
+           "fp32_compensated_vs_fp64": [], "fp32_compensated_vs_fp64_by_quantity": []}
     t = 0.0
     while t < t_end - 1e-12:
         t = min(t_end, t + every)
-        for s in (A, B, C):
+        for s in (A, B, C, D):
             s.advance(t_end=t, chunk=200)
         out["times"].append(t)
         out["fp32_vs_fp64"].append(precision_errors(C, B))
         out["fp64_vs_fp64_of_rounded_start"].append(precision_errors(B, A))
         out["fp32_vs_fp64_by_quantity"].append(state_errors(C, B))
+        out["fp32_compensated_vs_fp64"].append(precision_errors(D, B))
+        out["fp32_compensated_vs_fp64_by_quantity"].append(state_errors(D, B))
         Ub = interior(B).double().abs()
         out["magnitudes"].append({VAR_NAMES[v]: float(Ub[v].mean()) for v in range(10)})
     return out

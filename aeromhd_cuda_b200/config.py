@@ -115,6 +115,9 @@ class Config:
     noise_amp: float = 0.0
     seed: int = 0
     ic_frame: str = "lab"
+    # float32 run loop: accumulate the base state compensated (a float32 low part
+    # kept next to U, amhd_advance_compensated)
+    fp32_compensation: bool = False
 
     @property
     def dx(self) -> float:

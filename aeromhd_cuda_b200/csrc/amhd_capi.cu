@@ -173,7 +173,8 @@ cudaError_t run_dt_reduce(const amhd_grid *g, const void *A, int from_prim, amhd
 int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instance *insts, const int32_t *tile_inst,
                  int n_tiles, int tile_x, int grid, void *U, void *U1, void *U2, amhd_control *ctl, int use_ctl,
                  double dt, double ch, double decay, int fuse_dt, cudaStream_t s, const int32_t *tile_order = nullptr,
-                 const CUtensorMap *tmaps = nullptr, int n_inst = 1, int defer_fill = 0, int32_t *queue = nullptr)
+                 const CUtensorMap *tmaps = nullptr, int n_inst = 1, int defer_fill = 0, int32_t *queue = nullptr,
+                 void *ulo = nullptr)
 {
     StageParams p;
     memset(&p, 0, sizeof p);
@@ -206,6 +207,7 @@ int three_stages(const amhd_grid *g, const amhd_instance &one, const amhd_instan
         }
         p.u0 = U;
         p.uout = out[st - 1];
+        p.ulo = (st == 3 && is_march(tile_x)) ? ulo : nullptr;
         p.fuse_dt = st == 3 ? fuse_dt : 0;
         CK(run_stage(dtype, st, tile_x, p, grid, s));
     }
@@ -621,11 +623,12 @@ int amhd_control_resume(amhd_control *ctl, int32_t n, double snap_t, void *strea
     return AMHD_OK;
 }
 
-int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps, void *stream)
+static int advance_impl(const amhd_grid *g, void *U, void *Ulo, void *U1, void *U2, amhd_control *ctl,
+                        int32_t n_steps, void *stream)
 {
     if (int e = check_grid(g)) return e;
-    const void *ptrs[3] = {U, U1, U2};
-    if (int e = check_padded(g, ptrs, 3)) return e;
+    const void *ptrs[4] = {U, U1, U2, Ulo};
+    if (int e = check_padded(g, ptrs, Ulo ? 4 : 3)) return e;
     if (!ctl) return fail(AMHD_ERR_ARG, "NULL control");
     if (n_steps < 0) return fail(AMHD_ERR_ARG, "n_steps < 0");
     cudaStream_t s = S(stream);
@@ -636,13 +639,27 @@ int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *
     const int defer = is_march(tx);
     for (int k = 0; k < n_steps; ++k) {
         if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, grid, U, U1, U2, ctl, 1, 0, 0, 1, 1, s,
-                                 nullptr, nullptr, 1, defer))
+                                 nullptr, nullptr, 1, defer, nullptr, Ulo))
             return e;
         CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, 1, 0, s, defer));
     }
     if (defer && n_steps > 0)
         if (int e = fill_after_loop(g->dtype, one, nullptr, 1, U, s)) return e;
     return AMHD_OK;
+}
+
+int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps, void *stream)
+{
+    return advance_impl(g, U, nullptr, U1, U2, ctl, n_steps, stream);
+}
+
+int amhd_advance_compensated(const amhd_grid *g, void *U, void *U_lo, void *U1, void *U2, amhd_control *ctl,
+                             int32_t n_steps, void *stream)
+{
+    if (!U_lo) return fail(AMHD_ERR_ARG, "NULL low part");
+    if (g && g->dtype != AMHD_F32) return fail(AMHD_ERR_ARG, "the compensated loop is for float32 states");
+    if (g && !is_march(tile_of(g))) return fail(AMHD_ERR_UNSUPPORTED, "the compensated loop needs the marching kernel");
+    return advance_impl(g, U, U_lo, U1, U2, ctl, n_steps, stream);
 }
 
 int amhd_control_init_split(const amhd_grid *g, void *U, amhd_control *ctl, double t, double t_end, int64_t step,

@@ -128,12 +128,14 @@ struct PowellIn {
 // y; powell_in() gives the Powell inputs; base_at(v) / in_at(v) the cell's
 // value of U0 / of the stage input in plane v.  Without PUSH the caller fills
 // the ghost cells afterwards (march_bc_fill_kernel).
-template <typename R, int STAGE, bool PUSH = true, typename PowellFn, typename BaseFn, typename InFn>
+template <typename R, int STAGE, bool PUSH = true, bool COMP = false, typename PowellFn, typename BaseFn,
+          typename InFn>
 __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_grid &g, R *uout, int i, int j,
                                               const R dfx[NV], const R dfy[NV], PowellFn powell_in, BaseFn base_at,
                                               InFn in_at, double dt, double ch, double decay, unsigned long long q[4],
-                                              bool &bad)
+                                              bool &bad, R *ulo = nullptr)
 {
+    static_assert(!COMP || (STAGE == 3 && kFast<R>), "compensation is for the last float32 stage");
     const int64_t vs = g.var_stride;
     const int pitch = g.pitch;
     const int64_t gi = (int64_t)i * pitch + j;
@@ -181,6 +183,7 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
         rhs[RHOC] += R(0);
     }
     R out[NV];
+    R lo_new[NV];  // compensated stage 3 only: the new low part of the base state
     if (STAGE == 0) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) out[v] = rhs[v];
@@ -202,7 +205,25 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
                     o = __ffma2_rn(dt2, r, b0);
                 } else {
                     const float2 us = make_float2(in_at(v), in_at(v + 1));
-                    o = __ffma2_rn(w2, __ffma2_rn(dt2, r, __ffma2_rn(b0, m1, us)), b0);
+                    if constexpr (COMP) {
+                        // compensated: U = hi + lo; the increment w((U2 - hi) + dt R) is
+                        // the true one (U2 was formed from hi), added to hi + lo as
+                        // lo + inc, then TwoSum(hi, lo + inc) splits the result into the
+                        // stored float32 and its exact rounding error, the new lo
+                        const float2 inc = __fmul2_rn(w2, __ffma2_rn(dt2, r, __ffma2_rn(b0, m1, us)));
+                        const float2 lo = make_float2(ulo[v * g.var_stride + (int64_t)i * g.pitch + j],
+                                                      ulo[(v + 1) * g.var_stride + (int64_t)i * g.pitch + j]);
+                        const float2 t = __fadd2_rn(lo, inc);
+                        o = __fadd2_rn(b0, t);
+                        const float2 bb = __ffma2_rn(b0, m1, o);                 // o - hi
+                        const float2 ea = __ffma2_rn(__ffma2_rn(bb, m1, o), m1, b0);  // hi - (o - bb)
+                        const float2 eb = __ffma2_rn(bb, m1, t);                 // t - bb
+                        const float2 e = __fadd2_rn(ea, eb);
+                        lo_new[v] = e.x;
+                        lo_new[v + 1] = e.y;
+                    } else {
+                        o = __ffma2_rn(w2, __ffma2_rn(dt2, r, __ffma2_rn(b0, m1, us)), b0);
+                    }
                 }
                 out[v] = o.x;
                 out[v + 1] = o.y;
@@ -237,9 +258,14 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
             cc = np_min(np_max(out[RHOC] * fast::rcp(rho), R(0)), R(1));
         else
             cc = np_min(np_max(out[RHOC] / rho, R(0)), R(1));
+        const R rhoc_before = out[RHOC];
         out[RHOC] = rho * cc;
         if (STAGE == 3) {
             if (ch > 0.0) out[PSI] *= R(decay);  // solver.py:331-333
+            if constexpr (COMP) {
+                if (out[RHOC] != rhoc_before) lo_new[RHOC] = R(0);  // clamped: the stored value is the state
+                if (ch > 0.0) lo_new[PSI] *= R(decay);
+            }
             if (p.fuse_dt) {
                 double qd[4];
                 if constexpr (kFast<R>)
@@ -264,6 +290,10 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
     // write the cell, then every ghost that copies it (apply_bc, solver.py:158-197)
 #pragma unroll
     for (int v = 0; v < NV; ++v) uout[v * vs + gi] = out[v];
+    if constexpr (COMP) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) ulo[v * vs + gi] = lo_new[v];
+    }
     if (PUSH && STAGE != 0 && (feeds_ghosts(i, g.nx, g.bc_x) || feeds_ghosts(j, g.ny, g.bc_y)))
         push_ghosts(g, uout, i, j);
 }
@@ -696,7 +726,7 @@ __device__ __forceinline__ void fetch_wait() { asm volatile("cp.async.wait_group
 // One work item: rows [ib, ie) of a 28-column strip.  SPEC: the item runs the
 // van Leer limiter with GLM on (ch > 0), known at compile time -- the walk the
 // solver's loop takes; otherwise both are read at run time.
-template <typename R, int STAGE, bool SPEC, bool TMA>
+template <typename R, int STAGE, bool SPEC, bool TMA, bool COMP>
 __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TMA> &ms, const amhd_instance &in,
                                            int ii, const amhd_grid &g, int item, int lane, double dt, double ch,
                                            double decay, unsigned long long q[4], bool &bad, uint32_t &phase)
@@ -721,6 +751,7 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
     const R *uin = reinterpret_cast<const R *>(p.uin) + in.offset;
     const R *u0 = reinterpret_cast<const R *>(p.u0) + in.offset;
     R *uout = reinterpret_cast<R *>(p.uout) + in.offset;
+    R *ulo = COMP ? reinterpret_cast<R *>(p.ulo) + in.offset : nullptr;
     const bool out_lane = lane >= NG && lane < NG + kMarchCols && j < NG + g.ny;
     // U0 comes from its own buffer unless it is the stage input (stage 1 of a step)
     const bool own_base = STAGE >= 1 && p.u0 != p.uin;
@@ -987,7 +1018,8 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
                     load_cell(s0, ub);
                 auto in_at = [&](int v) { return us[v]; };
                 auto base_at = [&](int v) { return ub[v]; };
-                update_cell_d<R, STAGE, false>(p, g, uout, i, j, dfx, dfy, pw, base_at, in_at, dt, ch, decay, q, bad);
+                update_cell_d<R, STAGE, false, COMP>(p, g, uout, i, j, dfx, dfy, pw, base_at, in_at, dt, ch, decay, q,
+                                                     bad, ulo);
             }
         }
         // rows done with: input row i (slot s0) -> row i+3; U0 of row i -> row i+1
@@ -1008,7 +1040,7 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
 }
 
 // false when a row copy never completed (TMA): the warp then stops
-template <typename R, int STAGE, bool TMA>
+template <typename R, int STAGE, bool TMA, bool COMP>
 __device__ __forceinline__ bool march_item(const StageParams &p, MarchSmem<R, TMA> &ms, int item, int lane,
                                            unsigned long long q[4], bool &bad, amhd_control *&ctl_out,
                                            uint32_t &phase)
@@ -1027,9 +1059,9 @@ __device__ __forceinline__ bool march_item(const StageParams &p, MarchSmem<R, TM
     }
     bool ok;
     if (g.limiter == AMHD_LIMITER_VANLEER && R(ch) > R(0))
-        ok = march_walk<R, STAGE, true, TMA>(p, ms, in, ii, g, item, lane, dt, ch, decay, q, bad, phase);
+        ok = march_walk<R, STAGE, true, TMA, COMP>(p, ms, in, ii, g, item, lane, dt, ch, decay, q, bad, phase);
     else
-        ok = march_walk<R, STAGE, false, TMA>(p, ms, in, ii, g, item, lane, dt, ch, decay, q, bad, phase);
+        ok = march_walk<R, STAGE, false, TMA, COMP>(p, ms, in, ii, g, item, lane, dt, ch, decay, q, bad, phase);
     if (!ok && lane == 0 && ctl != nullptr) atomicOr(&ctl->flags, AMHD_FLAG_TIMEOUT);
     return ok;
 }
@@ -1040,7 +1072,7 @@ __device__ __forceinline__ bool march_item(const StageParams &p, MarchSmem<R, TM
 template <typename R, int STAGE>
 constexpr int kMarchMinBlocks = kFast<R> ? 4 : 2;
 
-template <typename R, int STAGE, bool TMA>
+template <typename R, int STAGE, bool TMA, bool COMP = false>
 __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) march_stage_kernel(
     const __grid_constant__ StageParams p)
 {
@@ -1072,7 +1104,7 @@ __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) ma
         unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
         bool bad = false;
         amhd_control *ctl = nullptr;
-        if (!march_item<R, STAGE, TMA>(p, ms, item, lane, q, bad, ctl, phase)) break;
+        if (!march_item<R, STAGE, TMA, COMP>(p, ms, item, lane, q, bad, ctl, phase)) break;
         if (STAGE == 3 && ctl != nullptr) {
             // warp reduction of the CFL maxima and of the non-finite flag of the item
 #pragma unroll

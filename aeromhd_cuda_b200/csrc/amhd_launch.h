@@ -38,6 +38,9 @@ struct StageParams {
                                    // loop fills them once after its last step, Launch::march_fill)
     int32_t pdl;                   // marching kernel: launch as a programmatic dependent of the
                                    // previous kernel in the stream (run loop)
+    void *ulo;                     // float32 stage 3 of the marching kernel: low part of the base
+                                   // state (U = U_hi + U_lo, same layout as U), read and rewritten
+                                   // so that the base state is accumulated compensated; nullptr: off
     int32_t *queue;                // marching kernel: device work queue {next position, warps
                                    // finished}, zero between launches; nullptr: warp w takes
                                    // positions w, w + warps, ... (static split)

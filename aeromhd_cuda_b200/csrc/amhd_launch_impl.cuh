@@ -125,25 +125,32 @@ static cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 bl
     return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-template <typename R, int ST, bool TMA>
+template <typename R, int ST, bool TMA, bool COMP = false>
 static cudaError_t launch_march_tt(const StageParams &p, int grid, cudaStream_t s)
 {
     constexpr size_t smem = kMarchSmem<R, TMA>;
     static PerDeviceOnce once;  // shared-memory opt-in, once per device
     cudaError_t e = once.run([] {
-        return cudaFuncSetAttribute(march_stage_kernel<R, ST, TMA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem);
+        return cudaFuncSetAttribute(march_stage_kernel<R, ST, TMA, COMP>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     });
     if (e != cudaSuccess) return e;
-    if (p.pdl) return launch_dependent(march_stage_kernel<R, ST, TMA>, dim3(grid), dim3(kMarchThreads), smem, s, p);
-    march_stage_kernel<R, ST, TMA><<<grid, kMarchThreads, smem, s>>>(p);
+    if (p.pdl)
+        return launch_dependent(march_stage_kernel<R, ST, TMA, COMP>, dim3(grid), dim3(kMarchThreads), smem, s, p);
+    march_stage_kernel<R, ST, TMA, COMP><<<grid, kMarchThreads, smem, s>>>(p);
     return cudaGetLastError();
 }
 
-// rows staged by TMA (p.use_tma: the tensor maps are in p) or by per-lane cp.async
+// rows staged by TMA (p.use_tma: the tensor maps are in p) or by per-lane cp.async;
+// the compensated last stage (p.ulo, float32) is built with cp.async rows only
 template <typename R, int ST>
 static cudaError_t launch_march_t(const StageParams &p, int grid, cudaStream_t s)
 {
+    if constexpr (ST == 3 && kFast<R>)
+        if (p.ulo != nullptr) {
+            if (p.use_tma) return cudaErrorNotSupported;
+            return launch_march_tt<R, ST, false, true>(p, grid, s);
+        }
     return p.use_tma ? launch_march_tt<R, ST, true>(p, grid, s) : launch_march_tt<R, ST, false>(p, grid, s);
 }
 

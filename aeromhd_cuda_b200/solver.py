@@ -73,6 +73,10 @@ class MHDSolver:
         self._store1, self._U1 = padded_state(config.nx, config.ny, self.dtype, self.device)
         self._store2, self._U2 = padded_state(config.nx, config.ny, self.dtype, self.device)
         self._ctl = control_tensor(1, self.device)
+        # float32 run loop with compensation: low part of the base state (zero at every loop start)
+        self._compensated = config.precision == "fp32" and bool(config.fp32_compensation)
+        self._store_lo, self._U_lo = (padded_state(config.nx, config.ny, self.dtype, self.device)
+                                      if self._compensated else (None, None))
         self._diag_out = torch.zeros(8, dtype=torch.float64, device=self.device)
         self._diag_rows = torch.zeros(7 * config.nx, dtype=torch.float64, device=self.device)
         self._diag_colour = torch.zeros(config.nx + config.ny, dtype=torch.float64, device=self.device)
@@ -315,13 +319,19 @@ class MHDSolver:
     def _loop_init(self, t_end: float, max_steps: int):
         """amhd_control_init: dt/ch of the current state, exactly as the loop head computes them."""
         self._ebnd_host = self._cumulative_boundary_energy
+        if self._compensated:
+            self._store_lo.zero_()  # U as given is exactly its float32 values
         _lib.call("amhd_control_init", self._grid(), ptr(self._U), ptr(self._ctl), float(self.t), float(t_end),
                   int(self.step), int(max_steps), stream_ptr())
         self._loop_ready = True
 
     def _advance_eager(self, n: int):
-        _lib.call("amhd_advance", self._grid(), ptr(self._U), ptr(self._U1), ptr(self._U2), ptr(self._ctl), int(n),
-                  stream_ptr())
+        if self._compensated:
+            _lib.call("amhd_advance_compensated", self._grid(), ptr(self._U), ptr(self._U_lo), ptr(self._U1),
+                      ptr(self._U2), ptr(self._ctl), int(n), stream_ptr())
+        else:
+            _lib.call("amhd_advance", self._grid(), ptr(self._U), ptr(self._U1), ptr(self._U2), ptr(self._ctl),
+                      int(n), stream_ptr())
 
     def _advance(self, n: int, graph: bool = True):
         """n device-loop iterations: as a CUDA graph replay (captured on first use) or eagerly."""

@@ -212,6 +212,16 @@ int amhd_control_resume(amhd_control *ctl, int32_t n, double snap_t, void *strea
  * dependents of one another (each waits for the one before on the device). */
 int amhd_advance(const amhd_grid *g, void *U, void *U1, void *U2, amhd_control *ctl, int32_t n_steps,
                  void *stream);
+/* amhd_advance for a float32 state accumulated with compensation: U_lo (same
+ * padded layout and dtype as U) holds the low part of the base state, U_hi +
+ * U_lo.  Stage 3 adds the step's increment to hi + lo and splits the sum into
+ * the stored float32 U and its exact rounding error (TwoSum), the new U_lo,
+ * so that the rounding of the stored state does not accumulate from step to
+ * step; stages 1 and 2 read U (the increment they feed is exact either way).
+ * Zero U_lo whenever U is set or changed outside this loop.  Marching kernel
+ * only.  No counterpart in the reference (float64 there). */
+int amhd_advance_compensated(const amhd_grid *g, void *U, void *U_lo, void *U1, void *U2, amhd_control *ctl,
+                             int32_t n_steps, void *stream);
 /* The run loop taken apart, for drivers that act between its pieces (a grid
  * split over GPUs by x rows exchanges ghost rows after every stage and
  * max-reduces the CFL maxima ctl->red[4] across GPUs before the dt):
