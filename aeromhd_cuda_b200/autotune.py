@@ -47,13 +47,14 @@ def candidates(ensemble: bool, precision: str = "fp32", tile_xs: Sequence[int] =
 
 
 def choose(timings: Dict[Candidate, float], rel_tie: float = 0.01) -> Candidate:
-    """Fastest candidate; within rel_tie of the best, prefer the simplest
-    (instance order, one CTA per tile, the tiled kernel, then the smaller tile)."""
+    """Fastest candidate; within rel_tie of the best, prefer the library's
+    defaults (instance order, a persistent grid -- one launch per stage --,
+    the marching kernel, then the shorter item or tile)."""
     if not timings:
         raise ValueError("no timings")
     best = min(timings.values())
     near = [c for c, t in timings.items() if t <= best * (1.0 + rel_tie)]
-    return sorted(near, key=lambda c: (c.order != "instance", c.ctas != -1, c.tile_x < 0, abs(c.tile_x)))[0]
+    return sorted(near, key=lambda c: (c.order != "instance", c.ctas != 0, c.tile_x > 0, abs(c.tile_x)))[0]
 
 
 def signature(precision: str, sizes: Iterable[tuple], device_name: str = "") -> str:

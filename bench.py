@@ -80,7 +80,9 @@ def parse_args(argv=None):
     ap.add_argument("--ensemble-ctas", type=int, default=0,
                     help="ensemble grid: 0 persistent (work queue, the default), -1 one CTA per 4 items, "
                          ">0 that many CTAs")
-    ap.add_argument("--ensemble-tune", action="store_true",
+    ap.add_argument("--no-ensemble-tune", dest="ensemble_tune", action="store_false",
+                    help="time the ensemble with its default schedule instead of the autotuned one")
+    ap.add_argument("--ensemble-tune", action="store_true", default=True,
                     help="choose the ensemble's work shape, order and grid with the autotuner first")
     return ap.parse_args(argv)
 
@@ -563,8 +565,11 @@ def run_ensemble(a, world):
     ens.start()
     tuned = None
     if a.ensemble_tune and a.tile_x == 0:
-        # work shape, order and grid chosen by the autotuner (untimed; fresh cache)
-        best, timings = tune_ensemble(ens, steps=5, cache=Cache())
+        # work shape, order and grid chosen by the autotuner (untimed; fresh cache): the
+        # marching work shapes, both grids and two work orders, 5 eager steps each
+        from aeromhd_cuda_b200.autotune import Candidate
+        cands = [Candidate(tx, o, g) for tx in (-16, -24, -32) for g in (0, -1) for o in ("instance", "largest_first")]
+        best, timings = tune_ensemble(ens, steps=5, cands=cands, cache=Cache())
         tuned = {"candidates": len(timings), "best_ms_per_step": round(min(timings.values()) / 5 * 1e3, 4)}
     k = max(3, min(a.steps // 5, 200))
     ens.advance(k)  # warm-up + graph capture

@@ -75,7 +75,9 @@ def test_candidates_and_choice():
     t = {Candidate(8, "instance", -1): 1.0, Candidate(4, "instance", -1): 1.005, Candidate(16, "interleave", 0): 1.2}
     assert choose(t) == Candidate(4, "instance", -1)  # tie within 1%: simplest, then smaller tile
     t = {Candidate(8, "instance", -1): 1.0, Candidate(-32, "instance", -1): 1.004}
-    assert choose(t) == Candidate(8, "instance", -1)  # tie: the tiled kernel
+    assert choose(t) == Candidate(-32, "instance", -1)  # tie: the marching kernel (the library default)
+    t = {Candidate(-24, "instance", -1): 1.0, Candidate(-24, "instance", 0): 1.006}
+    assert choose(t) == Candidate(-24, "instance", 0)  # tie: the persistent grid (one launch per stage)
     t = {Candidate(8, "instance", -1): 1.0, Candidate(-32, "instance", -1): 0.7}
     assert choose(t) == Candidate(-32, "instance", -1)
 
