@@ -116,7 +116,8 @@ class Config:
     seed: int = 0
     ic_frame: str = "lab"
     # float32 run loop: accumulate the base state compensated (a float32 low part
-    # kept next to U, amhd_advance_compensated)
+    # kept next to U, amhd_advance_compensated).  The low part starts at zero at
+    # every loop start and is not part of U or of a checkpoint.
     fp32_compensation: bool = False
 
     @property
