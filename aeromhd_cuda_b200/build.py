@@ -62,7 +62,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         return LIB
     os.makedirs(BUILD, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
+    objs, cmds = [], []
     for src, extra in UNITS.items():
         obj = os.path.join(BUILD, src.replace(".cu", ".o"))
         cmd = [nvcc, *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
@@ -70,8 +70,13 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             cmd.insert(1, "-Xptxas=-v")
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.check_call(cmd)
+        cmds.append(cmd)
         objs.append(obj)
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     tmp = LIB + ".tmp"
     cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     if verbose:
