@@ -128,17 +128,15 @@ struct PowellIn {
 // y; powell_in() gives the Powell inputs; base_at(v) / in_at(v) the cell's
 // value of U0 / of the stage input in plane v.  Without PUSH the caller fills
 // the ghost cells afterwards (march_bc_fill_kernel).
-template <typename R, int STAGE, bool PUSH = true, bool COMP = false, typename PowellFn, typename BaseFn,
-          typename InFn>
-__device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_grid &g, R *uout, int i, int j,
-                                              const R dfx[NV], const R dfy[NV], PowellFn powell_in, BaseFn base_at,
-                                              InFn in_at, double dt, double ch, double decay, unsigned long long q[4],
-                                              bool &bad, R *ulo = nullptr)
+// cell_values computes the new values (out; the compensated low part in lo_new)
+// without storing them; update_cell_d stores them as well.
+template <typename R, int STAGE, bool COMP = false, typename PowellFn, typename BaseFn, typename InFn>
+__device__ __forceinline__ void cell_values(const StageParams &p, const amhd_grid &g, int i, int j, const R dfx[NV],
+                                            const R dfy[NV], PowellFn powell_in, BaseFn base_at, InFn in_at,
+                                            double dt, double ch, double decay, unsigned long long q[4], bool &bad,
+                                            const R *ulo, R out[NV], R lo_new[NV])
 {
     static_assert(!COMP || (STAGE == 3 && kFast<R>), "compensation is for the last float32 stage");
-    const int64_t vs = g.var_stride;
-    const int pitch = g.pitch;
-    const int64_t gi = (int64_t)i * pitch + j;
     R rhs[NV];
     const R dx = R(g.dx), dy = R(g.dy);
     if constexpr (kFast<R>) {
@@ -182,8 +180,6 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
         rhs[PSI] += R(0);
         rhs[RHOC] += R(0);
     }
-    R out[NV];
-    R lo_new[NV];  // compensated stage 3 only: the new low part of the base state
     if (STAGE == 0) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) out[v] = rhs[v];
@@ -287,6 +283,21 @@ __device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_g
             }
         }
     }
+}
+
+template <typename R, int STAGE, bool PUSH = true, bool COMP = false, typename PowellFn, typename BaseFn,
+          typename InFn>
+__device__ __forceinline__ void update_cell_d(const StageParams &p, const amhd_grid &g, R *uout, int i, int j,
+                                              const R dfx[NV], const R dfy[NV], PowellFn powell_in, BaseFn base_at,
+                                              InFn in_at, double dt, double ch, double decay, unsigned long long q[4],
+                                              bool &bad, R *ulo = nullptr)
+{
+    const int64_t vs = g.var_stride;
+    const int64_t gi = (int64_t)i * g.pitch + j;
+    R out[NV];
+    R lo_new[NV];  // compensated stage 3 only: the new low part of the base state
+    cell_values<R, STAGE, COMP>(p, g, i, j, dfx, dfy, powell_in, base_at, in_at, dt, ch, decay, q, bad, ulo, out,
+                                lo_new);
     // write the cell, then every ghost that copies it (apply_bc, solver.py:158-197)
 #pragma unroll
     for (int v = 0; v < NV; ++v) uout[v * vs + gi] = out[v];
@@ -1072,22 +1083,13 @@ __device__ __forceinline__ bool march_item(const StageParams &p, MarchSmem<R, TM
 template <typename R, int STAGE>
 constexpr int kMarchMinBlocks = kFast<R> ? 4 : 2;
 
-template <typename R, int STAGE, bool TMA, bool COMP = false>
-__global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) march_stage_kernel(
-    const __grid_constant__ StageParams p)
+// The work loop of a marching kernel's warp: take items (from the queue or the
+// static split), run each (run_item(item, q, bad, ctl) returns false when the
+// warp must stop), reduce each item's CFL maxima and non-finite flag into its
+// instance's control block (last stage), and reset the queue at the end.
+template <int STAGE, typename ItemFn>
+__device__ __forceinline__ void march_items(const StageParams &p, int lane, ItemFn run_item)
 {
-    extern __shared__ __align__(128) unsigned char march_smem[];
-    // run loop: the next launch may take SM slots as this grid drains; nothing
-    // of the previous launch (stage input, controls) is read before it is done
-    pdl_trigger();
-    pdl_wait();
-    MarchSmem<R, TMA> &ms = reinterpret_cast<MarchSmem<R, TMA> *>(march_smem)[threadIdx.x >> 5];
-    const int lane = threadIdx.x & 31;
-    uint32_t phase = 0;  // TMA: parity of the next completion of each of the warp's 4 barriers
-    if constexpr (TMA) {
-        if (lane < 4) tma::mbar_init(&ms.bar[lane], 1);
-        __syncwarp();
-    }
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int n_warps = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
     // work positions: from the queue (each warp takes the next free position when it
@@ -1104,7 +1106,7 @@ __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) ma
         unsigned long long q[4] = {0ull, 0ull, 0ull, 0ull};
         bool bad = false;
         amhd_control *ctl = nullptr;
-        if (!march_item<R, STAGE, TMA, COMP>(p, ms, item, lane, q, bad, ctl, phase)) break;
+        if (!run_item(item, q, bad, ctl)) break;
         if (STAGE == 3 && ctl != nullptr) {
             // warp reduction of the CFL maxima and of the non-finite flag of the item
 #pragma unroll
@@ -1127,6 +1129,27 @@ __global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) ma
             atomicExch(&p.queue[1], 0);
         }
     }
+}
+
+template <typename R, int STAGE, bool TMA, bool COMP = false>
+__global__ void __launch_bounds__(kMarchThreads, (kMarchMinBlocks<R, STAGE>)) march_stage_kernel(
+    const __grid_constant__ StageParams p)
+{
+    extern __shared__ __align__(128) unsigned char march_smem[];
+    // run loop: the next launch may take SM slots as this grid drains; nothing
+    // of the previous launch (stage input, controls) is read before it is done
+    pdl_trigger();
+    pdl_wait();
+    MarchSmem<R, TMA> &ms = reinterpret_cast<MarchSmem<R, TMA> *>(march_smem)[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    uint32_t phase = 0;  // TMA: parity of the next completion of each of the warp's 4 barriers
+    if constexpr (TMA) {
+        if (lane < 4) tma::mbar_init(&ms.bar[lane], 1);
+        __syncwarp();
+    }
+    march_items<STAGE>(p, lane, [&](int item, unsigned long long q[4], bool &bad, amhd_control *&ctl) {
+        return march_item<R, STAGE, TMA, COMP>(p, ms, item, lane, q, bad, ctl, phase);
+    });
 }
 
 // ---------------------------------------------------------------------------
