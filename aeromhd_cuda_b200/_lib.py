@@ -124,6 +124,8 @@ _SIGS = {
     "amhd_nn_im2col3": ([_P, _I32, _I32, _I32, _I32, _P, _P], _c.c_int),
     "amhd_nn_col2im3": ([_P, _I32, _I32, _I32, _I32, _P, _P], _c.c_int),
     "amhd_nn_cast_bf16": ([_P, _P, _I64, _P], _c.c_int),
+    "amhd_nn_flip3": ([_P, _I32, _I32, _I32, _P, _P], _c.c_int),
+    "amhd_nn_pad_cols": ([_P, _I32, _I32, _I32, _P, _P], _c.c_int),
     "amhd_nn_bias_act": ([_P, _P, _I32, _I64, _I32, _P], _c.c_int),
     "amhd_nn_relu_bwd": ([_P, _P, _I64, _P], _c.c_int),
     "amhd_nn_bias_grad": ([_P, _I32, _I64, _P, _P], _c.c_int),

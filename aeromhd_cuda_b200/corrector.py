@@ -52,6 +52,10 @@ def architecture(ch=(32, 64, 128, 256), nin: int = 10, nout: int = 10) -> List[C
     ]
 
 
+def _round8(k: int) -> int:
+    return (k + 7) // 8 * 8
+
+
 def n_params(specs: List[ConvSpec]) -> int:
     return sum(s.cout * s.cin * s.k * s.k + s.cout for s in specs)
 
@@ -92,6 +96,7 @@ class Corrector:
         self._hyper = torch.zeros(6, dtype=F32, device=self.device)  # lr, b1, b2, eps, c1, c2
         self._graphs: Dict[int, tuple] = {}
         self._ws: Dict[str, torch.Tensor] = {}
+        self._pad_shapes: Dict[str, tuple] = {}  # workspaces whose padding rows are zeroed
         self._act: Dict[str, torch.Tensor] = {}
         self.in_mean = torch.zeros(10, device=self.device)
         self.in_istd = torch.ones(10, device=self.device)
@@ -106,6 +111,16 @@ class Corrector:
             self._ws[key] = t
         return t[:n].view(*shape)
 
+    def _padded_rows(self, key: str, rows: int, rows_p: int, N: int) -> torch.Tensor:
+        """A BF16 [rows_p][N] workspace whose rows rows .. rows_p-1 are zero: zeroed
+        when the buffer or its shape is new (the eager step before a graph
+        capture), never inside a captured step."""
+        t = self._buf(key, (rows_p, N), BF16)
+        if rows_p > rows and self._pad_shapes.get(key) != (rows, rows_p, N, t.data_ptr()):
+            t[rows:].zero_()
+            self._pad_shapes[key] = (rows, rows_p, N, t.data_ptr())
+        return t
+
     def host_params(self) -> dict:
         return {s.name: {"w": self.p[s.name]["w"].detach().cpu().reshape(s.cout, s.cin, s.k, s.k).clone(),
                          "b": self.p[s.name]["b"].detach().cpu().clone()} for s in self.specs}
@@ -114,16 +129,21 @@ class Corrector:
     def _conv_fwd(self, s: ConvSpec, X: torch.Tensor, B: int, H: int, W: int) -> torch.Tensor:
         N = B * H * W
         st = stream_ptr()
+        K = s.cin * s.k * s.k
+        Kp = _round8(K)  # GEMM operands with a row pitch of whole 16-byte pieces (the TMA path)
+        wb = self.p[s.name]["wb"]
         if s.k == 3:
-            col = self._buf(f"{s.name}.col", (s.cin * 9, N), BF16)
+            col = self._padded_rows(f"{s.name}.col", K, Kp, N)
             _lib.call("amhd_nn_im2col3", ptr(X), s.cin, B, H, W, ptr(col), st)
         else:
-            col = self._buf(f"{s.name}.col", (s.cin, N), BF16)
+            col = self._padded_rows(f"{s.name}.col", K, Kp, N)
             _lib.call("amhd_nn_cast_bf16", ptr(X), ptr(col), X.numel(), st)
-        K = s.cin * s.k * s.k
+        if Kp != K:
+            wp = self._buf(f"{s.name}.wpad", (s.cout, Kp), BF16)
+            _lib.call("amhd_nn_pad_cols", ptr(wb), s.cout, K, Kp, ptr(wp), st)
+            wb = wp
         Y = self._buf(f"{s.name}.y", (s.cout, N))
-        _lib.call("amhd_nn_gemm", 0, 0, s.cout, N, K, ptr(self.p[s.name]["wb"]), K, ptr(col), N, ptr(Y), N,
-                  1.0, 0.0, 1, st)
+        _lib.call("amhd_nn_gemm", 0, 0, s.cout, N, Kp, ptr(wb), Kp, ptr(col), N, ptr(Y), N, 1.0, 0.0, 1, st)
         _lib.call("amhd_nn_bias_act", ptr(Y), ptr(self.p[s.name]["b"]), s.cout, N, int(s.relu), st)
         return Y
 
@@ -138,7 +158,7 @@ class Corrector:
         _lib.call("amhd_nn_bias_grad", ptr(dY), s.cout, N, ptr(P["gb"]), st)
         dYb = self._buf(f"{s.name}.dyb", (s.cout, N), BF16)
         _lib.call("amhd_nn_cast_bf16", ptr(dY), ptr(dYb), dY.numel(), st)
-        col = self._ws[f"{s.name}.col"][: K * N]
+        col = self._ws[f"{s.name}.col"][: K * N]  # the forward's columns (its first K rows)
         splits = max(1, min(64, N // 4096))
         # dW[cout][K] = dY[cout][N] x col[K][N]^T
         _lib.call("amhd_nn_gemm", 0, 1, s.cout, K, N, ptr(dYb), N, ptr(col), N, ptr(P["gw"]), K, 1.0, 0.0,
@@ -146,10 +166,16 @@ class Corrector:
         if not need_dx:
             return None
         if s.k == 3:
-            dcol = self._buf(f"{s.name}.dcol", (K, N))
-            _lib.call("amhd_nn_gemm", 1, 0, K, N, s.cout, ptr(P["wb"]), K, ptr(dYb), N, ptr(dcol), N, 1.0, 0.0, 1, st)
+            # the adjoint of the zero-padded 3x3 convolution: the same convolution of dY
+            # with the transposed weights turned by 180 degrees (amhd_nn_flip3), one GEMM
+            # of K = cout x 9 instead of a [cin x 9][N] product and its col2im gather
+            Kg = _round8(s.cout * 9)
+            colg = self._padded_rows(f"{s.name}.colg", s.cout * 9, Kg, N)
+            _lib.call("amhd_nn_im2col3", ptr(dY), s.cout, B, H, W, ptr(colg), st)
+            wt = self._buf(f"{s.name}.wt", (s.cin, Kg), BF16)
+            _lib.call("amhd_nn_flip3", ptr(P["wb"]), s.cout, s.cin, Kg, ptr(wt), st)
             dX = self._buf(f"{s.name}.dx", (s.cin, N))
-            _lib.call("amhd_nn_col2im3", ptr(dcol), s.cin, B, H, W, ptr(dX), st)
+            _lib.call("amhd_nn_gemm", 0, 0, s.cin, N, Kg, ptr(wt), Kg, ptr(colg), N, ptr(dX), N, 1.0, 0.0, 1, st)
         else:
             dX = self._buf(f"{s.name}.dx", (s.cin, N))
             _lib.call("amhd_nn_gemm", 1, 0, s.cin, N, s.cout, ptr(P["wb"]), s.cin, ptr(dYb), N, ptr(dX), N,

@@ -45,6 +45,8 @@ int nn_fail(int code, const char *fmt, ...)
 
 inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
 inline int blocks_for(int64_t n, int threads = 256)
 {
     int64_t b = (n + threads - 1) / threads;
@@ -630,6 +632,199 @@ __global__ void col2im3_kernel(const float *dcol, int C, int B, int H, int W, fl
     dX[(int64_t)c * N + n] = s;
 }
 
+// The same convolution helpers, several pixels per thread (used when the image
+// rows allow): identical values and summation order, 32-bit index arithmetic
+// once per thread, 16-byte loads and stores.
+//
+// im2col, W % 8 == 0: a thread takes 8 consecutive pixels of one image row and
+// writes all 9 taps of one channel (grid: x over the 8-pixel groups, y over C)
+__global__ void im2col3_vec8_kernel(const float *X, int H, int W, int N, bf16 *col)
+{
+    const int n0 = 8 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (n0 >= N) return;
+    const int c = blockIdx.y;
+    const int q = n0 / W, w0 = n0 - q * W, h = q % H;  // q = b H + h
+    const float *xc = X + (int64_t)c * N;
+#pragma unroll
+    for (int dy = -1; dy <= 1; ++dy) {
+        float v[10];  // source columns w0 - 1 .. w0 + 8 of image row h + dy (zero outside the image)
+        if (h + dy >= 0 && h + dy < H) {
+            const float *r = xc + (int64_t)(q + dy) * W;
+            const float4 a = *reinterpret_cast<const float4 *>(r + w0);
+            const float4 b = *reinterpret_cast<const float4 *>(r + w0 + 4);
+            v[0] = w0 > 0 ? r[w0 - 1] : 0.f;
+            v[1] = a.x, v[2] = a.y, v[3] = a.z, v[4] = a.w;
+            v[5] = b.x, v[6] = b.y, v[7] = b.z, v[8] = b.w;
+            v[9] = w0 + 8 < W ? r[w0 + 8] : 0.f;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 10; ++i) v[i] = 0.f;
+        }
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int tap = 3 * (dy + 1) + dx + 1;
+            uint32_t w[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const __nv_bfloat162 t = __floats2bfloat162_rn(v[2 * i + 1 + dx], v[2 * i + 2 + dx]);
+                w[i] = *reinterpret_cast<const uint32_t *>(&t);
+            }
+            *reinterpret_cast<uint4 *>(col + (int64_t)(c * 9 + tap) * N + n0) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+}
+
+// col2im, W % 4 == 0: 4 consecutive pixels of one image row per thread, taps in
+// the order of col2im3_kernel (grid: x over the 4-pixel groups, y over C)
+__global__ void col2im3_vec4_kernel(const float *dcol, int H, int W, int N, float *dX)
+{
+    const int n0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (n0 >= N) return;
+    const int c = blockIdx.y;
+    const int q = n0 / W, w0 = n0 - q * W, h = q % H;
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f, s3 = 0.f;
+#pragma unroll
+    for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+        if (h - dy < 0 || h - dy >= H) continue;
+        const float *r = dcol + (int64_t)(c * 9 + tap) * N + (int64_t)(q - dy) * W;
+        const float4 a = *reinterpret_cast<const float4 *>(r + w0);
+        // pixel w0 + i reads column w0 + i - dx of the row
+        if (dx == 0) {
+            s0 += a.x, s1 += a.y, s2 += a.z, s3 += a.w;
+        } else if (dx == 1) {
+            if (w0 > 0) s0 += r[w0 - 1];
+            s1 += a.x, s2 += a.y, s3 += a.z;
+        } else {
+            s0 += a.y, s1 += a.z, s2 += a.w;
+            if (w0 + 4 < W) s3 += r[w0 + 4];
+        }
+    }
+    *reinterpret_cast<float4 *>(dX + (int64_t)c * N + n0) = make_float4(s0, s1, s2, s3);
+}
+
+// float -> bfloat16, four values per thread (n % 4 == 0, 16-byte aligned)
+__global__ void cast_bf16_vec4_kernel(const float4 *x, uint2 *y, int64_t n4)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n4; k += (int64_t)gridDim.x * blockDim.x) {
+        const float4 v = x[k];
+        const __nv_bfloat162 a = __floats2bfloat162_rn(v.x, v.y), b = __floats2bfloat162_rn(v.z, v.w);
+        y[k] = make_uint2(*reinterpret_cast<const uint32_t *>(&a), *reinterpret_cast<const uint32_t *>(&b));
+    }
+}
+
+// bias (+ ReLU), N % 4 == 0: grid y over the channels, x over the channel's float4s
+__global__ void bias_act_vec4_kernel(float4 *Y, const float *bias, int64_t n4, int relu)
+{
+    const float b = bias[blockIdx.y];
+    float4 *row = Y + (int64_t)blockIdx.y * n4;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n4; k += (int64_t)gridDim.x * blockDim.x) {
+        float4 v = row[k];
+        v.x += b, v.y += b, v.z += b, v.w += b;
+        if (relu) v.x = fmaxf(v.x, 0.f), v.y = fmaxf(v.y, 0.f), v.z = fmaxf(v.z, 0.f), v.w = fmaxf(v.w, 0.f);
+        row[k] = v;
+    }
+}
+
+__global__ void relu_bwd_vec4_kernel(float4 *dY, const float4 *Y, int64_t n4)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n4; k += (int64_t)gridDim.x * blockDim.x) {
+        const float4 y = Y[k];
+        float4 d = dY[k];
+        if (!(y.x > 0.f)) d.x = 0.f;
+        if (!(y.y > 0.f)) d.y = 0.f;
+        if (!(y.z > 0.f)) d.z = 0.f;
+        if (!(y.w > 0.f)) d.w = 0.f;
+        dY[k] = d;
+    }
+}
+
+__global__ void axpy_vec4_kernel(float4 *y, const float4 *x, float a, int64_t n4)
+{
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n4; k += (int64_t)gridDim.x * blockDim.x) {
+        const float4 u = x[k];
+        float4 v = y[k];
+        v.x += a * u.x, v.y += a * u.y, v.z += a * u.z, v.w += a * u.w;
+        y[k] = v;
+    }
+}
+
+// 2x2 pooling / nearest upsampling and their gradients, one plane per grid row
+// (y), four input or output columns per thread (W % 4 == 0 for pooling, w % 2
+// == 0 for upsampling), the sums in the scalar kernels' order
+__global__ void pool2_vec_kernel(const float *X, int H, int W, float *Y)
+{
+    const int h2 = H / 2, w2 = W / 2;
+    const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x);  // first of two outputs
+    if (k >= h2 * w2) return;
+    const int h = k / w2, w = k - h * w2;
+    const float *x = X + (int64_t)blockIdx.y * H * W + (int64_t)(2 * h) * W + 2 * w;
+    const float4 a = *reinterpret_cast<const float4 *>(x), b = *reinterpret_cast<const float4 *>(x + W);
+    *reinterpret_cast<float2 *>(Y + (int64_t)blockIdx.y * h2 * w2 + k) =
+        make_float2(0.25f * (a.x + a.y + b.x + b.y), 0.25f * (a.z + a.w + b.z + b.w));
+}
+
+__global__ void pool2_bwd_vec_kernel(const float *dY, int H, int W, float *dX)
+{
+    const int h2 = H / 2, w2 = W / 2;
+    const int k = 4 * (blockIdx.x * blockDim.x + threadIdx.x);  // first of four outputs
+    if (k >= H * W) return;
+    const int h = k / W, w = k - h * W;
+    const float *d = dY + (int64_t)blockIdx.y * h2 * w2 + (int64_t)(h / 2) * w2 + w / 2;
+    const float u = 0.25f * d[0], v = 0.25f * d[1];
+    *reinterpret_cast<float4 *>(dX + (int64_t)blockIdx.y * H * W + k) = make_float4(u, u, v, v);
+}
+
+__global__ void up2_vec_kernel(const float *X, int h, int w, float *Y)
+{
+    const int W = 2 * w, H = 2 * h;
+    const int k = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (k >= H * W) return;
+    const int y = k / W, x = k - y * W;
+    const float *s = X + (int64_t)blockIdx.y * h * w + (int64_t)(y / 2) * w + x / 2;
+    const float u = s[0], v = s[1];
+    *reinterpret_cast<float4 *>(Y + (int64_t)blockIdx.y * H * W + k) = make_float4(u, u, v, v);
+}
+
+__global__ void up2_bwd_vec_kernel(const float *dY, int h, int w, float *dX)
+{
+    const int W = 2 * w;
+    const int k = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (k >= h * w) return;
+    const int y = k / w, x = k - y * w;
+    const float *d = dY + (int64_t)blockIdx.y * 4 * h * w + (int64_t)(2 * y) * W + 2 * x;
+    const float4 a = *reinterpret_cast<const float4 *>(d), b = *reinterpret_cast<const float4 *>(d + W);
+    *reinterpret_cast<float2 *>(dX + (int64_t)blockIdx.y * h * w + k) =
+        make_float2(a.x + a.y + b.x + b.y, a.z + a.w + b.z + b.w);
+}
+
+// Weights of a 3x3 convolution, w[co][ci*9 + tap] (BF16), rearranged for the
+// gradient with respect to its input: wt[ci][co*9 + t] = w[co][ci*9 + 8 - t]
+// (transposed, taps turned by 180 degrees: the adjoint of a zero-padded 3x3
+// convolution is the convolution of dY with these weights), columns
+// cout*9 .. ldo-1 zero.  One thread per output value.
+__global__ void flip3_kernel(const bf16 *w, int cout, int cin, int ldo, bf16 *wt)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= cin * ldo) return;
+    const int ci = k / ldo, j = k - ci * ldo;
+    bf16 v = __float2bfloat16(0.f);
+    if (j < cout * 9) {
+        const int co = j / 9, t = j - 9 * co;
+        v = w[(int64_t)co * cin * 9 + ci * 9 + 8 - t];
+    }
+    wt[k] = v;
+}
+
+// rows x cols BF16 values into rows x ldo (columns cols .. ldo-1 zero)
+__global__ void pad_cols_kernel(const bf16 *w, int rows, int cols, int ldo, bf16 *out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= rows * ldo) return;
+    const int r = k / ldo, c = k - r * ldo;
+    out[k] = c < cols ? w[(int64_t)r * cols + c] : __float2bfloat16(0.f);
+}
+
 __global__ void cast_bf16_kernel(const float *x, bf16 *y, int64_t n)
 {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
@@ -980,9 +1175,15 @@ int tma_gemm(int transA, int transB, int M, int N, int K, const void *A, int lda
     return AMHD_OK;
 }
 
-// shapes on which the tcgen05 pipeline beats mma.sync (B200): at least half a
-// 128-row MMA tile, or a long K (weight gradients)
-bool prefer_tc(int M, int N, int K) { return (M >= 64 && N >= 64) || K >= 4096; }
+// shapes on which the tcgen05 pipeline beats mma.sync (B200): a full 64-column
+// output tile, whatever M (the rows past M are zero-filled by the TMA box and
+// not stored: at M = 32 / 10, N = 262144, K = 288 tcgen05 runs 54 / 17 TFLOP/s
+// against 29 / 10), or a long K (weight gradients)
+bool prefer_tc(int M, int N, int K)
+{
+    (void)M;
+    return N >= 64 || K >= 4096;
+}
 
 }  // namespace
 
@@ -1081,8 +1282,12 @@ int amhd_nn_im2col3(const float *X, int32_t C, int32_t B, int32_t H, int32_t W, 
     if (!X || !col || C <= 0 || B <= 0 || H <= 0 || W <= 0) return nn_fail(AMHD_ERR_ARG, "bad im2col arguments");
     const int64_t n_pix = (int64_t)B * H * W;
     if (n_pix > INT32_MAX || (int64_t)C * 9 > 65535) return nn_fail(AMHD_ERR_ARG, "im2col size beyond the grid");
-    im2col3_kernel<<<dim3((unsigned)((n_pix + 255) / 256), (unsigned)(C * 9)), 256, 0, S(stream)>>>(
-        X, C, B, H, W, static_cast<bf16 *>(col));
+    if (W % 8 == 0 && aligned16(X) && aligned16(col))
+        im2col3_vec8_kernel<<<dim3((unsigned)((n_pix / 8 + 255) / 256), (unsigned)C), 256, 0, S(stream)>>>(
+            X, H, W, (int)n_pix, static_cast<bf16 *>(col));
+    else
+        im2col3_kernel<<<dim3((unsigned)((n_pix + 255) / 256), (unsigned)(C * 9)), 256, 0, S(stream)>>>(
+            X, C, B, H, W, static_cast<bf16 *>(col));
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }
@@ -1092,7 +1297,34 @@ int amhd_nn_col2im3(const float *dcol, int32_t C, int32_t B, int32_t H, int32_t 
     if (!dcol || !dX || C <= 0 || B <= 0 || H <= 0 || W <= 0) return nn_fail(AMHD_ERR_ARG, "bad col2im arguments");
     const int64_t n_pix = (int64_t)B * H * W;
     if (n_pix > INT32_MAX || C > 65535) return nn_fail(AMHD_ERR_ARG, "col2im size beyond the grid");
-    col2im3_kernel<<<dim3((unsigned)((n_pix + 255) / 256), (unsigned)C), 256, 0, S(stream)>>>(dcol, C, B, H, W, dX);
+    if (W % 4 == 0 && aligned16(dcol) && aligned16(dX))
+        col2im3_vec4_kernel<<<dim3((unsigned)((n_pix / 4 + 255) / 256), (unsigned)C), 256, 0, S(stream)>>>(
+            dcol, H, W, (int)n_pix, dX);
+    else
+        col2im3_kernel<<<dim3((unsigned)((n_pix + 255) / 256), (unsigned)C), 256, 0, S(stream)>>>(dcol, C, B, H, W,
+                                                                                                    dX);
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_flip3(const void *w, int32_t cout, int32_t cin, int32_t ldo, void *wt, void *stream)
+{
+    if (!w || !wt || cout <= 0 || cin <= 0 || ldo < cout * 9 || (int64_t)cin * ldo > INT32_MAX)
+        return nn_fail(AMHD_ERR_ARG, "bad flip3 arguments");
+    const int n = cin * ldo;
+    flip3_kernel<<<(n + 255) / 256, 256, 0, S(stream)>>>(static_cast<const bf16 *>(w), cout, cin, ldo,
+                                                         static_cast<bf16 *>(wt));
+    NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_pad_cols(const void *w, int32_t rows, int32_t cols, int32_t ldo, void *out, void *stream)
+{
+    if (!w || !out || rows <= 0 || cols <= 0 || ldo < cols || (int64_t)rows * ldo > INT32_MAX)
+        return nn_fail(AMHD_ERR_ARG, "bad pad_cols arguments");
+    const int n = rows * ldo;
+    pad_cols_kernel<<<(n + 255) / 256, 256, 0, S(stream)>>>(static_cast<const bf16 *>(w), rows, cols, ldo,
+                                                            static_cast<bf16 *>(out));
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }
@@ -1100,7 +1332,11 @@ int amhd_nn_col2im3(const float *dcol, int32_t C, int32_t B, int32_t H, int32_t 
 int amhd_nn_cast_bf16(const float *x, void *y, int64_t n, void *stream)
 {
     if (n < 0 || (n && (!x || !y))) return nn_fail(AMHD_ERR_ARG, "bad cast arguments");
-    if (n) cast_bf16_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(x, static_cast<bf16 *>(y), n);
+    if (n && n % 4 == 0 && aligned16(x) && aligned16(y))
+        cast_bf16_vec4_kernel<<<blocks_for(n / 4), 256, 0, S(stream)>>>(reinterpret_cast<const float4 *>(x),
+                                                                        static_cast<uint2 *>(y), n / 4);
+    else if (n)
+        cast_bf16_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(x, static_cast<bf16 *>(y), n);
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }
@@ -1108,7 +1344,14 @@ int amhd_nn_cast_bf16(const float *x, void *y, int64_t n, void *stream)
 int amhd_nn_bias_act(float *Y, const float *bias, int32_t C, int64_t N, int32_t relu, void *stream)
 {
     if (!Y || !bias || C <= 0 || N < 0) return nn_fail(AMHD_ERR_ARG, "bad bias arguments");
-    bias_act_kernel<<<blocks_for((int64_t)C * N), 256, 0, S(stream)>>>(Y, bias, C, N, relu);
+    if (N % 4 == 0 && C <= 65535 && aligned16(Y)) {
+        int64_t bx = (N / 4 + 255) / 256;
+        if (bx > 64) bx = 64;
+        if (N) bias_act_vec4_kernel<<<dim3((unsigned)bx, (unsigned)C), 256, 0, S(stream)>>>(
+            reinterpret_cast<float4 *>(Y), bias, N / 4, relu);
+    } else {
+        bias_act_kernel<<<blocks_for((int64_t)C * N), 256, 0, S(stream)>>>(Y, bias, C, N, relu);
+    }
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }
@@ -1116,7 +1359,12 @@ int amhd_nn_bias_act(float *Y, const float *bias, int32_t C, int64_t N, int32_t 
 int amhd_nn_relu_bwd(float *dY, const float *Y, int64_t n, void *stream)
 {
     if (!dY || !Y || n < 0) return nn_fail(AMHD_ERR_ARG, "bad relu arguments");
-    relu_bwd_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(dY, Y, n);
+    if (n % 4 == 0 && aligned16(dY) && aligned16(Y)) {
+        if (n) relu_bwd_vec4_kernel<<<blocks_for(n / 4), 256, 0, S(stream)>>>(reinterpret_cast<float4 *>(dY),
+                                                                               reinterpret_cast<const float4 *>(Y), n / 4);
+    } else {
+        relu_bwd_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(dY, Y, n);
+    }
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }
@@ -1132,8 +1380,14 @@ int amhd_nn_bias_grad(const float *dY, int32_t C, int64_t N, float *db, void *st
 int amhd_nn_pool2(const float *X, int32_t CB, int32_t H, int32_t W, float *Y, int32_t backward, void *stream)
 {
     if (!X || !Y || CB <= 0 || H < 2 || W < 2 || (H & 1) || (W & 1)) return nn_fail(AMHD_ERR_ARG, "bad pool arguments");
-    if (backward)
+    const bool vec = W % 4 == 0 && CB <= 65535 && aligned16(X) && aligned16(Y);
+    if (backward && vec)
+        pool2_bwd_vec_kernel<<<dim3((unsigned)((H * W / 4 + 255) / 256), (unsigned)CB), 256, 0, S(stream)>>>(X, H, W,
+                                                                                                           Y);
+    else if (backward)
         pool2_bwd_kernel<<<blocks_for((int64_t)CB * H * W), 256, 0, S(stream)>>>(X, CB, H, W, Y);
+    else if (vec)
+        pool2_vec_kernel<<<dim3((unsigned)((H * W / 8 + 255) / 256), (unsigned)CB), 256, 0, S(stream)>>>(X, H, W, Y);
     else
         pool2_kernel<<<blocks_for((int64_t)CB * H * W / 4), 256, 0, S(stream)>>>(X, CB, H, W, Y);
     NNCK(cudaGetLastError());
@@ -1143,8 +1397,13 @@ int amhd_nn_pool2(const float *X, int32_t CB, int32_t H, int32_t W, float *Y, in
 int amhd_nn_up2(const float *X, int32_t CB, int32_t h, int32_t w, float *Y, int32_t backward, void *stream)
 {
     if (!X || !Y || CB <= 0 || h <= 0 || w <= 0) return nn_fail(AMHD_ERR_ARG, "bad upsample arguments");
-    if (backward)
+    const bool vec = w % 2 == 0 && CB <= 65535 && aligned16(X) && aligned16(Y);
+    if (backward && vec)
+        up2_bwd_vec_kernel<<<dim3((unsigned)((h * w / 2 + 255) / 256), (unsigned)CB), 256, 0, S(stream)>>>(X, h, w, Y);
+    else if (backward)
         up2_bwd_kernel<<<blocks_for((int64_t)CB * h * w), 256, 0, S(stream)>>>(X, CB, h, w, Y);
+    else if (vec)
+        up2_vec_kernel<<<dim3((unsigned)((4 * h * w / 4 + 255) / 256), (unsigned)CB), 256, 0, S(stream)>>>(X, h, w, Y);
     else
         up2_kernel<<<blocks_for((int64_t)CB * 4 * h * w), 256, 0, S(stream)>>>(X, CB, h, w, Y);
     NNCK(cudaGetLastError());
@@ -1154,7 +1413,11 @@ int amhd_nn_up2(const float *X, int32_t CB, int32_t h, int32_t w, float *Y, int3
 int amhd_nn_axpy(float *y, const float *x, float a, int64_t n, void *stream)
 {
     if (!y || !x || n < 0) return nn_fail(AMHD_ERR_ARG, "bad axpy arguments");
-    if (n) axpy_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(y, x, a, n);
+    if (n && n % 4 == 0 && aligned16(y) && aligned16(x))
+        axpy_vec4_kernel<<<blocks_for(n / 4), 256, 0, S(stream)>>>(reinterpret_cast<float4 *>(y),
+                                                                   reinterpret_cast<const float4 *>(x), a, n / 4);
+    else if (n)
+        axpy_kernel<<<blocks_for(n), 256, 0, S(stream)>>>(y, x, a, n);
     NNCK(cudaGetLastError());
     return AMHD_OK;
 }

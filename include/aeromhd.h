@@ -396,6 +396,13 @@ int amhd_nn_gemm(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_t K
 int amhd_nn_im2col3(const float *X, int32_t C, int32_t B, int32_t H, int32_t W, void *col, void *stream);
 /* adjoint of im2col3: dX[c][b][h][w] = sum over taps of dcol (gather, fixed order) */
 int amhd_nn_col2im3(const float *dcol, int32_t C, int32_t B, int32_t H, int32_t W, float *dX, void *stream);
+/* the 3x3 weights w[co][ci*9+tap] (BF16) for the input gradient:
+ * wt[ci][co*9+t] = w[co][ci*9+8-t], columns cout*9 .. ldo-1 zero; then
+ * dX = wt x im2col3(dY) (the adjoint of a zero-padded 3x3 convolution) */
+int amhd_nn_flip3(const void *w, int32_t cout, int32_t cin, int32_t ldo, void *wt, void *stream);
+/* rows x cols BF16 values into rows x ldo, columns cols .. ldo-1 zero (a GEMM
+ * operand whose row pitch is a multiple of 8 values, as the TMA path needs) */
+int amhd_nn_pad_cols(const void *w, int32_t rows, int32_t cols, int32_t ldo, void *out, void *stream);
 int amhd_nn_cast_bf16(const float *x, void *y, int64_t n, void *stream);
 /* Y[c][n] = act(Y[c][n] + bias[c]), act = ReLU if relu else identity */
 int amhd_nn_bias_act(float *Y, const float *bias, int32_t C, int64_t N, int32_t relu, void *stream);

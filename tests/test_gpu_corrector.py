@@ -17,10 +17,11 @@ def bf(t):
 @pytest.mark.parametrize("path", [1, 0])
 @pytest.mark.parametrize("transA,transB", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("M,N,K,splits", [(37, 91, 53, 1), (128, 300, 700, 4), (10, 4096, 288, 1), (64, 64, 5000, 7),
-                                          (256, 320, 704, 4)])
+                                          (256, 320, 704, 4), (32, 2048, 96, 1), (10, 640, 96, 1)])
 def test_gemm_matches_float_matmul(transA, transB, M, N, K, splits, path):
     """amhd_nn_gemm on mma.sync (path 1) and with the per-shape choice of
-    kernel (path 0: tcgen05 for the large shapes whose operands qualify)."""
+    kernel (path 0: tcgen05 wherever N >= 64 or K >= 4096 and the operands
+    qualify, M below a tile included)."""
     from aeromhd_cuda_b200 import _lib
     from aeromhd_cuda_b200._tensors import stream_ptr
     g = torch.Generator(device="cuda").manual_seed(M * N + K)
@@ -227,7 +228,7 @@ def test_graphed_training_step_matches_eager():
     assert float((wa - wb).abs().max()) <= 1e-4 * float(wa.abs().max())
 
 
-@pytest.mark.parametrize("C,B,H,W", [(3, 2, 5, 7), (10, 4, 32, 16), (16, 1, 8, 8)])
+@pytest.mark.parametrize("C,B,H,W", [(3, 2, 5, 7), (10, 4, 32, 16), (16, 1, 8, 8), (8, 2, 16, 64), (5, 3, 6, 12)])
 def test_im2col_col2im_bias_grad_against_torch(C, B, H, W):
     """The convolution helpers against torch: im2col3 (3x3, zero padding) as
     unfold, col2im3 as its adjoint (fold), bias_grad as a row sum (N both a
@@ -253,6 +254,85 @@ def test_im2col_col2im_bias_grad_against_torch(C, B, H, W):
         db = torch.empty(C, device="cuda")
         _lib.call("amhd_nn_bias_grad", dY.data_ptr(), C, n, db.data_ptr(), stream_ptr())
         assert torch.allclose(db, dY.double().sum(1).float(), atol=1e-3, rtol=1e-5)
+
+
+def _shifted(t):
+    """A copy of t that starts 4 bytes past a 16-byte boundary (the library's scalar kernels)."""
+    buf = torch.empty(t.numel() + 4, dtype=t.dtype, device=t.device)
+    v = buf[1:1 + t.numel()].view(t.shape)
+    v.copy_(t)
+    return v
+
+
+@pytest.mark.parametrize("CB,H,W", [(6, 8, 16), (12, 32, 64), (3, 6, 10)])
+def test_elementwise_helpers_vector_and_scalar_paths(CB, H, W):
+    """Pooling, upsampling (and their gradients), bias + ReLU, the ReLU
+    gradient, axpy and the bfloat16 cast: the several-values-per-thread
+    kernels (16-byte aligned operands, rows a multiple of 4) give the same bits
+    as the one-value-per-thread kernels (operands 4 bytes off), and both match
+    torch."""
+    import ctypes
+    import torch.nn.functional as Fn
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import stream_ptr
+    g = torch.Generator(device="cuda").manual_seed(CB * 7 + W)
+    X = torch.randn((CB, H, W), device="cuda", generator=g)
+    h, w = H // 2, W // 2
+
+    def both(fn, out_shape, *ins):
+        res = []
+        for shift in (False, True):
+            args = [_shifted(t) if shift else t.clone() for t in ins]
+            out = torch.zeros(out_shape, device="cuda")
+            out = _shifted(out) if shift else out
+            fn(out, *args)
+            res.append(out.clone())
+        assert torch.equal(res[0], res[1])
+        return res[0]
+
+    pooled = both(lambda o, x: _lib.call("amhd_nn_pool2", x.data_ptr(), CB, H, W, o.data_ptr(), 0, stream_ptr()),
+                  (CB, h, w), X)
+    assert torch.allclose(pooled, Fn.avg_pool2d(X.unsqueeze(1), 2).squeeze(1), atol=1e-6)
+    dP = torch.randn((CB, h, w), device="cuda", generator=g)
+    dXp = both(lambda o, d: _lib.call("amhd_nn_pool2", d.data_ptr(), CB, H, W, o.data_ptr(), 1, stream_ptr()),
+               (CB, H, W), dP)
+    assert torch.equal(dXp, 0.25 * dP.repeat_interleave(2, 1).repeat_interleave(2, 2))
+    Xs = torch.randn((CB, h, w), device="cuda", generator=g)
+    up = both(lambda o, x: _lib.call("amhd_nn_up2", x.data_ptr(), CB, h, w, o.data_ptr(), 0, stream_ptr()),
+              (CB, H, W), Xs)
+    assert torch.equal(up, Xs.repeat_interleave(2, 1).repeat_interleave(2, 2))
+    dU = torch.randn((CB, H, W), device="cuda", generator=g)
+    dXs = both(lambda o, d: _lib.call("amhd_nn_up2", d.data_ptr(), CB, h, w, o.data_ptr(), 1, stream_ptr()),
+               (CB, h, w), dU)
+    assert torch.allclose(dXs, 4.0 * Fn.avg_pool2d(dU.unsqueeze(1), 2).squeeze(1), atol=1e-5)
+    # bias + ReLU over [C][N], N = H * W per channel
+    C, N = CB, H * W
+    bias = torch.randn(C, device="cuda", generator=g)
+    for relu in (0, 1):
+        def ba(o, y):
+            o.copy_(y)
+            _lib.call("amhd_nn_bias_act", o.data_ptr(), bias.data_ptr(), C, N, relu, stream_ptr())
+        Y = both(ba, (C, N), X.view(C, N))
+        ref = X.view(C, N) + bias[:, None]
+        assert torch.equal(Y, ref.clamp_min(0.0) if relu else ref)
+
+    def rb(o, d, y):
+        o.copy_(d)
+        _lib.call("amhd_nn_relu_bwd", o.data_ptr(), y.data_ptr(), C * N, stream_ptr())
+    Yr = torch.randn((C, N), device="cuda", generator=g)
+    dY = torch.randn((C, N), device="cuda", generator=g)
+    assert torch.equal(both(rb, (C, N), dY, Yr), torch.where(Yr > 0, dY, torch.zeros_like(dY)))
+
+    def ax(o, y, x):
+        o.copy_(y)
+        _lib.call("amhd_nn_axpy", o.data_ptr(), x.data_ptr(), ctypes.c_float(0.37), C * N, stream_ptr())
+    assert torch.allclose(both(ax, (C, N), dY, Yr), dY + 0.37 * Yr, atol=1e-6)
+    for shift in (False, True):
+        src = _shifted(X) if shift else X
+        out = torch.empty(X.numel() + 8, dtype=torch.bfloat16, device="cuda")
+        dst = out[4 if shift else 0:][:X.numel()]
+        _lib.call("amhd_nn_cast_bf16", src.data_ptr(), dst.data_ptr(), X.numel(), stream_ptr())
+        assert torch.equal(dst.view(X.shape), X.to(torch.bfloat16))
 
 
 def test_restrict_pack_apply():
