@@ -121,6 +121,7 @@ _SIGS = {
     "amhd_nn_gemm_status": ([_P], _c.c_int),
     "amhd_nn_gemm_tc_paths": ([_P, _P], _c.c_int),
     "amhd_nn_set_gemm_path": ([_I32], _c.c_int),
+    "amhd_nn_set_gemm_persistent": ([_I32], _c.c_int),
     "amhd_nn_im2col3": ([_P, _I32, _I32, _I32, _I32, _P, _P], _c.c_int),
     "amhd_nn_col2im3": ([_P, _I32, _I32, _I32, _I32, _P, _P], _c.c_int),
     "amhd_nn_cast_bf16": ([_P, _P, _I64, _P], _c.c_int),

@@ -436,7 +436,8 @@ constexpr uint64_t kSwizzle128 = 2ull << 61;  // descriptor layout type SWIZZLE_
 __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ CUtensorMap mapA,
                                                        const __grid_constant__ CUtensorMap mapB, int a_kmajor,
                                                        int b_kmajor, int M, int N, int K, float *C, int ldc,
-                                                       float alpha, float beta, int k_per_split, int *err_flag)
+                                                       float alpha, float beta, int k_per_split, int a_tx,
+                                                       int a_two, int *err_flag)
 {
     extern __shared__ unsigned char tma_raw[];
     TmaSmem &sm = *reinterpret_cast<TmaSmem *>((reinterpret_cast<uintptr_t>(tma_raw) + 1023) & ~uintptr_t(1023));
@@ -477,14 +478,14 @@ __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ C
                 break;
             }
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem_addr(&sm.full[s])),
-                         "r"(kTmaABytes + kTmaBBytes)
+                         "r"(a_tx + kTmaBBytes)
                          : "memory");
             const int k0 = kbeg + kt * TK;
             if (a_kmajor) {
                 tma_load(sm.a[s], &mapA, k0, m0, &sm.full[s]);
             } else {
                 tma_load(sm.a[s], &mapA, m0, k0, &sm.full[s]);
-                tma_load(sm.a[s] + kTmaABytes / 2, &mapA, m0 + TM / 2, k0, &sm.full[s]);
+                if (a_two) tma_load(sm.a[s] + kTmaABytes / 2, &mapA, m0 + TM / 2, k0, &sm.full[s]);
             }
             if (b_kmajor)
                 tma_load(sm.b[s], &mapB, k0, n0, &sm.full[s]);
@@ -578,6 +579,229 @@ __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ C
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN2) : "memory");
+    }
+    if (tid == 0 && sm.err) atomicOr(err_flag, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent form of the same GEMM (no split-K): one CTA per SM walks the
+// output tiles t = blockIdx.x, blockIdx.x + gridDim.x, ... (128 x 64 each, M
+// fastest), with the roles split over its six warps so that a tile's epilogue
+// overlaps the next tile's loads and MMAs:
+//   warp 0 (one thread) -- TMA producer: every K step of every tile through a
+//     ring of kPStages shared-memory stages (full / empty mbarriers);
+//   warp 1 (one thread) -- MMA issuer: tcgen05.mma into one of two TMEM
+//     accumulators (64 columns each), committed to the stage's empty barrier
+//     and, after a tile's last K step, to the accumulator's full barrier;
+//   warps 2..5 -- epilogue: tcgen05.ld of their 32 TMEM lanes (warp w reads
+//     lanes 32 (w % 4) ..), alpha / beta, stores; then they release the
+//     accumulator (its empty barrier, one arrival per warp).
+// Shared memory, descriptors, boxes and the instruction descriptor are those
+// of gemm_tma_kernel.  Every wait is bounded: a role that gives up marks the
+// CTA and stops, the others then give up at their next wait; before the TMEM
+// columns are freed the producer waits (bounded) for its loads in flight and
+// every thread for the MMAs issued.
+// ---------------------------------------------------------------------------
+constexpr int kPStages = 8;  // 8 x 24 KB: one CTA per SM
+constexpr int kPThreads = 192;
+
+struct PersistSmem {
+    alignas(1024) unsigned char a[kPStages][kTmaABytes];
+    alignas(1024) unsigned char b[kPStages][kTmaBBytes];
+    uint64_t full[kPStages], empty[kPStages], acc_full[2], acc_empty[2], done;
+    uint32_t tmem;
+    int err;
+};
+constexpr int kPersistSmemBytes = (int)sizeof(PersistSmem) + 1024;
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_addr(bar)), "r"(count) : "memory");
+}
+
+__global__ void __launch_bounds__(kPThreads, 1) gemm_tma_persistent_kernel(
+    const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int a_kmajor, int b_kmajor,
+    int M, int N, int K, float *C, int ldc, float alpha, float beta, int a_tx, int a_two, int *err_flag)
+{
+    extern __shared__ unsigned char tma_raw[];
+    PersistSmem &sm =
+        *reinterpret_cast<PersistSmem *>((reinterpret_cast<uintptr_t>(tma_raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int tiles_m = (M + TM - 1) / TM, tiles = tiles_m * ((N + TN2 - 1) / TN2);
+    const int nk = (K + TK - 1) / TK;
+    const int my_tiles = blockIdx.x < tiles ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem_addr(&sm.tmem)),
+                     "r"(2 * TN2)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        sm.err = 0;
+        for (int s = 0; s < kPStages; ++s) {
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&sm.acc_full[a], 1);
+            mbar_init(&sm.acc_empty[a], 4);  // one arrival per epilogue warp
+        }
+        mbar_init(&sm.done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = sm.tmem;
+
+    if (tid == 0) {
+        // producer: load g (g-th K step of this CTA) goes to stage g % kPStages once the
+        // MMAs of load g - kPStages have released it
+        int g = 0;
+        bool ok = true;
+        for (int i = 0; i < my_tiles && ok; ++i) {
+            const int t = blockIdx.x + i * gridDim.x;
+            const int m0 = (t % tiles_m) * TM, n0 = (t / tiles_m) * TN2;
+            for (int kt = 0; kt < nk; ++kt, ++g) {
+                const int s = g % kPStages;
+                if (g >= kPStages && !tc_wait(&sm.empty[s], (uint32_t)((g / kPStages) - 1) & 1u)) {
+                    sm.err = 1;
+                    ok = false;
+                    break;
+                }
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem_addr(&sm.full[s])),
+                             "r"(a_tx + kTmaBBytes)
+                             : "memory");
+                const int k0 = kt * TK;
+                if (a_kmajor) {
+                    tma_load(sm.a[s], &mapA, k0, m0, &sm.full[s]);
+                } else {
+                    tma_load(sm.a[s], &mapA, m0, k0, &sm.full[s]);
+                    if (a_two) tma_load(sm.a[s] + kTmaABytes / 2, &mapA, m0 + TM / 2, k0, &sm.full[s]);
+                }
+                if (b_kmajor)
+                    tma_load(sm.b[s], &mapB, k0, n0, &sm.full[s]);
+                else
+                    tma_load(sm.b[s], &mapB, n0, k0, &sm.full[s]);
+            }
+        }
+        // the loads still in flight land before the CTA can leave: the last one of each stage
+        for (int s = 0; s < kPStages && s < g; ++s) {
+            const int uses = (g - 1 - s) / kPStages + 1;
+            if (!tc_wait(&sm.full[s], (uint32_t)(uses - 1) & 1u)) sm.err = 1;
+        }
+    } else if (tid == 32) {
+        // MMA issuer
+        int g = 0;
+        bool ok = true;
+        const uint32_t idesc = kTmaIdesc | (a_kmajor ? 0u : 1u << 15) | (b_kmajor ? 0u : 1u << 16);
+        for (int i = 0; i < my_tiles && ok; ++i) {
+            const int acc = i & 1;
+            if (i >= 2 && !tc_wait(&sm.acc_empty[acc], (uint32_t)((i >> 1) - 1) & 1u)) {
+                sm.err = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t d = tmem + (uint32_t)(acc * TN2);
+            for (int kt = 0; kt < nk; ++kt, ++g) {
+                const int s = g % kPStages;
+                if (!tc_wait(&sm.full[s], (uint32_t)(g / kPStages) & 1u)) {
+                    sm.err = 1;
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < TK / 16; ++j) {
+                    const uint64_t da = kSwizzle128 | (a_kmajor ? tc_desc(sm.a[s] + j * 32, 16u, 1024u)
+                                                                : tc_desc(sm.a[s] + j * 2048, kTmaABytes / 2, 1024u));
+                    const uint64_t db = kSwizzle128 | (b_kmajor ? tc_desc(sm.b[s] + j * 32, 16u, 1024u)
+                                                                : tc_desc(sm.b[s] + j * 2048, kTmaABytes / 2, 1024u));
+                    const uint32_t accum = (kt == 0 && j == 0) ? 0u : 1u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+                        "l"(da), "l"(db), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+                        : "memory");
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 tc_smem_addr(&sm.empty[s]))
+                             : "memory");
+            }
+            if (ok)
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 tc_smem_addr(&sm.acc_full[acc]))
+                             : "memory");
+        }
+        // arrives once every MMA issued above has completed
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         tc_smem_addr(&sm.done))
+                     : "memory");
+    } else if (warp >= 2) {
+        // epilogue: warp w owns TMEM lanes 32 (w % 4) .. + 31, i.e. tile rows of that quarter
+        const int quarter = warp & 3;
+        const bool vec = beta == 0.f && (ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+        for (int i = 0; i < my_tiles; ++i) {
+            const int acc = i & 1;
+            // one decision for the warp: the TMEM loads below are warp-collective
+            if (!__all_sync(0xffffffffu, tc_wait(&sm.acc_full[acc], (uint32_t)(i >> 1) & 1u))) {
+                sm.err = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int t = blockIdx.x + i * gridDim.x;
+            const int m0 = (t % tiles_m) * TM, n0 = (t / tiles_m) * TN2;
+            const int row = m0 + quarter * 32 + lane;
+#pragma unroll 1
+            for (int c0 = 0; c0 < TN2; c0 += 16) {
+                uint32_t r[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                      "=r"(r[15])
+                    : "r"(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * TN2 + c0)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (row < M) {
+                    float *crow = C + (int64_t)row * ldc;
+                    if (vec && n0 + c0 + 16 <= N) {
+#pragma unroll
+                        for (int q = 0; q < 16; q += 4)
+                            *reinterpret_cast<float4 *>(crow + n0 + c0 + q) =
+                                make_float4(alpha * __uint_as_float(r[q]), alpha * __uint_as_float(r[q + 1]),
+                                            alpha * __uint_as_float(r[q + 2]), alpha * __uint_as_float(r[q + 3]));
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) {
+                            const int col = n0 + c0 + q;
+                            if (col < N) {
+                                float *p = crow + col;
+                                const float v = alpha * __uint_as_float(r[q]);
+                                *p = (beta != 0.f) ? v + beta * (*p) : v;
+                            }
+                        }
+                    }
+                }
+            }
+            // this warp is done reading the accumulator: the MMAs of tile i + 2 may overwrite it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc_smem_addr(&sm.acc_empty[acc]))
+                             : "memory");
+        }
+    }
+    // the role threads wait for the last MMAs; the idle lanes of warps 0 and 1 go
+    // straight to the barrier (no polling beside the producer and the issuer)
+    if ((tid == 0 || tid == 32 || warp >= 2) && !tc_wait(&sm.done, 0u)) sm.err = 1;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TN2) : "memory");
     }
     if (tid == 0 && sm.err) atomicOr(err_flag, 1);
 }
@@ -1126,6 +1350,16 @@ bool operand_map(CUtensorMap *map, const void *base, int ld, int rows, int K, in
 
 std::atomic<long long> g_tc_tma_launches{0}, g_tc_staged_launches{0};
 std::atomic<int> g_gemm_path{0};  // amhd_nn_set_gemm_path
+std::atomic<int> g_persistent{1};  // amhd_nn_set_gemm_persistent
+
+// multiprocessors of the current device (the persistent GEMM's grid)
+int nn_sm_count()
+{
+    int dev = 0, n = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+        return kNumSMs;
+    return n;
+}
 
 // split-K: K per split rounded up to whole K steps of `step`; returns the split count
 int split_k(int K, int splits, int step, int *kps_out)
@@ -1145,8 +1379,16 @@ int tma_gemm(int transA, int transB, int M, int N, int K, const void *A, int lda
 {
     *launched = false;
     const bool a_kmajor = !transA, b_kmajor = transB != 0;
+    // A boxes no taller than M needs (rounded to whole 8-row swizzle atoms; a
+    // K-major box of R rows delivers R x 128 bytes, an MN-major A of M <= 64 rows
+    // takes one of its two 64-row boxes): the rows past the box are whatever the
+    // stage held before and only reach accumulator rows that are never stored
+    const int a_rows = a_kmajor ? std::min(TM, (M + 7) / 8 * 8) : TM;
+    const int a_two = a_kmajor ? 0 : (M > TM / 2 ? 1 : 0);
+    const int a_tx = a_kmajor ? a_rows * TK * 2 : (a_two ? kTmaABytes : kTmaABytes / 2);
     CUtensorMap map_a, map_b;
-    if (K <= 0 || !operand_map(&map_a, A, lda, M, K, TM, a_kmajor) || !operand_map(&map_b, B, ldb, N, K, TN2, b_kmajor))
+    if (K <= 0 || !operand_map(&map_a, A, lda, M, K, a_rows, a_kmajor) ||
+        !operand_map(&map_b, B, ldb, N, K, TN2, b_kmajor))
         return AMHD_OK;
     // function attributes are per device: set on every call (cheap), so that any
     // device current in this thread has the opt-in before the launch
@@ -1162,13 +1404,26 @@ int tma_gemm(int transA, int transB, int M, int N, int K, const void *A, int lda
     }
     int kps;
     splits = split_k(K, splits, TK, &kps);
+    if (splits == 1 && g_persistent.load()) {
+        // one CTA per SM walks the tiles, each tile's epilogue under the next one's loads
+        NNCK(cudaFuncSetAttribute(gemm_tma_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kPersistSmemBytes));
+        const int grid = std::min(tiles, nn_sm_count());
+        gemm_tma_persistent_kernel<<<grid, kPThreads, kPersistSmemBytes, s>>>(map_a, map_b, a_kmajor, b_kmajor, M,
+                                                                               N, K, C, ldc, alpha, beta, a_tx, a_two,
+                                                                               err);
+        NNCK(cudaGetLastError());
+        ++g_tc_tma_launches;
+        *launched = true;
+        return AMHD_OK;
+    }
     if (splits > 1) {
         scale_kernel<<<blocks_for((int64_t)M * N), 256, 0, s>>>(C, M, N, ldc, beta);
         NNCK(cudaGetLastError());
     }
     dim3 grid((N + TN2 - 1) / TN2, (M + TM - 1) / TM, splits);
     gemm_tma_kernel<<<grid, 128, kTmaSmemBytes, s>>>(map_a, map_b, a_kmajor, b_kmajor, M, N, K, C, ldc, alpha,
-                                                     splits > 1 ? 0.f : beta, kps, err);
+                                                     splits > 1 ? 0.f : beta, kps, a_tx, a_two, err);
     NNCK(cudaGetLastError());
     ++g_tc_tma_launches;
     *launched = true;
@@ -1220,6 +1475,13 @@ int amhd_nn_gemm_tc(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_
                                                    static_cast<const bf16 *>(B), ldb, C, ldc, alpha,
                                                    splits > 1 ? 0.f : beta, kps, err);
     NNCK(cudaGetLastError());
+    return AMHD_OK;
+}
+
+int amhd_nn_set_gemm_persistent(int32_t on)
+{
+    if (on != 0 && on != 1) return nn_fail(AMHD_ERR_ARG, "persistent GEMM switch must be 0 or 1, got %d", on);
+    g_persistent.store(on);
     return AMHD_OK;
 }
 

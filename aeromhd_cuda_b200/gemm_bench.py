@@ -10,9 +10,14 @@ Adam step of that network (forward, backward, update) on mma.sync only and
 with the default choice.
 
     python -m aeromhd_cuda_b200.gemm_bench [--shapes tA,tB,M,N,K ...] [--iters 20] [--warmup 3] [--train-step]
+                                           [--graph]
 
 Prints one JSON object: per shape and path the mean time of a launch (CUDA
-events around `iters` back-to-back launches) and its TFLOP/s.
+events around `iters` back-to-back launches) and its TFLOP/s.  Each launch is
+a call from Python through the C ABI (tensor maps encoded on the host per
+call), so small shapes can be bound by the host; --graph captures the `iters`
+launches into one CUDA graph and times its replay instead (the kernels alone,
+as the captured training step runs them).
 """
 from __future__ import annotations
 
@@ -25,11 +30,24 @@ CORRECTOR_SHAPES = [(0, 0, 32, 262144, 90), (0, 0, 64, 65536, 288), (0, 0, 128, 
 PATHS = {"mma.sync": ("amhd_nn_gemm", 1), "tcgen05": ("amhd_nn_gemm_tc", 0), "auto": ("amhd_nn_gemm", 0)}
 
 
-def _events_ms(fn, iters: int, warmup: int) -> float:
+def _events_ms(fn, iters: int, warmup: int, graph: bool = False) -> float:
     import torch
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
+    if graph:
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for _ in range(iters):
+                fn()
+        g.replay()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        g.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / iters
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(iters):
@@ -47,7 +65,8 @@ def _check_waits() -> None:
         raise RuntimeError("amhd_nn_gemm_tc: a tensor-core wait timed out")
 
 
-def time_shape(tA: int, tB: int, M: int, N: int, K: int, iters: int, warmup: int, paths=tuple(PATHS)) -> dict:
+def time_shape(tA: int, tB: int, M: int, N: int, K: int, iters: int, warmup: int, paths=tuple(PATHS),
+               graph: bool = False) -> dict:
     import torch
     from . import _lib
     from ._tensors import stream_ptr
@@ -65,7 +84,7 @@ def time_shape(tA: int, tB: int, M: int, N: int, K: int, iters: int, warmup: int
             def launch():
                 _lib.call(fn_name, tA, tB, M, N, K, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1],
                           C.data_ptr(), N, 1.0, 0.0, splits, stream_ptr())
-            ms = _events_ms(launch, iters, warmup)
+            ms = _events_ms(launch, iters, warmup, graph)
             out[name] = {"ms": round(ms, 4), "TFLOP/s": round(2.0 * M * N * K / ms / 1e9, 2)}
     finally:
         _lib.call("amhd_nn_set_gemm_path", 0)
@@ -103,11 +122,12 @@ def main(argv=None) -> None:
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--train-step", action="store_true")
+    ap.add_argument("--graph", action="store_true", help="time the launches replayed as one CUDA graph")
     args = ap.parse_args(argv)
     shapes = CORRECTOR_SHAPES if not args.shapes else [tuple(int(x) for x in s.split(",")) for s in args.shapes]
     res = {}
     for (tA, tB, M, N, K) in shapes:
-        res[f"{tA}{tB} {M}x{N}x{K}"] = time_shape(tA, tB, M, N, K, args.iters, args.warmup)
+        res[f"{tA}{tB} {M}x{N}x{K}"] = time_shape(tA, tB, M, N, K, args.iters, args.warmup, graph=args.graph)
     if args.train_step:
         res["train_step 256x64 batch 16"] = time_train_step(args.iters, args.warmup)
     print(json.dumps(res))

@@ -364,9 +364,13 @@ const char *amhd_nn_last_error(void);
  * splits > 1 divides K over CTAs and accumulates atomically. */
 /* The same contract on the 5th-generation tensor cores (tcgen05.mma, FP32
  * accumulator in tensor memory).  Operands whose base is 16-byte aligned and
- * whose ld is a multiple of 8 are loaded by TMA (128-byte swizzle) into a
- * 4-stage pipeline (128 x 64 tiles), where splits > 1 may be raised to fill
- * the GPU; others are staged by the CTA's threads (128 x 128 tiles).
+ * whose ld is a multiple of 8 are loaded by TMA (128-byte swizzle), 128 x 64
+ * output tiles: without split-K by a persistent kernel (one CTA per SM, an
+ * 8-stage load ring, two TMEM accumulators so that a tile's epilogue overlaps
+ * the next tile's loads and MMAs; amhd_nn_set_gemm_persistent(0) takes the
+ * one-tile-per-CTA kernel instead), with splits > 1 (which may be raised to
+ * fill the GPU) one tile per CTA and a 3-stage ring; others are staged by the
+ * CTA's threads (128 x 128 tiles).
  * amhd_nn_gemm_status returns (and clears) 1 if a load or MMA completion wait
  * gave up since the last call, else 0; amhd_nn_gemm_tc_paths counts the
  * launches of either path since the library was loaded. */
@@ -376,10 +380,13 @@ int amhd_nn_gemm_tc(int32_t transA, int32_t transB, int32_t M, int32_t N, int32_
 int amhd_nn_gemm_status(int32_t *flag);
 int amhd_nn_gemm_tc_paths(int64_t *tma, int64_t *staged);
 /* Which kernel amhd_nn_gemm runs (process-wide): 0 (default) the tcgen05
- * TMA pipeline on the shapes where it is faster on B200 -- M >= 64 and
- * N >= 64, or K >= 4096 -- when the operands qualify, mma.sync otherwise;
- * 1 always mma.sync; 2 always amhd_nn_gemm_tc. */
+ * TMA pipeline on the shapes where it is faster on B200 -- N >= 64 or
+ * K >= 4096 -- when the operands qualify, mma.sync otherwise; 1 always
+ * mma.sync; 2 always amhd_nn_gemm_tc. */
 int amhd_nn_set_gemm_path(int32_t mode);
+/* 1 (default): unsplit TMA GEMMs run the persistent kernel; 0: one tile per CTA
+ * (process-wide; for measurement) */
+int amhd_nn_set_gemm_persistent(int32_t on);
 
 /* Self-test of the bounded device waits every kernel of this library uses on
  * an mbarrier (TMA staging, tensor-core completion; no counterpart in the

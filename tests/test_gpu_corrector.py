@@ -44,7 +44,8 @@ def test_gemm_matches_float_matmul(transA, transB, M, N, K, splits, path):
 
 @pytest.mark.parametrize("transA,transB", [(0, 0), (0, 1), (1, 0), (1, 1)])
 @pytest.mark.parametrize("M,N,K,splits", [(128, 128, 64, 1), (37, 91, 53, 1), (256, 300, 700, 4), (10, 4096, 288, 1),
-                                          (64, 64, 5000, 7), (256, 320, 704, 4), (200, 136, 96, 1)])
+                                          (64, 64, 5000, 7), (256, 320, 704, 4), (200, 136, 96, 1),
+                                          (256, 19200, 200, 1), (130, 12800, 72, 1)])
 def test_tcgen05_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
     """amhd_nn_gemm_tc (tcgen05.mma, FP32 accumulator in tensor memory) against a
     float64 matmul of the same BF16 operands, every transpose and split-K case,
@@ -69,6 +70,36 @@ def test_tcgen05_gemm_matches_float_matmul(transA, transB, M, N, K, splits):
     ref = 0.5 * (opA.double() @ opB.double()) + 2.0 * C0.double()
     err = float((C.double() - ref).abs().max() / ref.abs().max())
     assert err < 2e-6, err
+
+
+@pytest.mark.parametrize("transA,transB", [(0, 0), (1, 1), (0, 1)])
+@pytest.mark.parametrize("M,N,K", [(256, 19200, 200), (32, 262144, 96), (128, 16384, 576)])
+def test_persistent_gemm_equals_one_tile_per_cta(transA, transB, M, N, K):
+    """The persistent TMA GEMM (one CTA per SM, several tiles each, two TMEM
+    accumulators) and the one-tile-per-CTA kernel accumulate every tile in the
+    same K order: identical bits; no wait gave up."""
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200._tensors import stream_ptr
+    import ctypes
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = bf(torch.randn((K, M) if transA else (M, K), device="cuda", generator=g))
+    B = bf(torch.randn((N, K) if transB else (K, N), device="cuda", generator=g))
+    out = []
+    try:
+        for persistent in (1, 0):
+            _lib.call("amhd_nn_set_gemm_persistent", persistent)
+            C = torch.full((M, N), float("nan"), device="cuda")
+            _lib.call("amhd_nn_gemm_tc", transA, transB, M, N, K, A.data_ptr(), A.shape[1], B.data_ptr(), B.shape[1],
+                      C.data_ptr(), N, 1.0, 0.0, 1, stream_ptr())
+            out.append(C)
+    finally:
+        _lib.call("amhd_nn_set_gemm_persistent", 1)
+    torch.cuda.synchronize()
+    flag = ctypes.c_int32(-1)
+    _lib.call("amhd_nn_gemm_status", ctypes.byref(flag))
+    assert flag.value == 0
+    assert torch.isfinite(out[0]).all()
+    assert torch.equal(out[0], out[1])
 
 
 def test_tcgen05_gemm_operand_paths():
