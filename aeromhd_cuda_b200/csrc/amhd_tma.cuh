@@ -6,7 +6,7 @@
 // bounded: if the transfer has not completed within kTmaWaitNs (read from
 // %globaltimer; kTmaWaitIters polls as a backstop) the caller gets `false`
 // back, records AMHD_FLAG_TIMEOUT and the CTA leaves.
-// No multicast: every CTA loads its own box from this GPU's memory.
+// Every CTA loads its own box, from this GPU's memory only.
 #pragma once
 #include <cuda.h>
 #include <cuda_runtime.h>
