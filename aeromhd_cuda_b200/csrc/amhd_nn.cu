@@ -433,6 +433,106 @@ __device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, int 
 
 constexpr uint64_t kSwizzle128 = 2ull << 61;  // descriptor layout type SWIZZLE_128B
 
+// Pieces shared by the two TMA kernels below.
+//
+// the loads of K step k0 of the output tile (m0, n0) into one stage, counted on `bar`
+__device__ __forceinline__ void tma_stage_loads(unsigned char *a, unsigned char *b, const CUtensorMap *mapA,
+                                                const CUtensorMap *mapB, int a_kmajor, int b_kmajor, int a_tx,
+                                                int a_two, int m0, int n0, int k0, uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem_addr(bar)),
+                 "r"(a_tx + kTmaBBytes)
+                 : "memory");
+    if (a_kmajor) {
+        tma_load(a, mapA, k0, m0, bar);
+    } else {
+        tma_load(a, mapA, m0, k0, bar);
+        if (a_two) tma_load(a + kTmaABytes / 2, mapA, m0 + TM / 2, k0, bar);
+    }
+    if (b_kmajor)
+        tma_load(b, mapB, k0, n0, bar);
+    else
+        tma_load(b, mapB, n0, k0, bar);
+}
+
+// the four MMAs of one K step (K = 16 each) into the accumulator at TMEM address d;
+// first: the tile's first K step (overwrite instead of accumulate)
+__device__ __forceinline__ void mma_kstep(uint32_t d, const unsigned char *a, const unsigned char *b, int a_kmajor,
+                                          int b_kmajor, uint32_t idesc, bool first)
+{
+#pragma unroll
+    for (int j = 0; j < TK / 16; ++j) {
+        // K step j: 32 bytes into each swizzled row (K-major) or two 8-row atoms on (MN-major)
+        const uint64_t da = kSwizzle128 | (a_kmajor ? tc_desc(a + j * 32, 16u, 1024u)
+                                                    : tc_desc(a + j * 2048, kTmaABytes / 2, 1024u));
+        const uint64_t db = kSwizzle128 | (b_kmajor ? tc_desc(b + j * 32, 16u, 1024u)
+                                                    : tc_desc(b + j * 2048, kTmaABytes / 2, 1024u));
+        const uint32_t acc = (first && j == 0) ? 0u : 1u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d), "l"(da),
+            "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+            : "memory");
+    }
+}
+
+// arrives on `bar` once every tcgen05 operation this thread issued so far has completed
+__device__ __forceinline__ void mma_commit(uint64_t *bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     tc_smem_addr(bar))
+                 : "memory");
+}
+
+// epilogue of one warp: its 32 accumulator rows (TMEM lanes lane0 .. lane0 + 31,
+// columns col0 .. col0 + TN2 - 1) as C rows m0 + lane0 + lane, columns n0 ..;
+// alpha x acc (+ beta C), or atomically added under split-K
+__device__ __forceinline__ void store_tile_rows(uint32_t tmem, int lane0, int col0, int lane, int m0, int n0, int M,
+                                                int N, float *C, int ldc, float alpha, float beta, bool split)
+{
+    const int row = m0 + lane0 + lane;
+    const bool vec = !split && beta == 0.f && (ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+#pragma unroll 1
+    for (int c0 = 0; c0 < TN2; c0 += 16) {
+        uint32_t r[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+            "[%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(tmem + ((uint32_t)lane0 << 16) + (uint32_t)(col0 + c0)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < M) {
+            float *crow = C + (int64_t)row * ldc;
+            if (vec && n0 + c0 + 16 <= N) {
+#pragma unroll
+                for (int i = 0; i < 16; i += 4)
+                    *reinterpret_cast<float4 *>(crow + n0 + c0 + i) =
+                        make_float4(alpha * __uint_as_float(r[i]), alpha * __uint_as_float(r[i + 1]),
+                                    alpha * __uint_as_float(r[i + 2]), alpha * __uint_as_float(r[i + 3]));
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int col = n0 + c0 + i;
+                    if (col < N) {
+                        float *p = crow + col;
+                        const float v = alpha * __uint_as_float(r[i]);
+                        if (split)
+                            atomicAdd(p, v);
+                        else
+                            *p = (beta != 0.f) ? v + beta * (*p) : v;
+                    }
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_addr(bar)), "r"(count) : "memory");
+}
+
 __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ CUtensorMap mapA,
                                                        const __grid_constant__ CUtensorMap mapB, int a_kmajor,
                                                        int b_kmajor, int M, int N, int K, float *C, int ldc,
@@ -456,10 +556,10 @@ __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ C
     if (tid == 0) {
         sm.err = 0;
         for (int s = 0; s < kTmaStages; ++s) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.full[s])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.empty[s])) : "memory");
+            mbar_init(&sm.full[s], 1);
+            mbar_init(&sm.empty[s], 1);
         }
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem_addr(&sm.done)) : "memory");
+        mbar_init(&sm.done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -477,20 +577,8 @@ __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ C
                 sm.err = 1;
                 break;
             }
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem_addr(&sm.full[s])),
-                         "r"(a_tx + kTmaBBytes)
-                         : "memory");
-            const int k0 = kbeg + kt * TK;
-            if (a_kmajor) {
-                tma_load(sm.a[s], &mapA, k0, m0, &sm.full[s]);
-            } else {
-                tma_load(sm.a[s], &mapA, m0, k0, &sm.full[s]);
-                if (a_two) tma_load(sm.a[s] + kTmaABytes / 2, &mapA, m0 + TM / 2, k0, &sm.full[s]);
-            }
-            if (b_kmajor)
-                tma_load(sm.b[s], &mapB, k0, n0, &sm.full[s]);
-            else
-                tma_load(sm.b[s], &mapB, n0, k0, &sm.full[s]);
+            tma_stage_loads(sm.a[s], sm.b[s], &mapA, &mapB, a_kmajor, b_kmajor, a_tx, a_two, m0, n0,
+                            kbeg + kt * TK, &sm.full[s]);
             issued = kt + 1;
         }
         // the loads still in flight land before the CTA can leave: the last one of each stage
@@ -500,6 +588,7 @@ __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ C
         }
     } else if (tid == 32) {
         // MMA issuer
+        const uint32_t idesc = kTmaIdesc | (a_kmajor ? 0u : 1u << 15) | (b_kmajor ? 0u : 1u << 16);
         for (int kt = 0; kt < nk; ++kt) {
             const int s = kt % kTmaStages;
             if (!tc_wait(&sm.full[s], (uint32_t)(kt / kTmaStages) & 1u)) {
@@ -507,73 +596,16 @@ __global__ void __launch_bounds__(128) gemm_tma_kernel(const __grid_constant__ C
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t idesc = kTmaIdesc | (a_kmajor ? 0u : 1u << 15) | (b_kmajor ? 0u : 1u << 16);
-#pragma unroll
-            for (int j = 0; j < TK / 16; ++j) {
-                // K step j: 32 bytes into each swizzled row (K-major) or two 8-row atoms on (MN-major)
-                const uint64_t da = kSwizzle128 | (a_kmajor ? tc_desc(sm.a[s] + j * 32, 16u, 1024u)
-                                                            : tc_desc(sm.a[s] + j * 2048, kTmaABytes / 2, 1024u));
-                const uint64_t db = kSwizzle128 | (b_kmajor ? tc_desc(sm.b[s] + j * 32, 16u, 1024u)
-                                                            : tc_desc(sm.b[s] + j * 2048, kTmaABytes / 2, 1024u));
-                const uint32_t acc = (kt == 0 && j == 0) ? 0u : 1u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                    "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-                    : "memory");
-            }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             tc_smem_addr(&sm.empty[s]))
-                         : "memory");
+            mma_kstep(tmem, sm.a[s], sm.b[s], a_kmajor, b_kmajor, idesc, kt == 0);
+            mma_commit(&sm.empty[s]);
         }
-        // arrives once every MMA issued above has completed
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         tc_smem_addr(&sm.done))
-                     : "memory");
+        mma_commit(&sm.done);  // arrives once every MMA issued above has completed
     }
     if (!tc_wait(&sm.done, 0u)) sm.err = 1;
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (nk > 0 && !sm.err) {
-        const int row = m0 + warp * 32 + lane;
-        const bool split = gridDim.z > 1;
-        const bool vec = !split && beta == 0.f && (ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
-#pragma unroll 1
-        for (int c0 = 0; c0 < TN2; c0 += 16) {
-            uint32_t r[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                "[%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                  "=r"(r[15])
-                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < M) {
-                float *crow = C + (int64_t)row * ldc;
-                if (vec && n0 + c0 + 16 <= N) {
-#pragma unroll
-                    for (int i = 0; i < 16; i += 4)
-                        *reinterpret_cast<float4 *>(crow + n0 + c0 + i) =
-                            make_float4(alpha * __uint_as_float(r[i]), alpha * __uint_as_float(r[i + 1]),
-                                        alpha * __uint_as_float(r[i + 2]), alpha * __uint_as_float(r[i + 3]));
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        const int col = n0 + c0 + i;
-                        if (col < N) {
-                            float *p = crow + col;
-                            const float v = alpha * __uint_as_float(r[i]);
-                            if (split)
-                                atomicAdd(p, v);
-                            else
-                                *p = (beta != 0.f) ? v + beta * (*p) : v;
-                        }
-                    }
-                }
-            }
-        }
-    }
+    if (nk > 0 && !sm.err)
+        store_tile_rows(tmem, warp * 32, 0, lane, m0, n0, M, N, C, ldc, alpha, beta, gridDim.z > 1);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -613,11 +645,6 @@ struct PersistSmem {
     int err;
 };
 constexpr int kPersistSmemBytes = (int)sizeof(PersistSmem) + 1024;
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc_smem_addr(bar)), "r"(count) : "memory");
-}
 
 __global__ void __launch_bounds__(kPThreads, 1) gemm_tma_persistent_kernel(
     const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int a_kmajor, int b_kmajor,
@@ -671,20 +698,8 @@ __global__ void __launch_bounds__(kPThreads, 1) gemm_tma_persistent_kernel(
                     ok = false;
                     break;
                 }
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem_addr(&sm.full[s])),
-                             "r"(a_tx + kTmaBBytes)
-                             : "memory");
-                const int k0 = kt * TK;
-                if (a_kmajor) {
-                    tma_load(sm.a[s], &mapA, k0, m0, &sm.full[s]);
-                } else {
-                    tma_load(sm.a[s], &mapA, m0, k0, &sm.full[s]);
-                    if (a_two) tma_load(sm.a[s] + kTmaABytes / 2, &mapA, m0 + TM / 2, k0, &sm.full[s]);
-                }
-                if (b_kmajor)
-                    tma_load(sm.b[s], &mapB, k0, n0, &sm.full[s]);
-                else
-                    tma_load(sm.b[s], &mapB, n0, k0, &sm.full[s]);
+                tma_stage_loads(sm.a[s], sm.b[s], &mapA, &mapB, a_kmajor, b_kmajor, a_tx, a_two, m0, n0, kt * TK,
+                                &sm.full[s]);
             }
         }
         // the loads still in flight land before the CTA can leave: the last one of each stage
@@ -713,36 +728,15 @@ __global__ void __launch_bounds__(kPThreads, 1) gemm_tma_persistent_kernel(
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-                for (int j = 0; j < TK / 16; ++j) {
-                    const uint64_t da = kSwizzle128 | (a_kmajor ? tc_desc(sm.a[s] + j * 32, 16u, 1024u)
-                                                                : tc_desc(sm.a[s] + j * 2048, kTmaABytes / 2, 1024u));
-                    const uint64_t db = kSwizzle128 | (b_kmajor ? tc_desc(sm.b[s] + j * 32, 16u, 1024u)
-                                                                : tc_desc(sm.b[s] + j * 2048, kTmaABytes / 2, 1024u));
-                    const uint32_t accum = (kt == 0 && j == 0) ? 0u : 1u;
-                    asm volatile(
-                        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
-                        "l"(da), "l"(db), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
-                        : "memory");
-                }
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 tc_smem_addr(&sm.empty[s]))
-                             : "memory");
+                mma_kstep(d, sm.a[s], sm.b[s], a_kmajor, b_kmajor, idesc, kt == 0);
+                mma_commit(&sm.empty[s]);
             }
-            if (ok)
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 tc_smem_addr(&sm.acc_full[acc]))
-                             : "memory");
+            if (ok) mma_commit(&sm.acc_full[acc]);
         }
-        // arrives once every MMA issued above has completed
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         tc_smem_addr(&sm.done))
-                     : "memory");
+        mma_commit(&sm.done);  // arrives once every MMA issued above has completed
     } else if (warp >= 2) {
         // epilogue: warp w owns TMEM lanes 32 (w % 4) .. + 31, i.e. tile rows of that quarter
         const int quarter = warp & 3;
-        const bool vec = beta == 0.f && (ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
         for (int i = 0; i < my_tiles; ++i) {
             const int acc = i & 1;
             // one decision for the warp: the TMEM loads below are warp-collective
@@ -752,40 +746,8 @@ __global__ void __launch_bounds__(kPThreads, 1) gemm_tma_persistent_kernel(
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const int t = blockIdx.x + i * gridDim.x;
-            const int m0 = (t % tiles_m) * TM, n0 = (t / tiles_m) * TN2;
-            const int row = m0 + quarter * 32 + lane;
-#pragma unroll 1
-            for (int c0 = 0; c0 < TN2; c0 += 16) {
-                uint32_t r[16];
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                    "[%16];"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                      "=r"(r[15])
-                    : "r"(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * TN2 + c0)));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (row < M) {
-                    float *crow = C + (int64_t)row * ldc;
-                    if (vec && n0 + c0 + 16 <= N) {
-#pragma unroll
-                        for (int q = 0; q < 16; q += 4)
-                            *reinterpret_cast<float4 *>(crow + n0 + c0 + q) =
-                                make_float4(alpha * __uint_as_float(r[q]), alpha * __uint_as_float(r[q + 1]),
-                                            alpha * __uint_as_float(r[q + 2]), alpha * __uint_as_float(r[q + 3]));
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 16; ++q) {
-                            const int col = n0 + c0 + q;
-                            if (col < N) {
-                                float *p = crow + col;
-                                const float v = alpha * __uint_as_float(r[q]);
-                                *p = (beta != 0.f) ? v + beta * (*p) : v;
-                            }
-                        }
-                    }
-                }
-            }
+            store_tile_rows(tmem, quarter * 32, acc * TN2, lane, (t % tiles_m) * TM, (t / tiles_m) * TN2, M, N, C,
+                            ldc, alpha, beta, false);
             // this warp is done reading the accumulator: the MMAs of tile i + 2 may overwrite it
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
