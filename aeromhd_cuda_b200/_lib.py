@@ -53,7 +53,7 @@ class Grid(_c.Structure):
 class Control(_c.Structure):
     _fields_ = [("t", _D), ("t_end", _D), ("dt", _D), ("dt_cfl", _D), ("ch", _D), ("decay", _D), ("e_bnd", _D),
                 ("last_dt", _D), ("step", _I64), ("max_steps", _I64), ("active", _I32), ("flags", _I32),
-                ("red", _U64 * 4), ("tiles_done", _U32), ("pad_", _U32), ("snap_t", _D), ("scratch", _D),
+                ("red", _U64 * 4), ("queue", _I32 * 2), ("snap_t", _D), ("scratch", _D),
                 ("e_bnd_next", _D), ("reserved", _D)]
 
 

@@ -637,9 +637,12 @@ static int advance_impl(const amhd_grid *g, void *U, void *Ulo, void *U1, void *
     const int n_tiles = one.tiles_x * one.tiles_y;
     const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
     const int defer = is_march(tx);
+    // a persistent marching grid (fewer CTAs than items) draws its items from the
+    // control block's work queue, so that no warp idles while items remain
+    int32_t *queue = (is_march(tx) && grid * (kMarchThreads / 32) < n_tiles) ? ctl->queue : nullptr;
     for (int k = 0; k < n_steps; ++k) {
         if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, grid, U, U1, U2, ctl, 1, 0, 0, 1, 1, s,
-                                 nullptr, nullptr, 1, defer, nullptr, Ulo))
+                                 nullptr, nullptr, 1, defer, queue, Ulo))
             return e;
         CK(run_finalize(g->dtype, nullptr, 1, one, U, ctl, 1, 0, s, defer));
     }

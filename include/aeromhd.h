@@ -93,8 +93,9 @@ typedef struct amhd_control {
     uint64_t red[4];     /* dt reduction accumulators (bit patterns of         */
                          /* non-negative doubles): max cf^2, max(|vx|+|vy|),   */
                          /* max |vx|, max |vy|                                 */
-    uint32_t tiles_done; /* completion counter of the fused dt reduction       */
-    uint32_t pad_;
+    int32_t queue[2];    /* work queue of a persistent marching grid over this  */
+                         /* single grid: {next item, warps finished}, zero     */
+                         /* between launches (amhd_control_init zeroes it)     */
     double snap_t;       /* pause the loop after the step that brings t within */
                          /* 1.5 dt of snap_t (run(), solver.py:487-490);       */
                          /* +inf or NaN: never                                 */

@@ -469,6 +469,29 @@ def test_marching_tma_rows_match_cp_async_rows(amhd, precision, shape, rows, bcy
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("ctas_per_sm", [1, 4])
+def test_persistent_marching_grid_with_queue_equals_default(amhd, precision, ctas_per_sm):
+    """A persistent marching grid over one grid (ctas_per_sm CTAs per SM, fewer
+    warps than items: they draw items from the control block's work queue)
+    gives the bits of the default grid (one CTA per 4 items), step after step
+    through the run loop (the queue is reset by each launch's last warp)."""
+    from aeromhd_cuda_b200 import initial_conditions as ic
+    res = []
+    try:
+        for cps in (0, ctas_per_sm):
+            amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, cps)
+            s = amhd.solver.MHDSolver(ot_cfg(600, precision=precision))
+            s.set_primitive(ic.orszag_tang(s))
+            s.advance(max_steps=6, chunk=3, graph=False)
+            res.append((s.U.clone(), s.t))
+    finally:
+        amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, 0)
+    (a, ta), (b, tb) = res
+    assert ta == tb
+    assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("shape,rows", [((80, 80), -8), ((75, 61), -5), ((64, 130), -32), ((33, 29), -4),
                                         ((40, 200), -24)])
 def test_marching_kernel_matches_tiled(amhd, precision, shape, rows):
