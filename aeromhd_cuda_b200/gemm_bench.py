@@ -116,6 +116,21 @@ def time_train_step(iters: int, warmup: int, H: int = 256, W: int = 64, batch: i
     return out
 
 
+def profile_steps(steps: int = 2, H: int = 256, W: int = 64, batch: int = 16) -> None:
+    """`steps` eager Adam steps of the corrector U-Net on random inputs with the
+    library's GEMM choice and nothing else (a short program for a launch list)."""
+    import torch
+    from .corrector import Corrector
+    net = Corrector(H, W, seed=1)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.randn((10, batch * H * W), device="cuda", generator=g)
+    t = torch.randn((10, batch * H * W), device="cuda", generator=g) * 0.1
+    for _ in range(steps):
+        net.train_step(x, t, batch, lr=1e-5)
+        torch.cuda.synchronize()
+    _check_waits()
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--shapes", nargs="*", default=None, help="tA,tB,M,N,K (default: the corrector's shapes)")
@@ -123,7 +138,12 @@ def main(argv=None) -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--train-step", action="store_true")
     ap.add_argument("--graph", action="store_true", help="time the launches replayed as one CUDA graph")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="only run two eager training steps (for a profiler's launch list) and print nothing")
     args = ap.parse_args(argv)
+    if args.profile_step:
+        profile_steps()
+        return
     shapes = CORRECTOR_SHAPES if not args.shapes else [tuple(int(x) for x in s.split(",")) for s in args.shapes]
     res = {}
     for (tA, tB, M, N, K) in shapes:
