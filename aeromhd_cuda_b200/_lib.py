@@ -100,6 +100,7 @@ _SIGS = {
     "amhd_advance_compensated": ([_c.POINTER(Grid), _P, _P, _P, _P, _P, _I32, _P], _c.c_int),
     "amhd_advance_profile": ([_c.POINTER(Grid), _P, _P, _P, _P, _I32, _c.POINTER(_D), _P], _c.c_int),
     "amhd_step_host": ([_c.POINTER(Grid), _P, _P, _P, _P, _P, _D, _D, _c.POINTER(_D), _P], _c.c_int),
+    "amhd_step_host_n": ([_c.POINTER(Grid), _P, _P, _P, _P, _P, _D, _D, _I32, _c.POINTER(_D), _P], _c.c_int),
     "amhd_diagnostics": ([_c.POINTER(Grid), _P, _D, _P, _P, _P], _c.c_int),
     "amhd_diagnostics_noalloc": ([_c.POINTER(Grid), _P, _D, _P, _P], _c.c_int),
     "amhd_diagnostics_colour": ([_c.POINTER(Grid), _P, _D, _P, _P, _P, _P], _c.c_int),

@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -810,6 +811,110 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
         for (int v = 0; v < 10; ++v)
             CK(cudaMemcpy2DAsync(h + (size_t)v * nxt * nyt * es, (size_t)nyt * es, d + (size_t)v * g->var_stride * es,
                                  (size_t)g->pitch * es, (size_t)nyt * es, nxt, cudaMemcpyDeviceToHost, s));
+    amhd_control r;
+    CK(cudaMemcpyAsync(&r, ctl, sizeof r, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (out_host) {
+        out_host[0] = r.t;
+        out_host[1] = r.last_dt;
+        out_host[2] = r.ch;
+        out_host[3] = r.e_bnd;
+    }
+    if (r.flags & AMHD_FLAG_TIMEOUT) return fail(AMHD_ERR_TIMEOUT, "a bounded device wait expired; tiles not updated");
+    if (r.flags & AMHD_FLAG_NONFINITE) return fail(AMHD_ERR_NONFINITE, "non-finite value in the new state");
+    return AMHD_OK;
+}
+
+// Copy streams and events of amhd_step_host_n, created once per device: one
+// stream per direction (both PCIe directions busy at once), an event per plane
+// marking that a step's copy of that plane has reached the host.
+struct HostLoopStreams {
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t out[10] = {}, in_done = nullptr, step_done = nullptr, out_done = nullptr;
+};
+
+static HostLoopStreams *host_loop_streams()
+{
+    static std::mutex mu;
+    static std::map<int, HostLoopStreams> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(dev);
+    if (it != cache.end()) return &it->second;
+    HostLoopStreams h;
+    bool ok = cudaStreamCreateWithFlags(&h.h2d, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&h.d2h, cudaStreamNonBlocking) == cudaSuccess;
+    for (int v = 0; v < 10 && ok; ++v) ok = cudaEventCreateWithFlags(&h.out[v], cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&h.in_done, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.step_done, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventCreateWithFlags(&h.out_done, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) return nullptr;
+    return &(cache[dev] = h);
+}
+
+int amhd_step_host_n(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, void *dev_U2, amhd_control *ctl,
+                     double t, double t_end, int32_t n_steps, double *out_host, void *stream)
+{
+    if (int e = check_grid(g)) return e;
+    const void *ptrs[3] = {dev_U, dev_U1, dev_U2};
+    if (int e = check_padded(g, ptrs, 3)) return e;
+    if (!U_host || !ctl) return fail(AMHD_ERR_ARG, "NULL argument");
+    if (n_steps < 1) return fail(AMHD_ERR_ARG, "n_steps < 1");
+    HostLoopStreams *hs = host_loop_streams();
+    if (!hs) return fail(AMHD_ERR_CUDA, "copy streams could not be created");
+    cudaStream_t s = S(stream);
+    const size_t es = elem_size(g->dtype);
+    const int nxt = g->nx + 2 * kNG, nyt = g->ny + 2 * kNG;
+    char *h = static_cast<char *>(U_host);
+    char *d = static_cast<char *>(dev_U);
+    const bool contiguous = g->pitch == nyt;
+    auto copy_plane = [&](int v, bool to_device, cudaStream_t cs) -> cudaError_t {
+        char *hp = h + (size_t)v * nxt * nyt * es;
+        char *dp = d + (size_t)v * g->var_stride * es;
+        if (contiguous)
+            return to_device ? cudaMemcpyAsync(dp, hp, (size_t)nxt * nyt * es, cudaMemcpyHostToDevice, cs)
+                             : cudaMemcpyAsync(hp, dp, (size_t)nxt * nyt * es, cudaMemcpyDeviceToHost, cs);
+        return to_device ? cudaMemcpy2DAsync(dp, (size_t)g->pitch * es, hp, (size_t)nyt * es, (size_t)nyt * es, nxt,
+                                             cudaMemcpyHostToDevice, cs)
+                         : cudaMemcpy2DAsync(hp, (size_t)nyt * es, dp, (size_t)g->pitch * es, (size_t)nyt * es, nxt,
+                                             cudaMemcpyDeviceToHost, cs);
+    };
+    const int tx = tile_of(g);
+    const amhd_instance one = single_instance(g, tx);
+    const int n_tiles = one.tiles_x * one.tiles_y;
+    const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
+    // the copy streams start after what the caller queued before this call
+    CK(cudaEventRecord(hs->step_done, s));
+    CK(cudaStreamWaitEvent(hs->h2d, hs->step_done, 0));
+    if (int e = control_upload(ctl, t, t_end, 0, n_steps, s)) return e;
+    for (int k = 0; k < n_steps; ++k) {
+        // the inputs of step k, plane by plane, each as soon as step k-1's result
+        // for that plane is back in U_host (the other direction is still busy
+        // with the later planes)
+        for (int v = 0; v < 10; ++v) {
+            if (k > 0) CK(cudaStreamWaitEvent(hs->h2d, hs->out[v], 0));
+            CK(copy_plane(v, true, hs->h2d));
+        }
+        CK(cudaEventRecord(hs->in_done, hs->h2d));
+        CK(cudaStreamWaitEvent(s, hs->in_done, 0));
+        // as amhd_step_host: dt from the uploaded state, one SSP-RK3 step
+        CK(run_dt_reduce(g, dev_U, 0, ctl, s));
+        CK(run_finalize(g->dtype, nullptr, 1, one, dev_U, ctl, 0, 0, s));
+        CK(run_bc_fill(g, dev_U, s));
+        if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, grid, dev_U, dev_U1, dev_U2, ctl, 1, 0, 0, 1,
+                                 0, s))
+            return e;
+        CK(run_finalize(g->dtype, nullptr, 1, one, dev_U, ctl, 1, 0, s));
+        CK(cudaEventRecord(hs->step_done, s));
+        CK(cudaStreamWaitEvent(hs->d2h, hs->step_done, 0));
+        for (int v = 0; v < 10; ++v) {
+            CK(copy_plane(v, false, hs->d2h));
+            CK(cudaEventRecord(hs->out[v], hs->d2h));
+        }
+    }
+    CK(cudaEventRecord(hs->out_done, hs->d2h));
+    CK(cudaStreamWaitEvent(s, hs->out_done, 0));
     amhd_control r;
     CK(cudaMemcpyAsync(&r, ctl, sizeof r, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

@@ -57,7 +57,7 @@ def parse_args(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
     ap.add_argument("--n", type=int, default=2048)
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--fp32-compensation", action="store_true",
@@ -452,9 +452,11 @@ def run_ours(a, world, rank, local):
 
 
 def run_e2e(s, steps, world):
-    """Zone-updates/s through the host-buffer entry point (amhd_step_host): every step
-    copies the state from pinned host memory to the device, advances one run-loop
-    step and copies it back, timed with events on the launching stream."""
+    """Zone-updates/s through the host-buffer entry point (amhd_step_host_n): every
+    step copies the state from pinned host memory to the device, advances one
+    run-loop step and copies it back (the steps' copies overlapped plane by plane
+    across the two PCIe directions), timed with events on the launching stream;
+    the one-call-per-step amhd_step_host is timed beside it."""
     import torch
     from aeromhd_cuda_b200 import _lib, _tensors
     cfg, g, stream = s.cfg, s._grid(), _tensors.stream_ptr()
@@ -468,23 +470,46 @@ def run_e2e(s, steps, world):
                   _tensors.ptr(s._U2), _tensors.ptr(s._ctl), t, cfg.t_end, out, stream)
         return out[0]
 
+    def e2e_steps(t, n):
+        _lib.call("amhd_step_host_n", g, host.data_ptr(), _tensors.ptr(s._U), _tensors.ptr(s._U1),
+                  _tensors.ptr(s._U2), _tensors.ptr(s._ctl), t, cfg.t_end, n, out, stream)
+        return out[0]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        barrier(world)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        fn()
+        ev1.record()
+        torch.cuda.synchronize()
+        return max_over_ranks(ev0.elapsed_time(ev1), world)
+
     for _ in range(2):
         t_now = e2e_step(t_now)
-    torch.cuda.synchronize()
-    barrier(world)
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record()
-    for _ in range(steps):
-        t_now = e2e_step(t_now)
-    ev1.record()
-    torch.cuda.synchronize()
-    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    t_now = e2e_steps(t_now, 2)
+    state = {"t": t_now}
+
+    def one_call_per_step():
+        for _ in range(steps):
+            state["t"] = e2e_step(state["t"])
+
+    def one_call():
+        state["t"] = e2e_steps(state["t"], steps)
+
+    ms_single = timed(one_call_per_step)
+    ms = timed(one_call)
     state_bytes = host.numel() * host.element_size()
     ctl_bytes = ctypes.sizeof(_lib.Control)
     return {"value": world * cfg.nx * cfg.ny * steps / (ms / 1e3), "unit": UNIT,
-            "h2d_bytes_per_step": state_bytes + ctl_bytes, "d2h_bytes_per_step": state_bytes + ctl_bytes,
-            "ms_per_step": ms / steps, "precision": cfg.precision,
-            "path": "amhd_step_host: pinned host state -> device, one run-loop step, -> host"}
+            "h2d_bytes_per_step": state_bytes + round(ctl_bytes / steps),
+            "d2h_bytes_per_step": state_bytes + round(ctl_bytes / steps),
+            "ms_per_step": ms / steps, "precision": cfg.precision, "steps": steps,
+            "path": "amhd_step_host_n: every step the pinned host state -> device, one run-loop step, -> host; "
+                    "the copies of consecutive steps overlapped plane by plane across the two PCIe directions",
+            "one_call_per_step": {"value": world * cfg.nx * cfg.ny * steps / (ms_single / 1e3),
+                                  "ms_per_step": ms_single / steps,
+                                  "path": "amhd_step_host per step: copies in, step, copies out, serial"}}
 
 
 def reference_path(backend, n, steps, warmup, device="cuda"):

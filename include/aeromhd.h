@@ -265,6 +265,16 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
  * Synchronises. */
 int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, void *dev_U2, amhd_control *ctl,
                    double t, double t_end, double *out_host, void *stream);
+/* n_steps iterations of amhd_step_host in one call, the same bits: every step
+ * copies its input from U_host and its result back into U_host, plane by
+ * plane on two copy streams of the library (one per direction), so that a
+ * plane of step k+1 travels to the device as soon as step k's result for that
+ * plane is back, while the other planes of step k are still travelling the
+ * other way (with pinned U_host both PCIe directions are busy at once).
+ * out_host receives {t, dt of the last step, glm_ch, boundary energy flux x dt
+ * summed over the n steps}.  Synchronises. */
+int amhd_step_host_n(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, void *dev_U2, amhd_control *ctl,
+                     double t, double t_end, int32_t n_steps, double *out_host, void *stream);
 /* compute_diagnostics, solver.py:335-444 (the conserved-quantity part):
  * out_dev receives (float64) [0] mass = sum(rho) dx dy, [1] energy = sum(E)
  * dx dy (solver.py:430), [2] max|divB|, [3] sqrt(mean divB^2) (:419-428),

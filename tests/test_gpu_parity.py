@@ -349,6 +349,39 @@ def test_step_host_entry_point_matches_device_loop(amhd, n):
     assert rel_l1(host[:, 2:-2, 2:-2], np_(ref.U)[:, 2:-2, 2:-2]) < 1e-13
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [64, 60])  # 64: planes contiguous on both sides; 60: padded rows (2-D plane copies)
+@pytest.mark.parametrize("bcx", ["periodic", "extrapolation"])
+def test_step_host_n_equals_repeated_step_host(amhd, precision, n, bcx):
+    """amhd_step_host_n (n steps, each copying its input from pinned host memory
+    and its result back, the two directions overlapped plane by plane) gives the
+    bits of n calls of amhd_step_host, and the same t, dt, ch and summed
+    boundary energy."""
+    from aeromhd_cuda_b200 import _tensors, initial_conditions as ic
+    steps = 4
+    cfg = C(nx=n, ny=n, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, t_end=0.5, cfl=0.4, gamma=5.0 / 3.0,
+            powell_source=False, bc_x_type=bcx, bc_y_type="periodic", precision=precision)
+    s = amhd.solver.MHDSolver(cfg)
+    s.set_primitive(ic.orszag_tang(s))
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    hosts = [torch.empty(tuple(s.U.shape), dtype=dt).pin_memory() for _ in range(2)]
+    for h in hosts:
+        h.copy_(s.U.cpu())
+    args = (_tensors.ptr(s._U), _tensors.ptr(s._U1), _tensors.ptr(s._U2), _tensors.ptr(s._ctl))
+    out = (ctypes.c_double * 4)()
+    t, e_bnd = 0.0, 0.0
+    for _ in range(steps):
+        amhd.lib.call("amhd_step_host", s._grid(), hosts[0].data_ptr(), *args, t, 0.5, out, _tensors.stream_ptr())
+        t, e_bnd = out[0], e_bnd + out[3]
+    one = list(out)
+    outn = (ctypes.c_double * 4)()
+    amhd.lib.call("amhd_step_host_n", s._grid(), hosts[1].data_ptr(), *args, 0.0, 0.5, steps, outn,
+                  _tensors.stream_ptr())
+    assert torch.equal(hosts[0], hosts[1])
+    assert outn[0] == t and outn[1] == one[1] and outn[2] == one[2]
+    assert abs(outn[3] - e_bnd) <= 1e-12 * max(abs(e_bnd), 1e-300)
+
+
 def test_nonfinite_state_is_reported_not_trapped(amhd):
     """A NaN planted on the host is reported through the control flags; the context stays usable."""
     from aeromhd_cuda_b200 import initial_conditions as ic
