@@ -83,6 +83,51 @@ def test_argument_errors_are_codes_not_crashes(L):
     assert L.amhd_hlld_flux(0, 0, None, None, None, None, 0, 1.4, 1.0, None) == _lib.AMHD_OK
 
 
+def test_new_entry_points_reject_bad_arguments(L):
+    """amhd_step_host_n, the GEMM operand relayouts and the persistent-GEMM
+    switch refuse bad arguments with codes, before any device call."""
+    from aeromhd_cuda_b200 import _lib
+    p, r = ctypes.c_int32(), ctypes.c_int32()
+    assert L.amhd_padded_layout(8, 8, 0, ctypes.byref(p), ctypes.byref(r)) == _lib.AMHD_OK
+    g = _lib.Grid(nx=8, ny=8, pitch=p.value, dtype=0, var_stride=r.value * p.value, dx=0.1, dy=0.1, gamma=1.4,
+                  cfl=0.3, glm_alpha=1.5)
+    buf = ctypes.c_void_p(256)
+    out = (ctypes.c_double * 4)()
+    step_n = L.amhd_step_host_n
+    assert step_n(ctypes.byref(g), None, buf, buf, buf, buf, 0.0, 1.0, 3, out, None) == _lib.AMHD_ERR_ARG
+    assert step_n(ctypes.byref(g), buf, buf, buf, buf, buf, 0.0, 1.0, 0, out, None) == _lib.AMHD_ERR_ARG
+    assert b"n_steps" in L.amhd_last_error()
+    g.pitch = 4  # below ny + 4
+    assert step_n(ctypes.byref(g), buf, buf, buf, buf, buf, 0.0, 1.0, 3, out, None) == _lib.AMHD_ERR_ARG
+    assert L.amhd_nn_flip3(buf, 4, 3, 35, buf, None) == _lib.AMHD_ERR_ARG   # ldo < cout * 9
+    assert L.amhd_nn_flip3(None, 4, 3, 40, buf, None) == _lib.AMHD_ERR_ARG
+    assert L.amhd_nn_pad_cols(buf, 4, 90, 89, buf, None) == _lib.AMHD_ERR_ARG  # ldo < cols
+    assert L.amhd_nn_pad_cols(buf, 0, 90, 96, buf, None) == _lib.AMHD_ERR_ARG
+    assert L.amhd_nn_set_gemm_persistent(2) == _lib.AMHD_ERR_ARG
+    assert L.amhd_nn_set_gemm_persistent(0) == _lib.AMHD_OK
+    assert L.amhd_nn_set_gemm_persistent(1) == _lib.AMHD_OK
+
+
+def test_corrector_padding_rows_zeroed_once_per_shape():
+    """The corrector's zero-padded GEMM workspaces (K rounded up to a multiple of
+    8 for the TMA path): the padding rows are zeroed when the buffer or its
+    shape is new, and left alone on the next calls of the same shape (a captured
+    training step must not contain the fill)."""
+    import torch
+    from aeromhd_cuda_b200.corrector import Corrector, _round8
+    assert (_round8(90), _round8(96), _round8(1)) == (96, 96, 8)
+    c = Corrector(16, 16, device="cpu")
+    t = c._padded_rows("e1.col", 90, 96, 10)
+    assert t.shape == (96, 10) and torch.all(t[90:] == 0)
+    t.fill_(1.0)
+    t = c._padded_rows("e1.col", 90, 96, 10)
+    assert torch.all(t[90:] == 1)            # same shape: not refilled
+    t = c._padded_rows("e1.col", 90, 96, 8)  # new shape: the padding rows of the new view are zeroed
+    assert torch.all(t[90:] == 0)
+    u = c._padded_rows("colg", 96, 96, 10)   # nothing to pad
+    assert u.shape == (96, 10)
+
+
 def test_config_keeps_reference_fields_and_defaults():
     from aeromhd_cuda_b200.config import Config
     c = Config()
