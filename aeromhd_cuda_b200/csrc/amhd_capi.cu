@@ -832,6 +832,8 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
 // at 2048^2 (5.28 against 4.96 ms per step).
 constexpr int kHostPieces = 1;
 struct HostLoopStreams {
+    std::mutex busy;  // one call at a time per device (the call is synchronous)
+    bool ready = false;
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t out[10 * kHostPieces] = {}, in_done = nullptr, step_done = nullptr, out_done = nullptr;
 };
@@ -839,13 +841,12 @@ struct HostLoopStreams {
 static HostLoopStreams *host_loop_streams()
 {
     static std::mutex mu;
-    static std::map<int, HostLoopStreams> cache;
+    static std::map<int, HostLoopStreams> cache;  // nodes never move: the entries stay valid
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
     std::lock_guard<std::mutex> lock(mu);
-    auto it = cache.find(dev);
-    if (it != cache.end()) return &it->second;
-    HostLoopStreams h;
+    HostLoopStreams &h = cache[dev];
+    if (h.ready) return &h;
     bool ok = cudaStreamCreateWithFlags(&h.h2d, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&h.d2h, cudaStreamNonBlocking) == cudaSuccess;
     for (int v = 0; v < 10 * kHostPieces && ok; ++v)
@@ -854,7 +855,8 @@ static HostLoopStreams *host_loop_streams()
          cudaEventCreateWithFlags(&h.step_done, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventCreateWithFlags(&h.out_done, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) return nullptr;
-    return &(cache[dev] = h);
+    h.ready = true;
+    return &h;
 }
 
 int amhd_step_host_n(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, void *dev_U2, amhd_control *ctl,
@@ -867,6 +869,7 @@ int amhd_step_host_n(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1
     if (n_steps < 1) return fail(AMHD_ERR_ARG, "n_steps < 1");
     HostLoopStreams *hs = host_loop_streams();
     if (!hs) return fail(AMHD_ERR_CUDA, "copy streams could not be created");
+    std::lock_guard<std::mutex> busy(hs->busy);  // callers on other threads share the copy streams
     cudaStream_t s = S(stream);
     const size_t es = elem_size(g->dtype);
     const int nxt = g->nx + 2 * kNG, nyt = g->ny + 2 * kNG;

@@ -272,7 +272,8 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
  * plane is back, while the other planes of step k are still travelling the
  * other way (with pinned U_host both PCIe directions are busy at once).
  * out_host receives {t, dt of the last step, glm_ch, boundary energy flux x dt
- * summed over the n steps}.  Synchronises. */
+ * summed over the n steps}.  Synchronises; calls on one device from several
+ * threads run one after the other. */
 int amhd_step_host_n(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, void *dev_U2, amhd_control *ctl,
                      double t, double t_end, int32_t n_steps, double *out_host, void *stream);
 /* compute_diagnostics, solver.py:335-444 (the conserved-quantity part):
