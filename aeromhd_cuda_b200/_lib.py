@@ -59,7 +59,7 @@ class Control(_c.Structure):
 
 class Instance(_c.Structure):
     _fields_ = [("grid", Grid), ("offset", _I64), ("first_tile", _I32), ("tiles_x", _I32), ("tiles_y", _I32),
-                ("cut_x", _I32)]
+                ("cut_x", _I32), ("pack", _I32), ("reserved", _I32)]
 
 
 class NNTensor(_c.Structure):
@@ -111,6 +111,9 @@ _SIGS = {
                               _c.c_int),
     "amhd_ensemble_tensormaps": ([_P, _I32, _I32, _I32, _P, _P, _P, _P], _c.c_int),
     "amhd_set_tma": ([_I32], _c.c_int),
+    "amhd_march_pack": ([_I32], _c.c_int),
+    "amhd_march_items": ([_I32, _I32, _I32, _I32], _c.c_int),
+    "amhd_set_march_pack": ([_I32], _c.c_int),
     "amhd_selftest_wait": ([_I32, _I64, _P, _P], _c.c_int),
     "amhd_ensemble_continue": ([_P, _P, _I32, _I32, _P, _P, _D, _P], _c.c_int),
     "amhd_ensemble_init": ([_P, _P, _I32, _I32, _P, _P, _D, _I64, _P], _c.c_int),

@@ -44,6 +44,7 @@ constexpr int kTY = 32;
 int g_tile_x = 0;  // 0: per precision (tile_of)
 int g_ctas_per_sm = 0;
 int g_use_tma = 1;
+int g_march_pack = 1;  // single grids: the last strip's row chunks share warps (march_pack)
 
 inline size_t elem_size(int dtype) { return dtype == AMHD_F32 ? 4 : 8; }
 
@@ -104,11 +105,19 @@ amhd_instance single_instance(const amhd_grid *g, int tile_x)
     if (is_march(tile_x)) {
         in.tiles_x = (g->nx - tile_x - 1) / -tile_x;
         in.tiles_y = (g->ny + kMarchCols - 1) / kMarchCols;
+        // the last strip's chunks share warps unless the rows are staged by TMA
+        in.pack = (g_march_pack && !(g_use_tma & 2)) ? march_pack(g->ny) : 1;
     } else {
         in.tiles_x = (g->nx + tile_x - 1) / tile_x;
         in.tiles_y = (g->ny + kTY - 1) / kTY;
     }
     return in;
+}
+
+// work items of a single-grid launch of this geometry
+int n_items(const amhd_instance &in, int tile_x)
+{
+    return is_march(tile_x) ? march_item_count(in.grid.nx, in.grid.ny, -tile_x, in.pack) : in.tiles_x * in.tiles_y;
 }
 
 inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -346,6 +355,21 @@ int amhd_set_tma(int32_t mode)
     return AMHD_OK;
 }
 
+int amhd_march_pack(int32_t ny) { return ny > 0 ? march_pack(ny) : 1; }
+
+int amhd_march_items(int32_t nx, int32_t ny, int32_t rows, int32_t pack)
+{
+    if (nx <= 0 || ny <= 0 || rows <= 0) return 0;
+    return march_item_count(nx, ny, rows, pack);
+}
+
+int amhd_set_march_pack(int32_t on)
+{
+    if (on != 0 && on != 1) return fail(AMHD_ERR_ARG, "march pack switch must be 0 or 1, got %d", on);
+    g_march_pack = on;
+    return AMHD_OK;
+}
+
 int amhd_selftest_wait(int32_t arrive, int64_t limit_ns, int32_t *timed_out, int32_t *waited_us)
 {
     if (limit_ns <= 0 || limit_ns > 2000000000LL || !timed_out || !waited_us)
@@ -552,7 +576,7 @@ int amhd_compute_rhs(const amhd_grid *g, void *U, void *R, double ch, void *stre
     set_input(p, U, U, g, tx);
     p.uout = R;
     p.one = one;
-    p.n_tiles = one.tiles_x * one.tiles_y;
+    p.n_tiles = n_items(one, tx);
     p.ch = ch;
     CK(run_stage(g->dtype, 0, tx, p, stage_grid(g->dtype, tx, p.n_tiles, g_ctas_per_sm), s));
     return AMHD_OK;
@@ -575,7 +599,7 @@ int amhd_step_ssprk3(const amhd_grid *g, void *U, void *U1, void *U2, double dt,
     CK(run_bc_fill(g, U, s));  // compute_rhs(U0) fills U0's ghosts first (solver.py:276)
     const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
-    const int n_tiles = one.tiles_x * one.tiles_y;
+    const int n_tiles = n_items(one, tx);
     return three_stages(g, one, nullptr, nullptr, n_tiles, tx, stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm), U,
                         U1, U2, ctl, 0, dt, ch, ch > 0 ? decay : 1.0, 0, s);
 }
@@ -594,7 +618,7 @@ int amhd_rk_stage(const amhd_grid *g, int32_t stage, const void *Uin, const void
     set_input(p, Uin, U0, g, tx);
     p.uout = Uout;
     p.one = one;
-    p.n_tiles = one.tiles_x * one.tiles_y;
+    p.n_tiles = n_items(one, tx);
     p.dt = dt;
     p.ch = ch;
     p.decay = ch > 0 ? decay : 1.0;
@@ -635,7 +659,7 @@ static int advance_impl(const amhd_grid *g, void *U, void *Ulo, void *U1, void *
     cudaStream_t s = S(stream);
     const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
-    const int n_tiles = one.tiles_x * one.tiles_y;
+    const int n_tiles = n_items(one, tx);
     const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
     const int defer = is_march(tx);
     // a persistent marching grid (fewer CTAs than items) draws its items from the
@@ -695,7 +719,7 @@ int amhd_advance_stage(const amhd_grid *g, int32_t stage, void *U, void *U1, voi
     set_input(p, in[stage - 1], U, g, tx);
     p.uout = out[stage - 1];
     p.one = one;
-    p.n_tiles = one.tiles_x * one.tiles_y;
+    p.n_tiles = n_items(one, tx);
     p.ctl = ctl;
     p.use_ctl = 1;
     p.fuse_dt = stage == 3;
@@ -726,7 +750,7 @@ int amhd_advance_profile(const amhd_grid *g, void *U, void *U1, void *U2, amhd_c
     cudaStream_t s = S(stream);
     const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
-    const int n_tiles = one.tiles_x * one.tiles_y;
+    const int n_tiles = n_items(one, tx);
     const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
     std::vector<cudaEvent_t> ev(4 * (size_t)n_steps + 1);
     for (auto &e : ev) CK(cudaEventCreate(&e));
@@ -800,7 +824,7 @@ int amhd_step_host(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1, 
     const amhd_instance one = single_instance(g, tx);
     CK(run_finalize(g->dtype, nullptr, 1, one, dev_U, ctl, 0, 0, s));
     CK(run_bc_fill(g, dev_U, s));
-    const int n_tiles = one.tiles_x * one.tiles_y;
+    const int n_tiles = n_items(one, tx);
     if (int e = three_stages(g, one, nullptr, nullptr, n_tiles, tx, stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm),
                              dev_U, dev_U1, dev_U2, ctl, 1, 0, 0, 1, 0, s))
         return e;
@@ -892,7 +916,7 @@ int amhd_step_host_n(const amhd_grid *g, void *U_host, void *dev_U, void *dev_U1
     };
     const int tx = tile_of(g);
     const amhd_instance one = single_instance(g, tx);
-    const int n_tiles = one.tiles_x * one.tiles_y;
+    const int n_tiles = n_items(one, tx);
     const int grid = stage_grid(g->dtype, tx, n_tiles, g_ctas_per_sm);
     // the copy streams start after what the caller queued before this call
     CK(cudaEventRecord(hs->step_done, s));

@@ -742,9 +742,43 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
                                            int ii, const amhd_grid &g, int item, int lane, double dt, double ch,
                                            double decay, unsigned long long q[4], bool &bad, uint32_t &phase)
 {
+    // Item -> column strip, row chunk and this lane's column.  A plain item is one
+    // chunk of one strip across the warp's 32 lanes (28 columns updated).  With
+    // in.pack = P > 1 the items of the last strip, whose leftover columns (with
+    // their 2-column halo on each side) fit 32/P lanes, put P segments of 32/P
+    // lanes side by side, segment s walking chunk P m + s; all segments of an
+    // item have as many rows (the short last chunk has an item of its own).
+    // The packed items come first, the plain ones chunk-major after them.
     const int local = item - in.first_tile;
-    const int strip = local % in.tiles_y, chunk = local / in.tiles_y;
-    const int j = kMarchCols * strip + lane;  // storage column of this lane (first interior column - 2 + lane)
+    const int P = (TMA || in.pack <= 1) ? 1 : in.pack;
+    const int plain_strips = P > 1 ? in.tiles_y - 1 : in.tiles_y;
+    const int full_chunks = g.nx / p.march_rows;
+    const int n_full_packed = P > 1 ? (full_chunks + P - 1) / P : 0;
+    const int n_packed = P > 1 ? n_full_packed + (full_chunks * p.march_rows < g.nx ? 1 : 0) : 0;
+    int strip, chunk, n_rows, lane_c = lane, seg_w = 32;
+    bool seg_live = true;
+    if (local >= n_packed) {
+        strip = (local - n_packed) % plain_strips;
+        chunk = (local - n_packed) / plain_strips;
+        n_rows = min(p.march_rows, g.nx - chunk * p.march_rows);
+    } else {
+        const int m = local;
+        const int seg = P == 4 ? lane >> 3 : lane >> 4;
+        seg_w = P == 4 ? 8 : 16;
+        lane_c = lane - seg * seg_w;
+        strip = in.tiles_y - 1;
+        if (m < n_full_packed) {
+            chunk = m * P + seg;
+            seg_live = chunk < full_chunks;
+            if (!seg_live) chunk = m * P;  // walks the first segment's rows, stores nothing
+            n_rows = p.march_rows;
+        } else {
+            chunk = full_chunks;
+            seg_live = seg == 0;
+            n_rows = g.nx - full_chunks * p.march_rows;
+        }
+    }
+    const int j = kMarchCols * strip + lane_c;  // storage column of this lane (first interior column - 2 + lane_c)
     // ghost cells of the input: as stored, or (pull) taken from the interior cells
     // they copy (apply_bc, solver.py:158-197; psi zero in non-periodic x ghosts)
     const bool pull = p.pull_ghosts != 0;
@@ -755,15 +789,15 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
     auto ghost_psi = [&](int r, R u[NV]) {
         if (zero_psi && (r < NG || r >= NG + g.nx)) u[PSI] = R(0);
     };
-    const int ib = NG + chunk * p.march_rows;
-    const int ie = min(ib + p.march_rows, NG + g.nx);
+    const int ib = NG + chunk * p.march_rows;  // first row of this lane's chunk
     const int64_t vs = g.var_stride;
     const int pitch = g.pitch;
     const R *uin = reinterpret_cast<const R *>(p.uin) + in.offset;
     const R *u0 = reinterpret_cast<const R *>(p.u0) + in.offset;
     R *uout = reinterpret_cast<R *>(p.uout) + in.offset;
     R *ulo = COMP ? reinterpret_cast<R *>(p.ulo) + in.offset : nullptr;
-    const bool out_lane = lane >= NG && lane < NG + kMarchCols && j < NG + g.ny;
+    // the segment's two lanes on each side are its halo
+    const bool out_lane = seg_live && lane_c >= NG && lane_c < seg_w - NG && j < NG + g.ny;
     // U0 comes from its own buffer unless it is the stage input (stage 1 of a step)
     const bool own_base = STAGE >= 1 && p.u0 != p.uin;
 
@@ -861,11 +895,12 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
     // Rows ib-2 .. ib are fetched up front and row ib+1 behind them.  The walk
     // starts one row early: iteration ib-1 only computes the flux through face
     // ib-1/2 (no y faces, no update), so the x-face code is not repeated in a
-    // prologue.  Input row r lives in slot r % 3; each iteration fetches the
-    // input row three ahead and the next row of U0 once it is done with the
-    // slots they replace, and waits for them just before the x faces.
-    int s0 = (ib - 2) % 3;  // slot of row i (ib-2 here)
-    const int s1i = s0 == 2 ? 0 : s0 + 1, s2i = s1i == 2 ? 0 : s1i + 1;
+    // prologue.  Input row ib-2+k lives in slot k % 3 (the same slot in every
+    // segment of an item); each iteration fetches the input row three ahead and
+    // the next row of U0 once it is done with the slots they replace, and waits
+    // for them just before the x faces.
+    int s0 = 0;  // slot of row i (ib-2 here)
+    constexpr int s1i = 1, s2i = 2;
     fetch_in(s0, ib - 2);
     fetch_in(s1i, ib - 1);
     fetch_in(s2i, ib);
@@ -888,8 +923,9 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
     }
     s0 = s1i;  // slot of row ib-1
 
-    for (int i = ib - 1; i < ie; ++i) {
-        const bool full = i >= ib;  // warp-uniform: iteration ib-1 only prepares face ib-1/2
+    for (int r = -1; r < n_rows; ++r) {
+        const int i = ib + r;       // row of this lane's chunk
+        const bool full = r >= 0;  // warp-uniform: iteration ib-1 only prepares face ib-1/2
         const int s2 = s0 == 0 ? 2 : s0 - 1;  // slot of row i+2 (== (i + 2) % 3)
         __syncwarp();  // the left neighbour has read ms.fy of row i-1
         R bym = R(0), byp = R(0);
@@ -1034,7 +1070,7 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
             }
         }
         // rows done with: input row i (slot s0) -> row i+3; U0 of row i -> row i+1
-        if (i + 1 < ie) {
+        if (r + 1 < n_rows) {
             fetch_in(s0, i + 3);
             if (own_base) fetch_base(i + 1);
         }

@@ -52,6 +52,22 @@ struct StageParams {
 constexpr int kMarchCols = 28;     // 32 lanes minus a 2-column halo on each side
 constexpr int kMarchThreads = 128; // 4 independent warps per CTA
 inline bool is_march(int tile_x) { return tile_x < 0; }
+// row chunks of an instance's last column strip per work item: its ny mod 28
+// leftover columns plus a 2-column halo each side in 8 lanes (4 chunks to a
+// warp) or 16 lanes (2); 1 when the strip is full or wider than 12 columns
+inline int march_pack(int ny)
+{
+    const int rem = ny % kMarchCols;
+    return rem == 0 ? 1 : rem <= 4 ? 4 : rem <= 12 ? 2 : 1;
+}
+// work items of an nx x ny instance in chunks of `rows` rows with that packing
+inline int march_item_count(int nx, int ny, int rows, int pack)
+{
+    const int chunks = (nx + rows - 1) / rows, strips = (ny + kMarchCols - 1) / kMarchCols;
+    if (pack <= 1) return chunks * strips;
+    const int full = nx / rows;
+    return (strips - 1) * chunks + (full + pack - 1) / pack + (nx % rows ? 1 : 0);
+}
 inline bool valid_geometry(int tile_x)
 {
     return tile_x == 4 || tile_x == 8 || tile_x == 16 || (tile_x <= -4 && tile_x >= -1024);

@@ -81,8 +81,33 @@ def work_shape(tile_x: int) -> tuple:
     return (tile_x, 32) if tile_x > 0 else (-tile_x, MARCH_COLS)
 
 
-def tile_counts(configs: Sequence[Config], tile_x: int) -> np.ndarray:
+def march_pack(ny: int) -> int:
+    """Row chunks of the last column strip that share one warp-marching item
+    (amhd_march_pack): the strip's ny mod 28 columns plus a 2-column halo on
+    each side in 8 lanes (4 chunks) or 16 lanes (2); 1 when the strip is full or
+    wider than 12 columns."""
+    rem = ny % MARCH_COLS
+    return 1 if rem == 0 else 4 if rem <= 4 else 2 if rem <= 12 else 1
+
+
+def march_items(nx: int, ny: int, rows: int, pack: int) -> int:
+    """Work items of an nx x ny instance in chunks of `rows` rows (amhd_march_items):
+    chunks x strips unpacked; packed, the full-width strips' items, then
+    ceil(full-height chunks / pack) items of the last strip and one for a short
+    last chunk."""
+    chunks, strips = -(-nx // rows), -(-ny // MARCH_COLS)
+    if pack <= 1:
+        return chunks * strips
+    full = nx // rows
+    return (strips - 1) * chunks + -(-full // pack) + (1 if nx % rows else 0)
+
+
+def tile_counts(configs: Sequence[Config], tile_x: int, pack: bool = False) -> np.ndarray:
+    """Work items per instance; pack (marching kernel): the last strip's row
+    chunks share warps (march_pack)."""
     r, c_ = work_shape(tile_x)
+    if tile_x < 0 and pack:
+        return np.array([march_items(c.nx, c.ny, r, march_pack(c.ny)) for c in configs], dtype=np.int64)
     return np.array([((c.nx + r - 1) // r) * ((c.ny + c_ - 1) // c_) for c in configs], dtype=np.int64)
 
 
@@ -155,7 +180,7 @@ def default_tile_x(precision: str) -> int:
 
 class Ensemble:
     def __init__(self, configs: Sequence[Config], tile_x: int = 0, order: str = "instance", ctas: int = 0,
-                 device=None, use_tma: bool | None = None, dynamic: bool = True):
+                 device=None, use_tma: bool | None = None, dynamic: bool = True, pack: bool = True):
         if not configs:
             raise ValueError("empty ensemble")
         precs = {c.precision for c in configs}
@@ -184,6 +209,7 @@ class Ensemble:
         # zero between launches (the kernel's last warp resets it)
         self.queue = torch.zeros(2, dtype=torch.int32, device=self.device)
         self.dynamic = bool(dynamic)
+        self.pack = bool(pack)
         self._graphs = {}
         self.set_schedule(tile_x, order, ctas)
 
@@ -203,16 +229,19 @@ class Ensemble:
         the static split leaves warps idle at the end)."""
         rows, cols = work_shape(tile_x)
         self.tile_x, self.order, self.ctas = int(tile_x), order, int(ctas)
-        counts = tile_counts(self.configs, tile_x)
+        # marching items of the last column strips share warps unless rows are staged by TMA
+        pack = tile_x < 0 and self.pack and not self.tma_staging()
+        counts = tile_counts(self.configs, tile_x, pack)
         tile_order, tile_inst, first = work_list(counts, order)
         table = (_lib.Instance * self.n)()
-        for k, (c, (off, pitch, rows)) in enumerate(zip(self.configs, self.layouts)):
+        for k, c in enumerate(self.configs):
             inst = table[k]
             inst.grid = self._grid(k)
-            inst.offset = off
+            inst.offset = self.layouts[k][0]
             inst.tiles_x = (c.nx + rows - 1) // rows
             inst.tiles_y = (c.ny + cols - 1) // cols
             inst.first_tile = int(first[k])
+            inst.pack = march_pack(c.ny) if pack else 1
         self.n_tiles = int(counts.sum())
         self._table = table
         raw = np.frombuffer(bytes(table), dtype=np.uint8).copy()

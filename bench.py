@@ -67,6 +67,9 @@ def parse_args(argv=None):
     ap.add_argument("--tma", type=int, default=None,
                     help="TMA staging mode: bit 0 the tiled kernel's tiles, bit 1 the marching kernel's rows "
                          "(default: the library's)")
+    ap.add_argument("--no-march-pack", dest="march_pack", action="store_false",
+                    help="one row chunk of the last column strip per warp (default: 2 or 4 share a warp "
+                         "when its leftover columns fit 16 or 8 lanes)")
     ap.add_argument("--tile-x", type=int, default=0,
                     help="stage kernel geometry: 4, 8, 16 (tiled kernel rows), negative (warp-marching rows) "
                          "or 0 (the library default: marching, 24 rows in fp32, 16 in fp64)")
@@ -296,6 +299,7 @@ def run_ours(a, world, rank, local):
     _lib.call("amhd_init")
     tma = _lib.DEFAULT_TMA if a.tma is None else int(a.tma)
     _lib.call("amhd_set_tma", tma)
+    _lib.call("amhd_set_march_pack", 1 if a.march_pack else 0)
     _lib.call("amhd_set_tiling", int(a.tile_x), int(a.ctas_per_sm))
     tx = int(a.tile_x) or _lib.default_tile_x(a.precision)  # the geometry the fp32 / fp64 run uses
     cfg = ot_config(n, a.precision)
@@ -434,7 +438,8 @@ def run_ours(a, world, rank, local):
                    "l2": "inputs larger than L2 (3 state buffers of %.0f MB)" % (10 * (n + 4) * (n + 4) * es / 1e6),
                    "parallelism": f"replicas x{world}", "stage_kernel": stage_geometry(tx),
                    "staging": (("TMA rows (cp.async.bulk.tensor, one box per row)" if tma & 2 else "cp.async rows")
-                               if tx < 0 else "TMA cp.async.bulk.tensor" if tma & 1 else "128-bit loads")},
+                               if tx < 0 else "TMA cp.async.bulk.tensor" if tma & 1 else "128-bit loads"),
+                   "last_strip_packed": bool(a.march_pack and tx < 0 and not tma & 2)},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": loop_launches(tx, a.steps),
         "clocks": clk.summary(), "fp64": fp64, "ensemble": ens_line,
         "reference_cupy_shim": ref_gpu, "reference_numpy_shim": ref_host,
@@ -588,7 +593,8 @@ def run_ensemble(a, world):
     from aeromhd_cuda_b200.autotune import Cache, tune_ensemble
     cfgs = draw_configs(a.ensemble, seed=0, t_end=3.0, precision=a.precision)
     ens = Ensemble(cfgs, tile_x=a.tile_x, order="instance", ctas=a.ensemble_ctas,
-                   use_tma=None if a.tma is None else bool(a.tma & (2 if (a.tile_x or -1) < 0 else 1)))
+                   use_tma=None if a.tma is None else bool(a.tma & (2 if (a.tile_x or -1) < 0 else 1)),
+                   pack=a.march_pack)
     ens.initialize()
     ens.start()
     tuned = None
@@ -614,7 +620,7 @@ def run_ensemble(a, world):
         raise SystemExit("non-finite state in the ensemble benchmark")
     return {"value": world * cells * k / (ms / 1e3), "unit": "zone-updates/s", "instances": a.ensemble,
             "cells": cells, "steps": k, "ms_per_step": ms / k,
-            "schedule": {"tile_x": ens.tile_x, "order": ens.order,
+            "schedule": {"tile_x": ens.tile_x, "order": ens.order, "last_strip_packed": ens.pack,
                          "grid": ("persistent, device work queue" if ens.uses_queue() else "persistent")
                          if ens.ctas >= 0 else "one CTA per work group", "autotuned": tuned}}
 

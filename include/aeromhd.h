@@ -326,7 +326,26 @@ typedef struct amhd_instance {
     int32_t cut_x;           /* x sides that are cuts, not boundaries (bit 0 the
                                 first row, bit 1 the last): excluded from the
                                 boundary energy; 0 for a whole grid             */
+    int32_t pack;            /* marching kernel without TMA staging: row chunks
+                                of the last column strip that share one work
+                                item (amhd_march_pack); 0 or 1: none            */
+    int32_t reserved;        /* zero                                            */
 } amhd_instance;
+
+/* Work items of the warp-marching kernel (tile_x < 0: -tile_x rows x 28
+ * columns per warp).  An instance's last column strip holds ny mod 28
+ * columns; when they and their 2-column halo on each side fit 8 lanes (up to
+ * 4 columns) or 16 lanes (up to 12), amhd_march_pack returns 4 or 2 and that
+ * many row chunks of the strip share one warp, one segment of lanes each;
+ * otherwise 1.  amhd_march_items: the instance's work items with that pack
+ * value -- (chunks x strips) for pack 1, else (strips - 1) x chunks plus
+ * ceil(full-height chunks / pack) plus 1 for a short last chunk.  The packed
+ * items are numbered first, then the full-width strips' items chunk-major. */
+int amhd_march_pack(int32_t ny);
+int amhd_march_items(int32_t nx, int32_t ny, int32_t rows, int32_t pack);
+/* Switch the packing of single-grid calls (1, the default) off (0) or on;
+ * ensembles set amhd_instance.pack themselves.  Results do not depend on it. */
+int amhd_set_march_pack(int32_t on);
 
 /* Advance every active instance of a packed ensemble by n_steps run-loop
  * steps: one persistent launch per RK stage over the (instance, tile) work

@@ -41,7 +41,7 @@ def test_struct_layouts_match(L):
     from aeromhd_cuda_b200 import _lib
     assert L.amhd_control_size() == ctypes.sizeof(_lib.Control) == 160
     assert ctypes.sizeof(_lib.Grid) == 80
-    assert ctypes.sizeof(_lib.Instance) == 104
+    assert ctypes.sizeof(_lib.Instance) == 112
 
 
 def test_version_and_padded_layout(L):
@@ -106,6 +106,48 @@ def test_new_entry_points_reject_bad_arguments(L):
     assert L.amhd_nn_set_gemm_persistent(2) == _lib.AMHD_ERR_ARG
     assert L.amhd_nn_set_gemm_persistent(0) == _lib.AMHD_OK
     assert L.amhd_nn_set_gemm_persistent(1) == _lib.AMHD_OK
+
+
+def test_march_item_counts_agree_with_the_library(L):
+    """The ensemble's work-list arithmetic (ensemble.march_pack / march_items)
+    equals the library's (amhd_march_pack / amhd_march_items), and the packed
+    items cover every (chunk, strip) exactly once: the full-width strips' items
+    plus one segment per full-height chunk of the last strip and one item for
+    a short last chunk."""
+    from aeromhd_cuda_b200 import _lib
+    from aeromhd_cuda_b200.ensemble import MARCH_COLS, march_items, march_pack
+    for ny in range(1, 300):
+        P = march_pack(ny)
+        assert L.amhd_march_pack(ny) == P
+        rem = ny % MARCH_COLS
+        if P > 1:
+            assert rem + 4 <= 32 // P  # the leftover columns and their halo fit a segment
+        else:
+            assert rem == 0 or rem > 12
+    assert [march_pack(n) for n in (32, 64, 128, 256, 2048)] == [4, 2, 1, 4, 4]
+    for nx in (1, 2, 5, 23, 24, 25, 48, 100, 128, 256, 1024, 2048):
+        for ny in (2, 4, 16, 28, 29, 32, 40, 56, 64, 128, 256, 2048):
+            for rows in (4, 16, 24, 32):
+                chunks, strips = -(-nx // rows), -(-ny // MARCH_COLS)
+                for pack in (0, 1, march_pack(ny)):
+                    n = march_items(nx, ny, rows, pack)
+                    assert L.amhd_march_items(nx, ny, rows, pack) == n
+                    if pack <= 1:
+                        assert n == chunks * strips
+                    else:
+                        full = nx // rows
+                        segs = (n - (strips - 1) * chunks) * pack
+                        assert full <= segs - (pack if nx % rows else 0) < full + pack
+    assert ensemble_counts_2048() == (73 * 86 + 22 + 1, 74 * 86)
+    assert L.amhd_march_items(0, 8, 8, 1) == 0
+    assert L.amhd_set_march_pack(2) == _lib.AMHD_ERR_ARG
+    assert L.amhd_set_march_pack(0) == _lib.AMHD_OK
+    assert L.amhd_set_march_pack(1) == _lib.AMHD_OK
+
+
+def ensemble_counts_2048():
+    from aeromhd_cuda_b200.ensemble import march_items, march_pack
+    return march_items(2048, 2048, 24, march_pack(2048)), march_items(2048, 2048, 24, 1)
 
 
 def test_corrector_padding_rows_zeroed_once_per_shape():

@@ -68,13 +68,17 @@ def test_marching_work_queue_gives_identical_results(precision):
     """A persistent marching grid whose warps draw items from the device work
     queue, over several graph replays and eager calls in a row (each launch
     resets the queue for the next), equals one CTA per 4 items and the static
-    split bit for bit; the queue is back at zero after every call."""
+    split bit for bit, with the last strips' row chunks sharing warps or not;
+    the queue is back at zero after every call."""
     from aeromhd_cuda_b200.ensemble import Ensemble
     cfgs = small_configs(precision, n=5, seed=16)
     out = []
-    for order, ctas, dynamic in [("instance", -1, True), ("instance", 0, True), ("largest_first", 0, True),
-                                 ("interleave", 37, True), ("instance", 0, False)]:
-        ens = Ensemble(cfgs, tile_x=-16, order=order, ctas=ctas, dynamic=dynamic)
+    for order, ctas, dynamic, pack in [("instance", -1, True, True), ("instance", 0, True, True),
+                                       ("largest_first", 0, True, True), ("interleave", 37, True, True),
+                                       ("instance", 0, False, True), ("instance", 0, True, False),
+                                       ("interleave", -1, True, False)]:
+        # pack=False: one row chunk of the last column strip per warp instead of 2 or 4
+        ens = Ensemble(cfgs, tile_x=-16, order=order, ctas=ctas, dynamic=dynamic, pack=pack)
         assert ens.uses_queue() == (ctas >= 0 and dynamic)
         ens.initialize()
         ens.start(max_steps=9)
@@ -82,7 +86,7 @@ def test_marching_work_queue_gives_identical_results(precision):
         ens.advance(3)
         ens.advance(3, graph=False)
         torch.cuda.synchronize()
-        assert ens.queue.tolist() == [0, 0], (order, ctas, dynamic)
+        assert ens.queue.tolist() == [0, 0], (order, ctas, dynamic, pack)
         assert all(c.step == 9 for c in ens.controls())
         out.append(ens.U.clone())
     for u in out[1:]:

@@ -525,6 +525,43 @@ def test_persistent_marching_grid_with_queue_equals_default(amhd, precision, cta
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
+@pytest.mark.parametrize("shape,rows,bc_x,bc_y,limiter,cps", [
+    ((75, 32), -8, "periodic", "periodic", "vanleer", 0),        # 4 chunks to a warp, short last chunk
+    ((61, 64), -24, "characteristic", "periodic", "vanleer", 0),  # 2 chunks to a warp
+    ((33, 200), -4, "extrapolation", "extrapolation", "minmod", 0),
+    ((40, 3), -16, "periodic", "extrapolation", "vanleer", 0),   # one strip, all of it packed
+    ((96, 90), -16, "periodic", "periodic", "vanleer", 1),       # persistent grid with the work queue
+])
+def test_packed_last_strip_equals_unpacked(amhd, precision, shape, rows, bc_x, bc_y, limiter, cps):
+    """The last column strip's row chunks sharing warps (amhd_set_march_pack 1,
+    the default) gives the bits of one chunk per warp, step after step through
+    the run loop, for both precisions, every boundary kind and both limiters."""
+    from aeromhd_cuda_b200 import initial_conditions as ic
+    from aeromhd_cuda_b200.ensemble import march_pack
+    nx, ny = shape
+    assert march_pack(ny) > 1
+    res = []
+    try:
+        amhd.lib.call("amhd_set_tiling", rows, cps)
+        for pack in (0, 1):
+            amhd.lib.call("amhd_set_march_pack", pack)
+            cfg = C(nx=nx, ny=ny, x_min=0.0, x_max=1.0, y_min=0.0, y_max=1.0, t_end=0.5, cfl=0.4,
+                    gamma=5.0 / 3.0, powell_mode="on", bc_x_type=bc_x, bc_y_type=bc_y, limiter=limiter,
+                    precision=precision)
+            s = amhd.solver.MHDSolver(cfg)
+            s.set_primitive(ic.orszag_tang(s))
+            s.advance(max_steps=7, chunk=7, graph=False)
+            res.append((s.U.clone(), s.t, s.compute_rhs(s.U).clone()))
+    finally:
+        amhd.lib.call("amhd_set_march_pack", 1)
+        amhd.lib.call("amhd_set_tiling", amhd.lib.DEFAULT_TILE_X, 0)
+    (a, ta, ra), (b, tb, rb) = res
+    assert ta == tb
+    assert torch.equal(a, b)
+    assert torch.equal(ra, rb)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
 @pytest.mark.parametrize("shape,rows", [((80, 80), -8), ((75, 61), -5), ((64, 130), -32), ((33, 29), -4),
                                         ((40, 200), -24)])
 def test_marching_kernel_matches_tiled(amhd, precision, shape, rows):
