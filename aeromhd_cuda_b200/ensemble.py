@@ -224,9 +224,13 @@ class Ensemble:
         to SMs as they free up.  On a persistent marching grid each warp takes
         the next free item from a device work queue when it finishes one
         (``dynamic``, the default): on the uneven 256-instance ensemble as fast
-        as one CTA per 4 items (6.67 against 6.69 G zone-updates/s); with
-        dynamic=False warp w takes items w, w + warps, ... (20-30 % slower:
-        the static split leaves warps idle at the end)."""
+        as one CTA per 4 items (6.67 against 6.69 G zone-updates/s, measured
+        before the last strips were packed); with dynamic=False warp w takes
+        items w, w + warps, ... (20-30 % slower: the static split leaves warps
+        idle at the end).  With ``pack`` (the constructor's, default on) the
+        marching kernel runs 2 or 4 row chunks of an instance's narrow last
+        column strip in one warp (march_pack): 7.39 against 6.63 G on that
+        ensemble, identical results."""
         rows, cols = work_shape(tile_x)
         self.tile_x, self.order, self.ctas = int(tile_x), order, int(ctas)
         # marching items of the last column strips share warps unless rows are staged by TMA
