@@ -359,7 +359,9 @@ int amhd_march_pack(int32_t ny) { return ny > 0 ? march_pack(ny) : 1; }
 
 int amhd_march_items(int32_t nx, int32_t ny, int32_t rows, int32_t pack)
 {
-    if (nx <= 0 || ny <= 0 || rows <= 0) return 0;
+    if (nx <= 0 || ny <= 0 || rows <= 0) return fail(AMHD_ERR_ARG, "nx, ny and rows must be positive");
+    if (pack > 1 && pack != march_pack(ny))
+        return fail(AMHD_ERR_ARG, "pack must be 0, 1 or amhd_march_pack(%d) = %d, got %d", ny, march_pack(ny), pack);
     return march_item_count(nx, ny, rows, pack);
 }
 

@@ -748,9 +748,10 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
     // their 2-column halo on each side) fit 32/P lanes, put P segments of 32/P
     // lanes side by side, segment s walking chunk P m + s; all segments of an
     // item have as many rows (the short last chunk has an item of its own).
-    // The packed items come first, the plain ones chunk-major after them.
+    // The packed items come first, the plain ones chunk-major after them.  A pack
+    // value other than the rule's (march_pack) is taken as none.
     const int local = item - in.first_tile;
-    const int P = (TMA || in.pack <= 1) ? 1 : in.pack;
+    const int P = (TMA || in.pack <= 1 || in.pack != march_pack(g.ny)) ? 1 : in.pack;
     const int plain_strips = P > 1 ? in.tiles_y - 1 : in.tiles_y;
     const int full_chunks = g.nx / p.march_rows;
     const int n_full_packed = P > 1 ? (full_chunks + P - 1) / P : 0;
@@ -778,6 +779,7 @@ __device__ __forceinline__ bool march_walk(const StageParams &p, MarchSmem<R, TM
             n_rows = g.nx - full_chunks * p.march_rows;
         }
     }
+    if (n_rows <= 0) return true;  // an item past the instance's last (a work list that counts too many)
     const int j = kMarchCols * strip + lane_c;  // storage column of this lane (first interior column - 2 + lane_c)
     // ghost cells of the input: as stored, or (pull) taken from the interior cells
     // they copy (apply_bc, solver.py:158-197; psi zero in non-periodic x ghosts)

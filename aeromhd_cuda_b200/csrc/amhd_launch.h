@@ -55,7 +55,7 @@ inline bool is_march(int tile_x) { return tile_x < 0; }
 // row chunks of an instance's last column strip per work item: its ny mod 28
 // leftover columns plus a 2-column halo each side in 8 lanes (4 chunks to a
 // warp) or 16 lanes (2); 1 when the strip is full or wider than 12 columns
-inline int march_pack(int ny)
+__host__ __device__ inline int march_pack(int ny)
 {
     const int rem = ny % kMarchCols;
     return rem == 0 ? 1 : rem <= 4 ? 4 : rem <= 12 ? 2 : 1;

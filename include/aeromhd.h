@@ -328,7 +328,8 @@ typedef struct amhd_instance {
                                 boundary energy; 0 for a whole grid             */
     int32_t pack;            /* marching kernel without TMA staging: row chunks
                                 of the last column strip that share one work
-                                item (amhd_march_pack); 0 or 1: none            */
+                                item, amhd_march_pack(grid.ny); 0 or 1: none
+                                (any other value is taken as none)              */
     int32_t reserved;        /* zero                                            */
 } amhd_instance;
 
@@ -340,7 +341,10 @@ typedef struct amhd_instance {
  * otherwise 1.  amhd_march_items: the instance's work items with that pack
  * value -- (chunks x strips) for pack 1, else (strips - 1) x chunks plus
  * ceil(full-height chunks / pack) plus 1 for a short last chunk.  The packed
- * items are numbered first, then the full-width strips' items chunk-major. */
+ * items are numbered first, then the full-width strips' items chunk-major.
+ * Both return a count; amhd_march_items returns AMHD_ERR_ARG for a
+ * non-positive size or a pack other than 0, 1 or amhd_march_pack(ny).  A
+ * work list with more items than this count has the extra ones skipped. */
 int amhd_march_pack(int32_t ny);
 int amhd_march_items(int32_t nx, int32_t ny, int32_t rows, int32_t pack);
 /* Switch the packing of single-grid calls (1, the default) off (0) or on;

@@ -139,7 +139,9 @@ def test_march_item_counts_agree_with_the_library(L):
                         segs = (n - (strips - 1) * chunks) * pack
                         assert full <= segs - (pack if nx % rows else 0) < full + pack
     assert ensemble_counts_2048() == (73 * 86 + 22 + 1, 74 * 86)
-    assert L.amhd_march_items(0, 8, 8, 1) == 0
+    assert L.amhd_march_items(0, 8, 8, 1) == _lib.AMHD_ERR_ARG
+    assert L.amhd_march_items(64, 64, 8, 4) == _lib.AMHD_ERR_ARG  # 64 leaves 8 columns: 2 chunks to a warp
+    assert L.amhd_march_items(64, 128, 8, 2) == _lib.AMHD_ERR_ARG  # 128 leaves 16: none
     assert L.amhd_set_march_pack(2) == _lib.AMHD_ERR_ARG
     assert L.amhd_set_march_pack(0) == _lib.AMHD_OK
     assert L.amhd_set_march_pack(1) == _lib.AMHD_OK
