@@ -119,3 +119,58 @@ def test_ensemble_default_geometry():
     from aeromhd_cuda_b200.ensemble import default_tile_x
     assert default_tile_x("fp32") == -32
     assert default_tile_x("fp64") == _lib.default_tile_x("fp64") == -16
+
+
+def _packed_item_cells(nx, ny, rows, pack):
+    """Cells (row, column) each marching work item updates, restating the
+    kernel's item decode (march_walk, amhd_kernels.cuh): packed items first
+    (segments of 32/P lanes, segment s on row chunk P m + s, the short last
+    chunk alone), then the full-width strips' items chunk-major.  Also checks
+    that every segment of an item walks as many rows and reads rows inside
+    the padded grid."""
+    from aeromhd_cuda_b200.ensemble import MARCH_COLS, march_items
+    NG = 2
+    chunks, strips = -(-nx // rows), -(-ny // MARCH_COLS)
+    P = pack if pack > 1 else 1
+    plain = strips - 1 if P > 1 else strips
+    full = nx // rows
+    n_packed = (-(-full // P) + (1 if full * rows < nx else 0)) if P > 1 else 0
+    out = []
+    for local in range(march_items(nx, ny, rows, pack)):
+        cells, heights = [], set()
+        for lane in range(32):
+            seg_w, lane_c, live = 32, lane, True
+            if local >= n_packed:
+                strip, chunk = (local - n_packed) % plain, (local - n_packed) // plain
+                n_rows = min(rows, nx - chunk * rows)
+            else:
+                seg = lane >> 3 if P == 4 else lane >> 4
+                seg_w = 8 if P == 4 else 16
+                lane_c, strip = lane - seg * seg_w, strips - 1
+                if local < -(-full // P):
+                    chunk = local * P + seg
+                    live = chunk < full
+                    chunk = chunk if live else local * P
+                    n_rows = rows
+                else:
+                    chunk, live, n_rows = full, seg == 0, nx - full * rows
+            heights.add(n_rows)
+            j, ib = MARCH_COLS * strip + lane_c, NG + chunk * rows
+            assert 0 <= ib - 2 and ib + n_rows + 1 <= nx + 2 * NG - 1
+            if live and NG <= lane_c < seg_w - NG and j < NG + ny:
+                cells += [(i, j) for i in range(ib, ib + n_rows)]
+        assert len(heights) == 1 and heights.pop() >= 1
+        out.append(cells)
+    return out
+
+
+@pytest.mark.parametrize("nx,rows", [(1, 4), (23, 24), (24, 24), (75, 8), (100, 32), (256, 16)])
+def test_packed_items_update_every_cell_once(nx, rows):
+    """With the last strip's row chunks packed (march_pack) or not, the work
+    items of a grid update every interior cell exactly once."""
+    from aeromhd_cuda_b200.ensemble import march_pack
+    for ny in (1, 2, 3, 4, 5, 16, 28, 30, 32, 33, 40, 60, 64, 100, 128, 256):
+        want = {(i, j) for i in range(2, nx + 2) for j in range(2, ny + 2)}
+        for pack in (1, march_pack(ny)):
+            seen = [c for item in _packed_item_cells(nx, ny, rows, pack) for c in item]
+            assert len(seen) == len(set(seen)) and set(seen) == want, (nx, ny, rows, pack)
