@@ -5,8 +5,9 @@
  * CFL dt), plus the batched-ensemble driver.
  *
  * Conventions
- *   - Every entry point returns int: AMHD_OK (0) or a negative AMHD_ERR_*;
- *     amhd_last_error() gives a message for the calling thread.
+ *   - Every entry point returns int: AMHD_OK (0) or a negative AMHD_ERR_*
+ *     (amhd_march_pack and amhd_march_items return a count, or a negative
+ *     AMHD_ERR_*); amhd_last_error() gives a message for the calling thread.
  *   - All array pointers are DEVICE pointers owned by the caller unless the
  *     name says _host.  The library never allocates device memory on a step.
  *   - `stream` is a cudaStream_t passed as void*; calls are asynchronous on
